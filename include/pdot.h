@@ -1,0 +1,244 @@
+/*
+ * pdot.h — C ABI of libpdot.so, a B200 (sm_100a) implementation of PDOT's
+ * restarted, adaptive-step PDHG solver for discrete optimal transport.
+ *
+ * The ABI mirrors the reference's Julia API (MIT-Lu-Lab/PDOT.jl) so that a
+ * thin Julia module can `ccall` into it and keep the reference's types:
+ *
+ *   optimize(params::PdhgParameters, problem::OptimalTransportProblem)
+ *       -> SaddlePointOutput                         src/solver_gpu.jl:413-720
+ *
+ * Conventions
+ *   - Matrices are column-major with leading dimension num_row, exactly as a
+ *     Julia Matrix{Float64} is laid out: entry (i, j) sits at i + j*num_row.
+ *     i indexes sources (rows), j indexes targets (columns).
+ *   - Every enum value is the 0-based position of the matching member of the
+ *     reference's `@enum` declaration.
+ *   - Functions return 0 on success and a negative PDOT_ERR_* code on failure;
+ *     pdot_last_error() then returns a thread-local message. Solver outcomes
+ *     (optimal, iteration limit, numerical error, ...) are not errors: they are
+ *     reported in pdot_saddle_point_output.termination_reason.
+ *   - No C++ exception crosses this boundary. Calls are blocking.
+ */
+#ifndef PDOT_H
+#define PDOT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PDOT_ABI_VERSION 1
+
+/* ---- error codes ------------------------------------------------------- */
+enum {
+  PDOT_OK = 0,
+  PDOT_ERR_INVALID_ARGUMENT = -1, /* bad sizes, null pointers, parameter asserts */
+  PDOT_ERR_CUDA = -2,             /* a CUDA runtime call failed */
+  PDOT_ERR_OUT_OF_MEMORY = -3,    /* device allocation failed */
+  PDOT_ERR_NO_DEVICE = -4,        /* no CUDA device, or not an sm_100 device */
+  PDOT_ERR_TOO_LARGE = -5         /* a size exceeds a documented maximum */
+};
+
+/* ---- enums (values = 0-based order of the reference's @enum) ----------- */
+/* OptimalityNorm, src/termination.jl:2 */
+enum { PDOT_L_INF = 0, PDOT_L_2 = 1 };
+/* RestartScheme, src/saddle_point_gpu.jl:401 */
+enum { PDOT_NO_RESTARTS = 0, PDOT_FIXED_FREQUENCY = 1, PDOT_ADAPTIVE_KKT = 2 };
+/* RestartToCurrentMetric, src/saddle_point_gpu.jl:408 */
+enum { PDOT_NO_RESTART_TO_CURRENT = 0, PDOT_KKT_GREEDY = 1 };
+/* RestartChoice, src/solve_log.jl:15-20 */
+enum {
+  PDOT_RESTART_CHOICE_UNSPECIFIED = 0,
+  PDOT_RESTART_CHOICE_NO_RESTART = 1,
+  PDOT_RESTART_CHOICE_WEIGHTED_AVERAGE_RESET = 2,
+  PDOT_RESTART_CHOICE_RESTART_TO_AVERAGE = 3
+};
+/* PointType, src/solve_log.jl:35-41 */
+enum {
+  PDOT_POINT_TYPE_UNSPECIFIED = 0,
+  PDOT_POINT_TYPE_CURRENT_ITERATE = 1,
+  PDOT_POINT_TYPE_ITERATE_DIFFERENCE = 2,
+  PDOT_POINT_TYPE_AVERAGE_ITERATE = 3,
+  PDOT_POINT_TYPE_NONE = 4
+};
+/* TerminationReason, src/solve_log.jl:245-254 */
+enum {
+  PDOT_TERMINATION_REASON_UNSPECIFIED = 0,
+  PDOT_TERMINATION_REASON_OPTIMAL = 1,
+  PDOT_TERMINATION_REASON_TIME_LIMIT = 2,
+  PDOT_TERMINATION_REASON_ITERATION_LIMIT = 3,
+  PDOT_TERMINATION_REASON_KKT_MATRIX_PASS_LIMIT = 4,
+  PDOT_TERMINATION_REASON_NUMERICAL_ERROR = 5,
+  PDOT_TERMINATION_REASON_INVALID_PROBLEM = 6,
+  PDOT_TERMINATION_REASON_OTHER = 7
+};
+/* Union{AdaptiveStepsizeParams, ConstantStepsizeParams}, src/solver_gpu.jl:2-7,17-20 */
+enum { PDOT_STEP_SIZE_ADAPTIVE = 0, PDOT_STEP_SIZE_CONSTANT = 1 };
+
+/* ---- problem: OptimalTransportProblem, src/io.jl:1-5 -------------------- */
+typedef struct pdot_problem {
+  int64_t num_row;                    /* m, number of sources */
+  int64_t num_col;                    /* n, number of targets */
+  const double* cost_matrix;          /* m*n, column-major, ld = m (host memory) */
+  const double* source_distribution;  /* m (host memory) */
+  const double* target_distribution;  /* n (host memory) */
+} pdot_problem;
+
+/* ---- parameters --------------------------------------------------------- */
+/* TerminationCriteria, src/termination.jl:5-51 (same field order) */
+typedef struct pdot_termination_criteria {
+  int32_t optimality_norm;            /* PDOT_L_INF or PDOT_L_2 */
+  double eps_optimal_absolute;
+  double eps_optimal_relative;
+  double time_sec_limit;              /* +inf for none */
+  int32_t iteration_limit;            /* INT32_MAX for none */
+  double kkt_matrix_pass_limit;       /* +inf for none */
+} pdot_termination_criteria;
+
+/* RestartParameters, src/saddle_point_gpu.jl:411-441 (same field order) */
+typedef struct pdot_restart_parameters {
+  int32_t restart_scheme;             /* PDOT_NO_RESTARTS / FIXED_FREQUENCY / ADAPTIVE_KKT */
+  int32_t restart_to_current_metric;  /* PDOT_NO_RESTART_TO_CURRENT / PDOT_KKT_GREEDY */
+  int64_t restart_frequency_if_fixed;
+  double artificial_restart_threshold;
+  double sufficient_reduction_for_restart;
+  double necessary_reduction_for_restart;
+  double primal_weight_update_smoothing;
+} pdot_restart_parameters;
+
+/* PdhgParameters, src/solver_gpu.jl:9-21 (same field order; the
+ * Union{AdaptiveStepsizeParams, ConstantStepsizeParams} is a tag plus the
+ * AdaptiveStepsizeParams fields, src/solver_gpu.jl:2-7) */
+typedef struct pdot_pdhg_parameters {
+  double primal_importance;
+  int32_t scale_invariant_initial_primal_weight;  /* Bool */
+  int64_t verbosity;                              /* printing is left to the host language */
+  int32_t record_iteration_stats;                 /* Bool */
+  int32_t termination_evaluation_frequency;
+  pdot_termination_criteria termination_criteria;
+  pdot_restart_parameters restart_params;
+  int32_t step_size_policy;                       /* PDOT_STEP_SIZE_ADAPTIVE / _CONSTANT */
+  double reduction_exponent;                      /* AdaptiveStepsizeParams */
+  double growth_exponent;                         /* AdaptiveStepsizeParams */
+} pdot_pdhg_parameters;
+
+/* Options of this implementation that have no counterpart in the reference.
+ * Pass NULL for the defaults (device 0, FP64 drop-in, CUDA graphs on). */
+typedef struct pdot_solver_options {
+  int32_t device;                     /* CUDA device ordinal */
+  int32_t use_cuda_graph;             /* 1: replay captured iteration chunks */
+  int32_t reserved[14];               /* must be zero */
+} pdot_solver_options;
+
+/* ---- output -------------------------------------------------------------- */
+/* ConvergenceInformation, src/solve_log.jl:47-147 (same field order) */
+typedef struct pdot_convergence_information {
+  int32_t candidate_type;             /* PointType */
+  double primal_objective;
+  double dual_objective;
+  double corrected_dual_objective;
+  double l_inf_primal_residual;
+  double l2_primal_residual;
+  double l_inf_dual_residual;
+  double l2_dual_residual;
+  double relative_l_inf_primal_residual;
+  double relative_l2_primal_residual;
+  double relative_l_inf_dual_residual;
+  double relative_l2_dual_residual;
+  double relative_optimality_gap;
+  double l_inf_primal_variable;
+  double l2_primal_variable;
+  double l_inf_dual_variable;
+  double l2_dual_variable;
+} pdot_convergence_information;
+
+/* IterationStats, src/solve_log.jl:154-228 (same field order; the single
+ * ConvergenceInformation the reference stores is inlined and the one
+ * method-specific stat the reference records, src/solver_gpu.jl:579-581, is a
+ * field) */
+typedef struct pdot_iteration_stats {
+  int32_t iteration_number;
+  pdot_convergence_information convergence_information;
+  double cumulative_kkt_matrix_passes;
+  int32_t cumulative_rejected_steps;
+  double cumulative_time_sec;
+  int32_t restart_used;               /* RestartChoice */
+  double step_size;
+  double primal_weight;
+  double time_spent_doing_basic_algorithm;
+} pdot_iteration_stats;
+
+/* SaddlePointOutput, src/saddle_point_gpu.jl:2-34. The caller owns every
+ * array. A NULL solution pointer skips that copy. */
+typedef struct pdot_saddle_point_output {
+  double* primal_solution;            /* m*n column-major, or NULL */
+  double* dual_source_solution;       /* m, or NULL */
+  double* dual_target_solution;       /* n, or NULL */
+  pdot_iteration_stats* iteration_stats; /* capacity records, or NULL */
+  int64_t iteration_stats_capacity;
+  int64_t iteration_stats_count;      /* out: records produced (can exceed capacity) */
+  int32_t termination_reason;         /* out: TerminationReason */
+  int32_t iteration_count;            /* out: iterations, src/solver_gpu.jl:661 */
+  double solve_time_sec;              /* out: cumulative_time_sec of the last record */
+  pdot_iteration_stats final_stats;   /* out: the record that ended the solve */
+} pdot_saddle_point_output;
+
+/* ---- solver entry points ------------------------------------------------- */
+
+/* Library identity. Returns PDOT_ABI_VERSION. */
+int pdot_version(void);
+
+/* Thread-local description of the last error on this thread ("" if none). */
+const char* pdot_last_error(void);
+
+/* Replaces PDOT.optimize(params, problem), src/solver_gpu.jl:413-720, with
+ * the host->device copy of src/io.jl:18-36 and the device->host copy of
+ * src/io.jl:41-53 inside. Parameter validation follows
+ * src/solver_gpu.jl:420-422 and src/saddle_point_gpu.jl:455-461 and returns
+ * PDOT_ERR_INVALID_ARGUMENT where the reference raises. `options` may be NULL. */
+int pdot_optimize(const pdot_problem* problem,
+                  const pdot_pdhg_parameters* params,
+                  const pdot_solver_options* options,
+                  pdot_saddle_point_output* output);
+
+/* Fills `params` with the values scripts/solve.jl:58-86 uses
+ * (ADAPTIVE_KKT, KKT_GREEDY, 1000, 0.36, 0.1, 0.9, 0.5; L_2; eps = tolerance;
+ * primal_importance 1.0; record stats; evaluation every 128 iterations;
+ * AdaptiveStepsizeParams(2, 1)). */
+void pdot_default_parameters(double tolerance, pdot_pdhg_parameters* params);
+
+/* ---- device-level entry points of the hot path --------------------------- */
+/* These act on device memory (pointers from cudaMalloc or torch) and on the
+ * given CUDA stream (NULL = legacy default stream); they are the per-iteration
+ * building blocks that pdot_optimize chains. */
+
+/* One fused primal pass, replacing compute_next_primal_solution_kernel! plus
+ * the two `sum(delta_primal; dims)` reductions (src/solver_gpu.jl:125-174),
+ * `current_primal_solution .+= delta_primal` (src/solver_gpu.jl:242), the
+ * gradient refresh (src/solver_gpu.jl:249-250, recomputed on the fly from
+ * C, u, v instead of stored) and the primal weighted average
+ * (src/saddle_point_gpu.jl:115-135). For every entry:
+ *     g    = (C - u[i]) - v[j]                (g = 0 if flags & PDOT_PASS_ZERO_GRADIENT)
+ *     p    = max(X - step_over_weight*g, 0)
+ *     d    = p - X;   X <- X + d
+ *     Xavg <- (Xavg + X*avg_new_weight)*avg_scale   (Xavg <- X if flags & PDOT_PASS_FIRST_AVERAGE)
+ * and it returns delta_row_sum[i] = sum_j d, delta_col_sum[j] = sum_i d and
+ * delta_sq_norm[0] = sum d^2. Reductions are deterministic (fixed order).
+ * `workspace` must hold pdot_primal_pass_workspace_bytes(m, n) bytes. */
+enum { PDOT_PASS_ZERO_GRADIENT = 1, PDOT_PASS_FIRST_AVERAGE = 2 };
+int64_t pdot_primal_pass_workspace_bytes(int64_t m, int64_t n);
+int pdot_primal_pass_f64(int64_t m, int64_t n,
+                         const double* cost, double* primal, double* primal_avg,
+                         const double* dual_source, const double* dual_target,
+                         double step_over_weight, double avg_new_weight, double avg_scale,
+                         int32_t flags,
+                         double* delta_row_sum, double* delta_col_sum, double* delta_sq_norm,
+                         void* workspace, int64_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PDOT_H */

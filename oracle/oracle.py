@@ -1,0 +1,85 @@
+"""Python binding of the CPU oracle (oracle/libpdot_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and by
+bench.py's CPU-baseline leg, as the checker. The product (libpdot.so and the
+`pdot` package) never imports this module.
+
+It drives the oracle through the same C structs as libpdot.so (include/pdot.h),
+so `optimize` here takes and returns the same Python types as `pdot.optimize`.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpdot_oracle.so")
+
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return LIB_PATH
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        build()
+    from pdot import _abi
+
+    lib = ct.CDLL(LIB_PATH)
+    lib.pdot_oracle_optimize.restype = ct.c_int
+    lib.pdot_oracle_optimize.argtypes = [
+        ct.POINTER(_abi.ProblemC), ct.POINTER(_abi.PdhgParametersC),
+        ct.POINTER(_abi.SaddlePointOutputC), ct.c_int,
+    ]
+    P = ct.c_void_p
+    D = ct.c_double
+    lib.pdot_oracle_primal_pass.restype = None
+    lib.pdot_oracle_primal_pass.argtypes = [
+        ct.c_int64, ct.c_int64, P, P, P, P, P, D, D, D, ct.c_int32, P, P, P,
+    ]
+    lib.pdot_oracle_version.restype = ct.c_int
+    _lib = lib
+    return lib
+
+
+def optimize(params, problem, num_threads: int = 0):
+    """The oracle's PDOT.optimize: same inputs and outputs as pdot.optimize."""
+    from pdot import api, _abi
+
+    api.validate(params)
+    lib = load()
+    mp = api.MarshalledProblem(problem)
+    cp = api.marshal_params(params)
+    ob = api.OutputBuffers(mp.m, mp.n, api.stats_capacity_for(params))
+    rc = lib.pdot_oracle_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(ob.c), int(num_threads))
+    if rc != 0:
+        raise _abi.PdotError(rc, f"oracle optimize failed ({rc})")
+    return ob.to_output()
+
+
+def _p(a: np.ndarray):
+    return ct.c_void_p(a.ctypes.data)
+
+
+def primal_pass(C, X, Xa, u, v, step_over_weight, avg_new_weight, avg_scale, flags):
+    """Oracle counterpart of pdot_primal_pass_f64. X and Xa (Fortran order,
+    float64) are updated in place; returns (delta_row_sum, delta_col_sum, sq)."""
+    lib = load()
+    m, n = C.shape
+    for arr in (C, X, Xa):
+        assert arr.flags.f_contiguous and arr.dtype == np.float64
+    drow = np.zeros(m)
+    dcol = np.zeros(n)
+    dsq = np.zeros(1)
+    lib.pdot_oracle_primal_pass(m, n, _p(C), _p(X), _p(Xa), _p(u), _p(v), step_over_weight,
+                                avg_new_weight, avg_scale, flags, _p(drow), _p(dcol), _p(dsq))
+    return drow, dcol, float(dsq[0])

@@ -1,0 +1,764 @@
+/*
+ * pdot_oracle.c — CPU FP64 restatement of PDOT's restarted adaptive PDHG for
+ * discrete optimal transport (MIT-Lu-Lab/PDOT.jl).
+ *
+ * TEST INFRASTRUCTURE ONLY. This file is the checker: the parity tests, the
+ * smoke check and the CPU-baseline leg of bench.py call it to judge the CUDA
+ * solver. Nothing in the product links or calls it.
+ *
+ * Parity status: the reference is Julia + CUDA.jl and ships no tests, golden
+ * vectors or fixtures, and no Julia toolchain is available to run it, so the
+ * trajectory is "parity unpinned" against the reference itself. The final
+ * objectives this oracle reaches are pinned against an independent exact LP
+ * solve (scipy HiGHS) and against analytic optima in tests/test_oracle.py.
+ *
+ * The restatement follows the reference statement by statement, keeping the
+ * stored gradient G, the averaged gradient, the delta buffer and the restart
+ * copies exactly as the reference keeps them, so that it is also the honest
+ * "reference algorithm on CPU arrays" baseline. Elementwise arithmetic is done
+ * in the reference's operation order; compile with -ffp-contract=off so that
+ * no multiply-add is fused (Julia does not fuse them either). Reductions use a
+ * fixed order (per column, then over columns), independent of the thread count.
+ * The order inside CUDA.jl's sum/dot/norm is not published, so sums agree with
+ * the reference only to rounding.
+ *
+ * The structs are the ones of include/pdot.h, so the oracle and libpdot.so
+ * are driven through the same C ABI.
+ */
+#include "../include/pdot.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef int64_t i64;
+
+/* ---- Julia scalar semantics ------------------------------------------- */
+
+/* Base.max(x, 0.0) for Float64: NaN propagates, -0.0 becomes 0.0. */
+static inline double jl_max0(double x) { return x > 0.0 ? x : (x != x ? x : 0.0); }
+/* Base.min(x, 0.0): NaN propagates, keeps -0.0. */
+static inline double jl_min0(double x) { return x < 0.0 ? x : (x != x ? x : (signbit(x) ? x : 0.0)); }
+/* Base.min(x, y) for Float64 (NaN propagating). */
+static inline double jl_min(double x, double y) {
+  if (x != x) return x;
+  if (y != y) return y;
+  return y < x ? y : x;
+}
+
+static double now_sec(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+/* ---- deterministic reductions ---------------------------------------- */
+
+typedef struct {
+  i64 m, n;
+  double* colbuf; /* n partials */
+} red_ctx;
+
+static double vec_dot(const double* x, const double* y, i64 len) {
+  double s = 0.0;
+  for (i64 i = 0; i < len; ++i) s += x[i] * y[i];
+  return s;
+}
+static double vec_sumsq(const double* x, i64 len) {
+  double s = 0.0;
+  for (i64 i = 0; i < len; ++i) s += x[i] * x[i];
+  return s;
+}
+static double vec_maxabs(const double* x, i64 len) {
+  double s = 0.0;
+  for (i64 i = 0; i < len; ++i) {
+    double a = fabs(x[i]);
+    if (a != a) return a;
+    if (a > s) s = a;
+  }
+  return s;
+}
+/* norm([x; y], 2) and norm([x; y], Inf) */
+static double cat_nrm2(const double* x, i64 lx, const double* y, i64 ly) {
+  return sqrt(vec_sumsq(x, lx) + vec_sumsq(y, ly));
+}
+static double cat_nrminf(const double* x, i64 lx, const double* y, i64 ly) {
+  double a = vec_maxabs(x, lx), b = vec_maxabs(y, ly);
+  if (a != a) return a;
+  if (b != b) return b;
+  return a > b ? a : b;
+}
+
+static double sum_cols(red_ctx* R) {
+  double s = 0.0;
+  for (i64 j = 0; j < R->n; ++j) s += R->colbuf[j];
+  return s;
+}
+static double max_cols(red_ctx* R) {
+  double s = 0.0;
+  for (i64 j = 0; j < R->n; ++j) {
+    double a = R->colbuf[j];
+    if (a != a) return a;
+    if (a > s) s = a;
+  }
+  return s;
+}
+
+/* CUDA.dot(A, B) over m*n entries */
+static double mat_dot(red_ctx* R, const double* A, const double* B) {
+  const i64 m = R->m, n = R->n;
+#pragma omp parallel for schedule(static)
+  for (i64 j = 0; j < n; ++j) {
+    const double* a = A + j * m;
+    const double* b = B + j * m;
+    double s = 0.0;
+    for (i64 i = 0; i < m; ++i) s += a[i] * b[i];
+    R->colbuf[j] = s;
+  }
+  return sum_cols(R);
+}
+/* CUDA.norm(A) (Frobenius) */
+static double mat_nrm2(red_ctx* R, const double* A) {
+  const i64 m = R->m, n = R->n;
+#pragma omp parallel for schedule(static)
+  for (i64 j = 0; j < n; ++j) {
+    const double* a = A + j * m;
+    double s = 0.0;
+    for (i64 i = 0; i < m; ++i) s += a[i] * a[i];
+    R->colbuf[j] = s;
+  }
+  return sqrt(sum_cols(R));
+}
+/* CUDA.norm(A, Inf) */
+static double mat_nrminf(red_ctx* R, const double* A) {
+  const i64 m = R->m, n = R->n;
+#pragma omp parallel for schedule(static)
+  for (i64 j = 0; j < n; ++j) {
+    const double* a = A + j * m;
+    double s = 0.0;
+    for (i64 i = 0; i < m; ++i) {
+      double v = fabs(a[i]);
+      if (v != v) { s = v; break; }
+      if (v > s) s = v;
+    }
+    R->colbuf[j] = s;
+  }
+  return max_cols(R);
+}
+
+/* ---- state, mirroring the reference's structs ------------------------ */
+
+typedef struct {
+  /* CuOptimalTransportProblem, src/io.jl:7-13 */
+  i64 m, n;
+  const double *C, *a, *b;
+  /* CachedOTInfo, src/termination.jl:87-92 */
+  double linf_obj, linf_rhs, l2_obj, l2_rhs;
+  /* CuPdhgSolverState, src/solver_gpu.jl:23-36 */
+  double *X, *u, *v, *r, *c, *G;
+  double step_size, primal_weight, kkt_passes;
+  int numerical_error;
+  i64 total_iters;
+  /* CuSolutionWeightedAverage, src/saddle_point_gpu.jl:52-65 */
+  double *Xa, *ua, *va, *ra, *ca, *Ga;
+  i64 pcount, scount, tcount;
+  double Sp, Ss, St;
+  /* CuBufferState, src/solver_gpu.jl:39-49 */
+  double *dX, *nu, *nv, *du, *dv, *dr, *dc, *nr, *nc;
+  /* CuRestartInfo, src/saddle_point_gpu.jl:332-366 */
+  double *Xl, *ul, *vl, *rl, *cl, *Gl;
+  i64 last_restart_length;
+  double pdist, ddist, ratio_last_trial;
+  /* buffer_kkt's scratch vectors */
+  double *viol_s, *viol_t;
+  red_ctx R;
+} ostate;
+
+/* ---- src/solver_gpu.jl:125-174  compute_next_primal_solution! ------- */
+static void next_primal(ostate* S, double step_size, double primal_weight) {
+  const i64 m = S->m, n = S->n;
+  const double sg = step_size / primal_weight;
+#pragma omp parallel for schedule(static)
+  for (i64 j = 0; j < n; ++j) {
+    const double* X = S->X + j * m;
+    const double* G = S->G + j * m;
+    double* d = S->dX + j * m;
+    double cs = 0.0;
+    for (i64 i = 0; i < m; ++i) {
+      double t = X[i] - sg * G[i];   /* :139 */
+      t = jl_max0(t);                /* :140 */
+      t -= X[i];                     /* :141 */
+      d[i] = t;
+      cs += t;
+    }
+    S->nc[j] = cs; /* sum(delta_primal, dims=1), completed below */
+  }
+  /* :172 next_primal_row_sum = sum(delta_primal, dims=2) + current_primal_row_sum */
+#pragma omp parallel
+  {
+#ifdef _OPENMP
+    int nt = omp_get_num_threads(), t = omp_get_thread_num();
+#else
+    int nt = 1, t = 0;
+#endif
+    i64 lo = m * t / nt, hi = m * (t + 1) / nt;
+    for (i64 i = lo; i < hi; ++i) S->nr[i] = 0.0;
+    for (i64 j = 0; j < n; ++j) {
+      const double* d = S->dX + j * m;
+      for (i64 i = lo; i < hi; ++i) S->nr[i] += d[i];
+    }
+    for (i64 i = lo; i < hi; ++i) S->nr[i] = S->nr[i] + S->r[i];
+  }
+  /* :173 */
+  for (i64 j = 0; j < n; ++j) S->nc[j] = S->nc[j] + S->c[j];
+}
+
+/* ---- src/solver_gpu.jl:177-234  compute_next_dual_solution! --------- */
+static void next_dual_1(const double* dist, const double* cur, const double* cur_sum,
+                        const double* next_sum, double step_size, double primal_weight,
+                        i64 len, double* next) {
+  const double tw = step_size * primal_weight;
+  for (i64 i = 0; i < len; ++i)
+    next[i] = cur[i] + tw * ((dist[i] - 2.0 * next_sum[i]) + cur_sum[i]); /* :191 */
+}
+static void next_dual(ostate* S, double step_size, double primal_weight) {
+  next_dual_1(S->a, S->u, S->r, S->nr, step_size, primal_weight, S->m, S->nu);
+  next_dual_1(S->b, S->v, S->c, S->nc, step_size, primal_weight, S->n, S->nv);
+}
+
+/* ---- src/saddle_point_gpu.jl:115-289  weighted averages -------------- */
+static void avg_weights(double Ssum, double w, double* nw, double* aw) {
+  if (Ssum > 0.0) {
+    *aw = Ssum / (Ssum + w);
+    *nw = w / Ssum;
+  } else {
+    *nw = 1.0;
+    *aw = 1.0;
+  }
+}
+static void avg_vec(double* avg, const double* cur, i64 len, double nw, double aw) {
+  for (i64 i = 0; i < len; ++i) avg[i] = avg[i] + cur[i] * nw;
+  for (i64 i = 0; i < len; ++i) avg[i] = avg[i] * aw;
+}
+static void avg_mat(ostate* S, double* avg, const double* cur, double nw, double aw) {
+  const i64 N = S->m * S->n;
+#pragma omp parallel for schedule(static)
+  for (i64 e = 0; e < N; ++e) avg[e] = (avg[e] + cur[e] * nw) * aw;
+}
+static void add_to_solution_weighted_average(ostate* S, double weight) {
+  double nw, aw;
+  /* :185-202 row sums and :204-221 col sums use the primal weights */
+  avg_weights(S->Sp, weight, &nw, &aw);
+  avg_vec(S->ra, S->r, S->m, nw, aw);
+  avg_vec(S->ca, S->c, S->n, nw, aw);
+  /* :223-241 gradient uses the dual-target weights */
+  avg_weights(S->St, weight, &nw, &aw);
+  avg_mat(S, S->Ga, S->G, nw, aw);
+  /* :115-135 primal */
+  avg_weights(S->Sp, weight, &nw, &aw);
+  avg_mat(S, S->Xa, S->X, nw, aw);
+  S->pcount += 1;
+  S->Sp += weight;
+  /* :140-160, :162-182 duals */
+  avg_weights(S->Ss, weight, &nw, &aw);
+  avg_vec(S->ua, S->u, S->m, nw, aw);
+  S->scount += 1;
+  S->Ss += weight;
+  avg_weights(S->St, weight, &nw, &aw);
+  avg_vec(S->va, S->v, S->n, nw, aw);
+  S->tcount += 1;
+  S->St += weight;
+}
+/* :93-110 */
+static void reset_solution_weighted_average(ostate* S) {
+  const i64 N = S->m * S->n;
+  memset(S->Xa, 0, sizeof(double) * N);
+  memset(S->Ga, 0, sizeof(double) * N);
+  memset(S->ua, 0, sizeof(double) * S->m);
+  memset(S->ra, 0, sizeof(double) * S->m);
+  memset(S->va, 0, sizeof(double) * S->n);
+  memset(S->ca, 0, sizeof(double) * S->n);
+  S->pcount = S->scount = S->tcount = 0;
+  S->Sp = S->Ss = S->St = 0.0;
+}
+
+/* ---- src/solver_gpu.jl:237-264  update_solution_in_solver_state! ------ */
+static void update_solution_in_solver_state(ostate* S) {
+  const i64 m = S->m, n = S->n;
+#pragma omp parallel for schedule(static)
+  for (i64 e = 0; e < m * n; ++e) S->X[e] = S->X[e] + S->dX[e]; /* :242 */
+  memcpy(S->u, S->nu, sizeof(double) * m);
+  memcpy(S->v, S->nv, sizeof(double) * n);
+  memcpy(S->r, S->nr, sizeof(double) * m);
+  memcpy(S->c, S->nc, sizeof(double) * n);
+#pragma omp parallel for schedule(static)
+  for (i64 j = 0; j < n; ++j) {
+    const double* C = S->C + j * m;
+    double* G = S->G + j * m;
+    const double vj = S->v[j];
+    for (i64 i = 0; i < m; ++i) {
+      double g = C[i] - S->u[i]; /* :249 */
+      G[i] = g - vj;             /* :250 */
+    }
+  }
+  add_to_solution_weighted_average(S, S->step_size); /* :252-263 */
+}
+
+/* ---- src/solver_gpu.jl:267-288  compute_interaction_and_movement ------ */
+static void interaction_and_movement(ostate* S, double* interaction, double* movement) {
+  const i64 m = S->m, n = S->n;
+  for (i64 i = 0; i < m; ++i) S->dr[i] = S->nr[i] - S->r[i];
+  for (i64 j = 0; j < n; ++j) S->dc[j] = S->nc[j] - S->c[j];
+  for (i64 i = 0; i < m; ++i) S->du[i] = S->nu[i] - S->u[i];
+  for (i64 j = 0; j < n; ++j) S->dv[j] = S->nv[j] - S->v[j];
+  double pdi = vec_dot(S->dr, S->du, m);
+  pdi += vec_dot(S->dc, S->dv, n);
+  *interaction = fabs(pdi);
+  double ndp = mat_nrm2(&S->R, S->dX);
+  double ndd = cat_nrm2(S->du, m, S->dv, n);
+  *movement = (0.5 * S->primal_weight) * (ndp * ndp) + (0.5 / S->primal_weight) * (ndd * ndd);
+}
+
+/* ---- src/solver_gpu.jl:290-367  take_step! (adaptive) ---------------- */
+static void take_step_adaptive(ostate* S, double reduction_exponent, double growth_exponent) {
+  double step_size = S->step_size;
+  int done = 0;
+  while (!done) {
+    S->total_iters += 1;
+    next_primal(S, S->step_size, S->primal_weight);
+    next_dual(S, S->step_size, S->primal_weight);
+    double interaction, movement;
+    interaction_and_movement(S, &interaction, &movement);
+    S->kkt_passes += 1;
+    double limit;
+    if (interaction > 0) {
+      limit = movement / interaction;
+      if (movement == 0.0) {
+        S->numerical_error = 1;
+        break;
+      }
+    } else {
+      limit = INFINITY;
+    }
+    if (step_size <= limit) {
+      update_solution_in_solver_state(S);
+      done = 1;
+    }
+    double k1 = (double)(S->total_iters + 1);
+    double first_term = (1.0 - 1.0 / pow(k1, reduction_exponent)) * limit;
+    double second_term = (1.0 + 1.0 / pow(k1, growth_exponent)) * step_size;
+    step_size = jl_min(first_term, second_term);
+    /* The reference loops forever when the limit is NaN (no step can pass
+     * `step_size <= NaN`); stop with a numerical error instead. */
+    if (!done && step_size != step_size) {
+      S->numerical_error = 1;
+      break;
+    }
+  }
+  S->step_size = step_size;
+}
+
+/* ---- src/solver_gpu.jl:370-410  take_step! (constant) ---------------- */
+static void take_step_constant(ostate* S) {
+  next_primal(S, S->step_size, S->primal_weight);
+  next_dual(S, S->step_size, S->primal_weight);
+  S->kkt_passes += 1;
+  update_solution_in_solver_state(S);
+}
+
+/* ---- src/utils_gpu.jl:68-129  compute_convergence_information -------- */
+static void convergence_information(ostate* S, const double* X, const double* u, const double* v,
+                                    const double* r, const double* c, const double* G,
+                                    double eps_ratio, pdot_convergence_information* ci) {
+  const i64 m = S->m, n = S->n;
+  memset(ci, 0, sizeof(*ci));
+  double pobj = mat_dot(&S->R, S->C, X); /* :84 */
+  for (i64 i = 0; i < m; ++i) S->viol_s[i] = S->a[i] - r[i]; /* :26 */
+  for (i64 j = 0; j < n; ++j) S->viol_t[j] = S->b[j] - c[j]; /* :27 */
+  ci->primal_objective = pobj;
+  ci->l_inf_primal_residual = cat_nrminf(S->viol_s, m, S->viol_t, n);
+  ci->l2_primal_residual = cat_nrm2(S->viol_s, m, S->viol_t, n);
+  ci->relative_l_inf_primal_residual = ci->l_inf_primal_residual / (eps_ratio + S->linf_rhs);
+  ci->relative_l2_primal_residual = ci->l2_primal_residual / (eps_ratio + S->l2_rhs);
+  ci->l_inf_primal_variable = mat_nrminf(&S->R, X);
+  ci->l2_primal_variable = mat_nrm2(&S->R, X);
+  /* :45-55 compute_dual_stats!: reduced costs min.(G, 0) */
+  {
+    const i64 N = m * n;
+    double* rc = S->dX; /* the reference aliases buffer_primal here (solver_gpu.jl:467) */
+#pragma omp parallel for schedule(static)
+    for (i64 e = 0; e < N; ++e) rc[e] = jl_min0(G[e]);
+    double dres_inf = mat_nrminf(&S->R, rc);
+    double dobj = vec_dot(S->a, u, m) + vec_dot(S->b, v, n); /* :54 */
+    ci->dual_objective = dobj;
+    ci->l_inf_dual_residual = dres_inf;
+    ci->l2_dual_residual = mat_nrm2(&S->R, rc); /* :108 */
+    ci->corrected_dual_objective = dres_inf == 0.0 ? dobj : -INFINITY; /* :57-63 */
+  }
+  ci->relative_l_inf_dual_residual = ci->l_inf_dual_residual / (eps_ratio + S->linf_obj);
+  ci->relative_l2_dual_residual = ci->l2_dual_residual / (eps_ratio + S->l2_obj);
+  /* :115-116 use the source duals twice */
+  ci->l_inf_dual_variable = cat_nrminf(u, m, u, m);
+  ci->l2_dual_variable = cat_nrm2(u, m, u, m);
+  double gap = fabs(ci->primal_objective - ci->dual_objective);
+  double abs_obj = fabs(ci->primal_objective) + fabs(ci->dual_objective);
+  ci->relative_optimality_gap = gap / (eps_ratio + abs_obj);
+  ci->candidate_type = PDOT_POINT_TYPE_AVERAGE_ITERATE;
+  (void)v;
+}
+
+/* ---- src/saddle_point_gpu.jl:299-330  compute_weight_kkt_residual ---- */
+static double weight_kkt_residual(ostate* S, const double* X, const double* u, const double* v,
+                                  const double* r, const double* c, const double* G,
+                                  double primal_weight) {
+  const i64 m = S->m, n = S->n;
+  double pobj = mat_dot(&S->R, S->C, X);
+  for (i64 i = 0; i < m; ++i) S->viol_s[i] = S->a[i] - r[i];
+  for (i64 j = 0; j < n; ++j) S->viol_t[j] = S->b[j] - c[j];
+  double l2_pres = cat_nrm2(S->viol_s, m, S->viol_t, n);
+  const i64 N = m * n;
+  double* rc = S->dX;
+#pragma omp parallel for schedule(static)
+  for (i64 e = 0; e < N; ++e) rc[e] = jl_min0(G[e]);
+  double dobj = vec_dot(S->a, u, m) + vec_dot(S->b, v, n);
+  double l2_dres = mat_nrm2(&S->R, rc);
+  double gap = fabs(pobj - dobj);
+  return sqrt(primal_weight * (l2_pres * l2_pres) + (1.0 / primal_weight) * (l2_dres * l2_dres) +
+              gap * gap);
+}
+
+/* ---- src/termination.jl:106-166 -------------------------------------- */
+static int optimality_criteria_met(const pdot_termination_criteria* tc, const ostate* S,
+                                   const pdot_convergence_information* ci) {
+  double abs_obj = fabs(ci->primal_objective) + fabs(ci->dual_objective);
+  double gap = fabs(ci->primal_objective - ci->dual_objective);
+  double perr, pbase, derr, dbase;
+  if (tc->optimality_norm == PDOT_L_INF) {
+    perr = ci->l_inf_primal_residual;
+    pbase = S->linf_rhs;
+    derr = ci->l_inf_dual_residual;
+    dbase = S->linf_obj;
+  } else {
+    perr = ci->l2_primal_residual;
+    pbase = S->l2_rhs;
+    derr = ci->l2_dual_residual;
+    dbase = S->l2_obj;
+  }
+  const double ea = tc->eps_optimal_absolute, er = tc->eps_optimal_relative;
+  return derr < ea + er * dbase && perr < ea + er * pbase && gap < ea + er * abs_obj;
+}
+static int check_termination_criteria(const pdot_termination_criteria* tc, const ostate* S,
+                                      const pdot_iteration_stats* st) {
+  if (optimality_criteria_met(tc, S, &st->convergence_information))
+    return PDOT_TERMINATION_REASON_OPTIMAL;
+  if (st->iteration_number >= tc->iteration_limit) return PDOT_TERMINATION_REASON_ITERATION_LIMIT;
+  if (st->cumulative_kkt_matrix_passes >= tc->kkt_matrix_pass_limit)
+    return PDOT_TERMINATION_REASON_KKT_MATRIX_PASS_LIMIT;
+  if (st->cumulative_time_sec >= tc->time_sec_limit) return PDOT_TERMINATION_REASON_TIME_LIMIT;
+  return 0;
+}
+
+/* ---- src/saddle_point_gpu.jl:733-780  update_last_restart_info! ------ */
+static void update_last_restart_info(ostate* S, double primal_weight, double pnp, double dnp,
+                                     i64 restart_length) {
+  const i64 m = S->m, n = S->n, N = m * n;
+  /* :753-755, with the average already reset to zero (saddle_point_gpu.jl:667) */
+#pragma omp parallel for schedule(static)
+  for (i64 e = 0; e < N; ++e) S->dX[e] = S->Xa[e] - S->Xl[e];
+  for (i64 i = 0; i < m; ++i) S->du[i] = S->ua[i] - S->ul[i];
+  for (i64 j = 0; j < n; ++j) S->dv[j] = S->va[j] - S->vl[j];
+  S->pdist = (sqrt(pnp) * mat_nrm2(&S->R, S->dX)) / sqrt(primal_weight);
+  S->ddist = (sqrt(dnp) * cat_nrm2(S->du, m, S->dv, n)) * sqrt(primal_weight);
+  memcpy(S->Xl, S->X, sizeof(double) * N);
+  memcpy(S->ul, S->u, sizeof(double) * m);
+  memcpy(S->vl, S->v, sizeof(double) * n);
+  S->last_restart_length = restart_length;
+  memcpy(S->rl, S->r, sizeof(double) * m);
+  memcpy(S->cl, S->c, sizeof(double) * n);
+  memcpy(S->Gl, S->G, sizeof(double) * N);
+}
+
+/* ---- src/saddle_point_gpu.jl:539-696  run_restart_scheme ------------- */
+static int run_restart_scheme(ostate* S, const pdot_restart_parameters* rp, i64 iterations_completed,
+                              double pnp, double dnp, double primal_weight) {
+  const i64 m = S->m, n = S->n, N = m * n;
+  if (!(S->pcount > 0 && S->scount > 0 && S->tcount > 0)) return PDOT_RESTART_CHOICE_NO_RESTART;
+  i64 restart_length = S->pcount;
+  int do_restart = 0;
+  if ((double)restart_length >= rp->artificial_restart_threshold * (double)iterations_completed)
+    do_restart = 1;
+  int reset_to_average;
+  double candidate = 0.0;
+  if (rp->restart_scheme == PDOT_NO_RESTARTS) {
+    reset_to_average = 0;
+  } else {
+    double cur = weight_kkt_residual(S, S->X, S->u, S->v, S->r, S->c, S->G, primal_weight);
+    double avg = weight_kkt_residual(S, S->Xa, S->ua, S->va, S->ra, S->ca, S->Ga, primal_weight);
+    /* :477-487 */
+    reset_to_average = rp->restart_to_current_metric == PDOT_KKT_GREEDY ? (cur >= avg) : 1;
+    candidate = reset_to_average ? avg : cur;
+  }
+  if (!do_restart) {
+    if (rp->restart_scheme == PDOT_ADAPTIVE_KKT) {
+      /* :492-533 should_do_adaptive_restart_kkt */
+      double last = weight_kkt_residual(S, S->Xl, S->ul, S->vl, S->rl, S->cl, S->Gl, primal_weight);
+      double ratio = candidate / last;
+      if (ratio < rp->necessary_reduction_for_restart) {
+        if (ratio < rp->sufficient_reduction_for_restart)
+          do_restart = 1;
+        else if (ratio > S->ratio_last_trial)
+          do_restart = 1;
+      }
+      S->ratio_last_trial = ratio;
+    } else if (rp->restart_scheme == PDOT_FIXED_FREQUENCY &&
+               rp->restart_frequency_if_fixed <= restart_length) {
+      do_restart = 1;
+    }
+  }
+  if (!do_restart) return PDOT_RESTART_CHOICE_NO_RESTART;
+  if (reset_to_average) {
+    memcpy(S->X, S->Xa, sizeof(double) * N);
+    memcpy(S->u, S->ua, sizeof(double) * m);
+    memcpy(S->v, S->va, sizeof(double) * n);
+    memcpy(S->r, S->ra, sizeof(double) * m);
+    memcpy(S->c, S->ca, sizeof(double) * n);
+    memcpy(S->G, S->Ga, sizeof(double) * N);
+  }
+  reset_solution_weighted_average(S);
+  update_last_restart_info(S, primal_weight, pnp, dnp, restart_length);
+  return reset_to_average ? PDOT_RESTART_CHOICE_RESTART_TO_AVERAGE
+                          : PDOT_RESTART_CHOICE_WEIGHTED_AVERAGE_RESET;
+}
+
+/* ---- src/saddle_point_gpu.jl:701-728  compute_new_primal_weight ------ */
+static double compute_new_primal_weight(const ostate* S, double primal_weight, double smoothing) {
+  double pd = S->pdist, dd = S->ddist;
+  if (pd > DBL_EPSILON && dd > DBL_EPSILON) {
+    double est = dd / pd;
+    double lp = smoothing * log(est) + (1.0 - smoothing) * log(primal_weight);
+    return exp(lp);
+  }
+  return primal_weight;
+}
+
+/* ---- validation: src/solver_gpu.jl:420-422, src/saddle_point_gpu.jl:455-461 */
+int pdot_oracle_validate(const pdot_problem* P, const pdot_pdhg_parameters* prm) {
+  if (!P || !prm) return PDOT_ERR_INVALID_ARGUMENT;
+  if (P->num_row < 1 || P->num_col < 1 || !P->cost_matrix || !P->source_distribution ||
+      !P->target_distribution)
+    return PDOT_ERR_INVALID_ARGUMENT;
+  if (!(prm->primal_importance > 0) || !isfinite(prm->primal_importance))
+    return PDOT_ERR_INVALID_ARGUMENT;
+  const pdot_restart_parameters* rp = &prm->restart_params;
+  if (!(rp->restart_frequency_if_fixed > 1)) return PDOT_ERR_INVALID_ARGUMENT;
+  if (!(0.0 < rp->artificial_restart_threshold && rp->artificial_restart_threshold <= 1.0))
+    return PDOT_ERR_INVALID_ARGUMENT;
+  if (!(0.0 < rp->sufficient_reduction_for_restart &&
+        rp->sufficient_reduction_for_restart <= rp->necessary_reduction_for_restart &&
+        rp->necessary_reduction_for_restart <= 1.0))
+    return PDOT_ERR_INVALID_ARGUMENT;
+  if (!(0.0 <= rp->primal_weight_update_smoothing && rp->primal_weight_update_smoothing <= 1.0))
+    return PDOT_ERR_INVALID_ARGUMENT;
+  if (prm->termination_evaluation_frequency < 1) return PDOT_ERR_INVALID_ARGUMENT;
+  return PDOT_OK;
+}
+
+static void* zalloc(i64 count) { return calloc((size_t)(count > 0 ? count : 1), sizeof(double)); }
+
+/* ---- src/solver_gpu.jl:413-720  optimize ----------------------------- */
+int pdot_oracle_optimize(const pdot_problem* P, const pdot_pdhg_parameters* prm,
+                         pdot_saddle_point_output* out, int num_threads) {
+  int rc = pdot_oracle_validate(P, prm);
+  if (rc != PDOT_OK) return rc;
+#ifdef _OPENMP
+  if (num_threads > 0) omp_set_num_threads(num_threads);
+#else
+  (void)num_threads;
+#endif
+  ostate St;
+  ostate* S = &St;
+  memset(S, 0, sizeof(*S));
+  const i64 m = P->num_row, n = P->num_col, N = m * n;
+  S->m = m;
+  S->n = n;
+  S->C = P->cost_matrix;
+  S->a = P->source_distribution;
+  S->b = P->target_distribution;
+  S->R.m = m;
+  S->R.n = n;
+  S->R.colbuf = zalloc(n);
+
+  /* cached_ot_info, src/termination.jl:94-101 */
+  S->linf_obj = mat_nrminf(&S->R, S->C);
+  S->linf_rhs = cat_nrminf(S->a, m, S->b, n);
+  S->l2_obj = mat_nrm2(&S->R, S->C);
+  S->l2_rhs = cat_nrm2(S->a, m, S->b, n);
+
+  S->X = zalloc(N); S->G = zalloc(N); S->Xa = zalloc(N); S->Ga = zalloc(N);
+  S->dX = zalloc(N); S->Xl = zalloc(N); S->Gl = zalloc(N);
+  S->u = zalloc(m); S->r = zalloc(m); S->ua = zalloc(m); S->ra = zalloc(m);
+  S->nu = zalloc(m); S->du = zalloc(m); S->dr = zalloc(m); S->nr = zalloc(m);
+  S->ul = zalloc(m); S->rl = zalloc(m); S->viol_s = zalloc(m);
+  S->v = zalloc(n); S->c = zalloc(n); S->va = zalloc(n); S->ca = zalloc(n);
+  S->nv = zalloc(n); S->dv = zalloc(n); S->dc = zalloc(n); S->nc = zalloc(n);
+  S->vl = zalloc(n); S->cl = zalloc(n); S->viol_t = zalloc(n);
+  if (!S->X || !S->G || !S->Xa || !S->Ga || !S->dX || !S->Xl || !S->Gl) {
+    rc = PDOT_ERR_OUT_OF_MEMORY;
+    goto cleanup;
+  }
+
+  const int adaptive = prm->step_size_policy == PDOT_STEP_SIZE_ADAPTIVE;
+  /* :476-482 */
+  S->step_size = adaptive ? 1.0 : (1.0 - 0.2) / sqrt((double)(m + n));
+  const double KKT_PASSES_PER_TERMINATION_EVALUATION = 2.0;
+  /* :486-496, select_initial_primal_weight saddle_point_gpu.jl:848-866 */
+  if (prm->scale_invariant_initial_primal_weight) {
+    double rhs = sqrt(1.0) * cat_nrm2(S->a, m, S->b, n);
+    double obj = sqrt(1.0) * mat_nrm2(&S->R, S->C);
+    S->primal_weight = (obj > 0.0 && rhs > 0.0) ? prm->primal_importance * (obj / rhs)
+                                                : prm->primal_importance;
+  } else {
+    S->primal_weight = prm->primal_importance;
+  }
+  const double smoothing = prm->restart_params.primal_weight_update_smoothing;
+  const double start_time = now_sec();
+  double basic_time = 0.0;
+  /* create_last_restart_info, saddle_point_gpu.jl:371-393 */
+  S->last_restart_length = 1;
+  S->pdist = 0.0;
+  S->ddist = 0.0;
+  S->ratio_last_trial = 1.0;
+
+  const pdot_termination_criteria* tc = &prm->termination_criteria;
+  const i64 iteration_limit = tc->iteration_limit;
+  const i64 freq = prm->termination_evaluation_frequency;
+  S->numerical_error = 0;
+
+  i64 nstats = 0;
+  i64 iteration = 0;
+  for (;;) {
+    iteration += 1;
+    if ((iteration - 1) % freq == 0 || iteration == iteration_limit + 1 || iteration <= 10 ||
+        S->numerical_error) {
+      S->kkt_passes += KKT_PASSES_PER_TERMINATION_EVALUATION;
+      pdot_iteration_stats st;
+      memset(&st, 0, sizeof(st));
+      st.iteration_number = (int32_t)iteration;
+      st.cumulative_kkt_matrix_passes = S->kkt_passes;
+      st.cumulative_time_sec = now_sec() - start_time;
+      const double eps_ratio = tc->eps_optimal_absolute / tc->eps_optimal_relative;
+      /* :537 (parses as `numerical_error || primal_solutions_count == 0`) */
+      if (S->numerical_error || S->pcount == 0)
+        convergence_information(S, S->X, S->u, S->v, S->r, S->c, S->G, eps_ratio,
+                                &st.convergence_information);
+      else
+        convergence_information(S, S->Xa, S->ua, S->va, S->ra, S->ca, S->Ga, eps_ratio,
+                                &st.convergence_information);
+      st.step_size = S->step_size;
+      st.primal_weight = S->primal_weight;
+      st.restart_used = PDOT_RESTART_CHOICE_UNSPECIFIED;
+      st.time_spent_doing_basic_algorithm = basic_time;
+      /* define_norms, solver_gpu.jl:51-56 */
+      const double pnp = 1.0 / S->step_size * S->primal_weight;
+      const double dnp = 1.0 / S->step_size / S->primal_weight;
+      int term = check_termination_criteria(tc, S, &st);
+      if (S->numerical_error && !term) term = PDOT_TERMINATION_REASON_NUMERICAL_ERROR;
+      const int record = prm->record_iteration_stats || term;
+      if (term) {
+        if (record) {
+          if (out->iteration_stats && nstats < out->iteration_stats_capacity)
+            out->iteration_stats[nstats] = st;
+          nstats++;
+        }
+        const int cur = (S->pcount == 0 || S->scount == 0 || S->tcount == 0);
+        if (out->primal_solution) memcpy(out->primal_solution, cur ? S->X : S->Xa, sizeof(double) * N);
+        if (out->dual_source_solution)
+          memcpy(out->dual_source_solution, cur ? S->u : S->ua, sizeof(double) * m);
+        if (out->dual_target_solution)
+          memcpy(out->dual_target_solution, cur ? S->v : S->va, sizeof(double) * n);
+        out->termination_reason = term;
+        out->iteration_count = (int32_t)(iteration - 1);
+        out->iteration_stats_count = nstats;
+        out->solve_time_sec = st.cumulative_time_sec;
+        out->final_stats = st;
+        break;
+      }
+      st.restart_used =
+          run_restart_scheme(S, &prm->restart_params, iteration - 1, pnp, dnp, S->primal_weight);
+      if (st.restart_used != PDOT_RESTART_CHOICE_NO_RESTART)
+        S->primal_weight = compute_new_primal_weight(S, S->primal_weight, smoothing);
+      if (record) {
+        if (out->iteration_stats && nstats < out->iteration_stats_capacity)
+          out->iteration_stats[nstats] = st;
+        nstats++;
+      }
+    }
+    double t0 = now_sec();
+    if (adaptive)
+      take_step_adaptive(S, prm->reduction_exponent, prm->growth_exponent);
+    else
+      take_step_constant(S);
+    basic_time += now_sec() - t0;
+  }
+  rc = PDOT_OK;
+
+cleanup:
+  free(S->R.colbuf);
+  free(S->X); free(S->G); free(S->Xa); free(S->Ga); free(S->dX); free(S->Xl); free(S->Gl);
+  free(S->u); free(S->r); free(S->ua); free(S->ra); free(S->nu); free(S->du); free(S->dr);
+  free(S->nr); free(S->ul); free(S->rl); free(S->viol_s);
+  free(S->v); free(S->c); free(S->va); free(S->ca); free(S->nv); free(S->dv); free(S->dc);
+  free(S->nc); free(S->vl); free(S->cl); free(S->viol_t);
+  return rc;
+}
+
+/*
+ * One primal pass with the semantics of pdot_primal_pass_f64 (include/pdot.h),
+ * composed from src/solver_gpu.jl:139-141 (projected step), :172-173 (delta
+ * sums), :242 (X += delta), :249-250 (gradient from C, u, v) and
+ * src/saddle_point_gpu.jl:129-130 (primal average). Used by the kernel-level
+ * parity tests.
+ */
+void pdot_oracle_primal_pass(i64 m, i64 n, const double* C, double* X, double* Xa,
+                             const double* u, const double* v, double step_over_weight,
+                             double avg_new_weight, double avg_scale, int32_t flags,
+                             double* drow, double* dcol, double* dsq) {
+  const int zero_g = (flags & PDOT_PASS_ZERO_GRADIENT) != 0;
+  const int first = (flags & PDOT_PASS_FIRST_AVERAGE) != 0;
+  double* d = (double*)zalloc(m * n);
+  double* colsq = (double*)zalloc(n);
+#pragma omp parallel for schedule(static)
+  for (i64 j = 0; j < n; ++j) {
+    double cs = 0.0, sq = 0.0;
+    for (i64 i = 0; i < m; ++i) {
+      const i64 e = i + j * m;
+      double g = zero_g ? 0.0 : (C[e] - u[i]) - v[j];
+      double t = X[e] - step_over_weight * g;
+      t = jl_max0(t);
+      t -= X[e];
+      d[e] = t;
+      double xn = X[e] + t;
+      X[e] = xn;
+      Xa[e] = first ? xn : (Xa[e] + xn * avg_new_weight) * avg_scale;
+      cs += t;
+      sq += t * t;
+    }
+    dcol[j] = cs;
+    colsq[j] = sq;
+  }
+  for (i64 i = 0; i < m; ++i) drow[i] = 0.0;
+  for (i64 j = 0; j < n; ++j)
+    for (i64 i = 0; i < m; ++i) drow[i] += d[i + j * m];
+  double s = 0.0;
+  for (i64 j = 0; j < n; ++j) s += colsq[j];
+  *dsq = s;
+  free(colsq);
+  free(d);
+}
+
+int pdot_oracle_version(void) { return PDOT_ABI_VERSION; }

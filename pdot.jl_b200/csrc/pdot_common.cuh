@@ -1,0 +1,153 @@
+// pdot_common.cuh — shared declarations of the sm_100a PDHG-for-OT solver.
+//
+// Data layout in HBM (one solve):
+//   C          m x n FP64, column-major (entry (i,j) at i + j*m), read-only
+//   X[2]       two m x n FP64 plans: X[buf] is the current iterate, X[1-buf]
+//              the running weighted average. A restart to the average flips
+//              `buf`, so restarts copy nothing.
+//   u[2] v[2]  source/target duals (current / average), FP64
+//   r[2] c[2]  row / column sums of the plan (current / average), FP64
+//   partials   per-CTA and per-(panel, column) partial sums; reductions are
+//              two-stage with a fixed order, so results are bitwise repeatable.
+//
+// Work decomposition of the matrix passes: the rows are cut into panels of
+// kPanelRows; a "unit" is one column of one panel (kPanelRows contiguous
+// doubles). Units are numbered panel-major (q = p*n + j) and CTA c owns the
+// contiguous range [c*U/G, (c+1)*U/G): every CTA streams the same number of
+// bytes. A warp handles a whole unit, so a column's partial sum is a warp
+// shuffle; row sums accumulate per lane across the units of a panel and are
+// combined across warps in shared memory when the panel ends.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pdot.h"
+
+namespace pdot {
+
+constexpr int kThreads = 256;              // CTA size of the matrix passes
+constexpr int kWarps = kThreads / 32;
+constexpr int kPanelRows = 256;            // rows per panel (one unit = 256 doubles)
+constexpr int kVecThreads = 256;           // CTA size of the vector passes
+constexpr int kEvalSums = 10;              // per-CTA partials of the eval matrix pass
+constexpr int kVecSums = 10;               // per-CTA partials of the eval vector pass
+constexpr int kStepSums = 2;               // per-CTA partials of the dual step
+constexpr int kNormSums = 2;               // per-CTA partials of the cost-norm pass
+
+struct Geometry {
+  int64_t m, n;
+  int64_t panels;      // P = ceil(m / kPanelRows)
+  int64_t units;       // U = P * n
+  int32_t grid;        // CTAs of the matrix passes (<= U)
+  int32_t vec;         // 2: 16-byte loads (m even), 1: scalar loads
+  int32_t row_blocks;  // CTAs of the vector passes covering m
+  int32_t col_blocks;  // CTAs of the vector passes covering n
+};
+
+__host__ __device__ __forceinline__ int64_t unit_begin(const Geometry& g, int64_t cta) {
+  return cta * g.units / g.grid;
+}
+// The CTA whose unit range holds unit q (the largest c with unit_begin(c) <= q).
+__host__ __device__ __forceinline__ int64_t cta_of_unit(const Geometry& g, int64_t q) {
+  return ((q + 1) * (int64_t)g.grid - 1) / g.units;
+}
+// Row partials of CTA c for panel p live in slot c + p: along the unit line,
+// both c and p are non-decreasing and one of them grows at every boundary, so
+// the slot is unique. There are at most grid + panels slots.
+__host__ __device__ __forceinline__ int64_t row_slot(int64_t cta, int64_t panel) { return cta + panel; }
+
+// Solver state in device memory. Every per-iteration decision is taken on the
+// device, so the host only reads this record between replayed chunks.
+struct DevState {
+  double step_size;          // solver_state.step_size (tau)
+  double primal_weight;      // solver_state.primal_weight (omega)
+  double kkt_passes;         // solver_state.cumulative_kkt_passes
+  double sum_weights;        // sum of averaging weights (all averages share it)
+  long long avg_count;       // primal_solutions_count
+  long long total_iters;     // solver_state.total_number_iterations
+  long long iteration;       // number of the next loop body of optimize()
+  // last restart point (saddle_point_gpu.jl:332-366 reduced to scalars)
+  double last_rp;            // its l2 primal residual
+  double last_rd;            // its l2 dual residual
+  double last_gap;           // |primal obj - dual obj|
+  double last_xnorm;         // ||X_last||_2
+  double last_ynorm;         // ||[u_last; v_last]||_2
+  double ratio_last_trial;   // kkt_reduction_ratio_last_trial
+  long long last_restart_length;
+  double pdist, ddist;       // distances moved in the last restart period
+  // cached_ot_info, termination.jl:87-92
+  double linf_obj, linf_rhs, l2_obj, l2_rhs;
+  // timing (globaltimer ns)
+  unsigned long long t_start_ns;
+  unsigned long long eval_t0_ns;
+  double eval_time_sec;      // device time spent in evaluations
+  long long num_stats;       // iteration-stats records written
+  int numerical_error;
+  int g_is_zero;             // the stored gradient is still its initial 0
+  int done;
+  int termination_reason;
+  int buf;                   // which half of each pair is the current iterate
+  int out_current;           // at termination: 1 = return current, 0 = average
+  int last_restart_choice;
+  unsigned int ticket_step;  // last-CTA tickets
+  unsigned int ticket_eval;
+  unsigned int ticket_init;
+  int pad_[2];
+};
+
+// Parameters of one solve, passed by value to the control kernels.
+struct SolveConfig {
+  int adaptive;
+  double reduction_exponent, growth_exponent;
+  int restart_scheme, restart_to_current_metric;
+  long long restart_frequency_if_fixed;
+  double artificial_restart_threshold;
+  double sufficient_reduction_for_restart;
+  double necessary_reduction_for_restart;
+  double primal_weight_update_smoothing;
+  int optimality_norm;
+  double eps_abs, eps_rel, time_sec_limit;
+  long long iteration_limit;
+  double kkt_matrix_pass_limit;
+  int record_iteration_stats;
+  int scale_invariant_initial_primal_weight;
+  double primal_importance;
+};
+
+struct Buffers {
+  const double* C;
+  const double* a;
+  const double* b;
+  double* X[2];
+  double* u[2];
+  double* v[2];
+  double* r[2];
+  double* c[2];
+  double* rowpart;   // (grid + panels) * kPanelRows
+  double* colpart;   // panels * n
+  double* sqpart;    // grid
+  double* steppart;  // (row_blocks + col_blocks) * kStepSums
+  double* evpart;    // grid * kEvalSums
+  double* vecpart;   // (row_blocks + col_blocks) * kVecSums
+  pdot_iteration_stats* ring;
+  int ring_cap;
+  DevState* st;
+};
+
+// ---- launchers (pdot_kernels.cu) ----------------------------------------
+Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device);
+size_t workspace_doubles(const Geometry& g);
+
+cudaError_t launch_init(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
+cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
+cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
+
+// Stand-alone primal pass on caller buffers (pdot_primal_pass_f64).
+cudaError_t launch_primal_pass(const Geometry& g, const double* C, double* X, double* Xa,
+                               const double* u, const double* v, double step_over_weight,
+                               double avg_new_weight, double avg_scale, int flags,
+                               double* drow, double* dcol, double* dsq, double* work,
+                               cudaStream_t s);
+
+}  // namespace pdot

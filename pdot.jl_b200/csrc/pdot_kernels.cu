@@ -1,0 +1,935 @@
+// pdot_kernels.cu — sm_100a kernels of the FP64 PDHG-for-OT drop-in.
+//
+// Per PDHG iteration two launches run (both captured in a CUDA graph):
+//   k1_primal  the fused matrix pass: reads C, X, Xavg once, writes X, Xavg,
+//              emits per-(panel, column) column sums of the step, per-(CTA,
+//              panel) row sums and per-CTA sum of squares. 40 B/entry in FP64.
+//   k2_dual    finishes the two-stage sums in a fixed order, takes the dual
+//              step and the vector averages, and its last CTA runs the
+//              adaptive step-size rule (accept / retry bookkeeping).
+// Every evaluation (iterations 1..10, then every termination_evaluation_
+// frequency iterations) adds two more:
+//   k3_eval    matrix reductions for the KKT statistics of the current and
+//              average points (24 B/entry)
+//   k4_eval    vector reductions; its last CTA computes the statistics, checks
+//              termination, runs the restart scheme and the primal-weight
+//              update, and writes one iteration-stats record.
+//
+// Elementwise arithmetic uses explicit round-to-nearest intrinsics in the
+// reference's operation order (no fused multiply-add), so the projected step,
+// the plan update and the averages round exactly as the reference's Julia code
+// does; only the order of the sums differs.
+#include <cfloat>
+#include <cmath>
+
+#include "pdot_common.cuh"
+
+namespace pdot {
+namespace {
+
+__device__ __forceinline__ double nanmax(double a, double b) { return (b > a || b != b) ? b : a; }
+
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Base.max(x, 0.0): NaN propagates, -0.0 becomes 0.0.
+__device__ __forceinline__ double jl_max0(double x) { return x > 0.0 ? x : (x != x ? x : 0.0); }
+// |min(x, 0.0)| with NaN propagating.
+__device__ __forceinline__ double neg_part(double x) { return x < 0.0 ? -x : (x != x ? x : 0.0); }
+// Base.min(x, y) for Float64.
+__device__ __forceinline__ double jl_min(double x, double y) {
+  if (x != x) return x;
+  if (y != y) return y;
+  return y < x ? y : x;
+}
+// x^y for the step-size rule; integral exponents 1 and 2 are exact as in Julia.
+__device__ __forceinline__ double powd(double x, double y) {
+  if (y == 1.0) return x;
+  if (y == 2.0) return x * x;
+  return pow(x, y);
+}
+
+// Deterministic block reduction of K values (bit k of maxmask: max, else sum),
+// result written by thread 0 to out[0..K). Blocks have 256 threads.
+template <int K>
+__device__ __forceinline__ void block_reduce(double (&vals)[K], unsigned maxmask, double* out) {
+  __shared__ double sh[kWarps][K];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    double x = vals[k];
+    const bool mx = (maxmask >> k) & 1u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double y = __shfl_xor_sync(0xffffffffu, x, o);
+      x = mx ? nanmax(x, y) : x + y;
+    }
+    if (lane == 0) sh[warp][k] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const bool mx = (maxmask >> k) & 1u;
+      double acc = sh[0][k];
+      for (int w = 1; w < kWarps; ++w) acc = mx ? nanmax(acc, sh[w][k]) : acc + sh[w][k];
+      out[k] = acc;
+    }
+  }
+  __syncthreads();
+}
+
+// One warp reduces `count` records of K partials in a fixed order; lane 0 holds
+// the result. Reads go through L2 (the partials were written by other CTAs).
+template <int K>
+__device__ __forceinline__ void warp_reduce_partials(const double* part, int64_t first, int64_t count,
+                                                     unsigned maxmask, double (&out)[K]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const bool mx = (maxmask >> k) & 1u;
+    double acc = 0.0;
+    for (int64_t c = lane; c < count; c += 32) {
+      const double v = __ldcg(part + (first + c) * K + k);
+      acc = mx ? nanmax(acc, v) : acc + v;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double y = __shfl_xor_sync(0xffffffffu, acc, o);
+      acc = mx ? nanmax(acc, y) : acc + y;
+    }
+    out[k] = acc;
+  }
+}
+
+// Last-CTA election for a grid-wide finish step.
+__device__ __forceinline__ bool elect_last_cta(unsigned int* ticket) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+template <int VEC>
+struct VecIO;
+template <>
+struct VecIO<1> {
+  static __device__ __forceinline__ void ld(const double* p, double (&v)[1]) { v[0] = *p; }
+  static __device__ __forceinline__ void ldg(const double* p, double (&v)[1]) { v[0] = __ldg(p); }
+  static __device__ __forceinline__ void st(double* p, const double (&v)[1]) { *p = v[0]; }
+};
+template <>
+struct VecIO<2> {
+  static __device__ __forceinline__ void ld(const double* p, double (&v)[2]) {
+    const double2 t = *reinterpret_cast<const double2*>(p);
+    v[0] = t.x;
+    v[1] = t.y;
+  }
+  static __device__ __forceinline__ void ldg(const double* p, double (&v)[2]) {
+    const double2 t = __ldg(reinterpret_cast<const double2*>(p));
+    v[0] = t.x;
+    v[1] = t.y;
+  }
+  static __device__ __forceinline__ void st(double* p, const double (&v)[2]) {
+    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// The fused primal pass. Per entry (src/solver_gpu.jl:139-141,242,249-250;
+// src/saddle_point_gpu.jl:129-130):
+//   g  = (C - u_i) - v_j ;  t = max(X - s*g, 0) ;  d = t - X ;  X' = X + d
+//   Xavg' = (Xavg + X'*nw)*aw      (Xavg' = X' after a reset of the average)
+template <int VEC>
+__device__ __forceinline__ void primal_pass_body(const double* __restrict__ C, double* __restrict__ X,
+                                                 double* __restrict__ Xa, const double* __restrict__ u,
+                                                 const double* __restrict__ v, const double s,
+                                                 const double nw, const double aw, const bool zero_g,
+                                                 const bool first, double* __restrict__ colpart,
+                                                 double* __restrict__ rowpart, double* __restrict__ sqpart,
+                                                 const Geometry g) {
+  constexpr int RPL = kPanelRows / (32 * VEC);
+  __shared__ double red[kWarps][kPanelRows];
+  __shared__ double sqw[kWarps];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t m = g.m, n = g.n;
+  const int64_t cta = blockIdx.x;
+  const int64_t q0 = unit_begin(g, cta), q1 = unit_begin(g, cta + 1);
+  double sq = 0.0;
+  for (int64_t p = q0 / n; p * n < q1; ++p) {
+    const int64_t jb = (q0 > p * n ? q0 : p * n) - p * n;
+    const int64_t je = (q1 < (p + 1) * n ? q1 : (p + 1) * n) - p * n;
+    const int64_t row0 = p * kPanelRows;
+    double acc[RPL][VEC];
+    double ur[RPL][VEC];
+    bool ok[RPL];
+#pragma unroll
+    for (int k = 0; k < RPL; ++k) {
+      const int64_t i = row0 + k * 32 * VEC + lane * VEC;
+      ok[k] = i < m;
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) {
+        acc[k][e] = 0.0;
+        ur[k][e] = (ok[k] && !zero_g) ? __ldg(u + i + e) : 0.0;
+      }
+    }
+    for (int64_t j = jb + warp; j < je; j += kWarps) {
+      const double vj = zero_g ? 0.0 : __ldg(v + j);
+      const int64_t base = j * m + row0 + lane * VEC;
+      double cv[RPL][VEC], xv[RPL][VEC], av[RPL][VEC];
+#pragma unroll
+      for (int k = 0; k < RPL; ++k) {
+        if (ok[k]) {
+          const int64_t idx = base + k * 32 * VEC;
+          VecIO<VEC>::ldg(C + idx, cv[k]);
+          VecIO<VEC>::ld(X + idx, xv[k]);
+          if (!first) VecIO<VEC>::ld(Xa + idx, av[k]);
+        }
+      }
+      double cs = 0.0;
+#pragma unroll
+      for (int k = 0; k < RPL; ++k) {
+        if (ok[k]) {
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) {
+            const double gg = zero_g ? 0.0 : __dsub_rn(__dsub_rn(cv[k][e], ur[k][e]), vj);
+            const double t = jl_max0(__dsub_rn(xv[k][e], __dmul_rn(s, gg)));
+            const double d = __dsub_rn(t, xv[k][e]);
+            const double xn = __dadd_rn(xv[k][e], d);
+            xv[k][e] = xn;
+            av[k][e] = first ? xn : __dmul_rn(__dadd_rn(av[k][e], __dmul_rn(xn, nw)), aw);
+            acc[k][e] += d;
+            cs += d;
+            sq += d * d;
+          }
+          const int64_t idx = base + k * 32 * VEC;
+          VecIO<VEC>::st(X + idx, xv[k]);
+          VecIO<VEC>::st(Xa + idx, av[k]);
+        }
+      }
+      cs = warp_sum(cs);
+      if (lane == 0) colpart[p * n + j] = cs;
+    }
+    // this panel's row sums: combine the warps in a fixed order
+#pragma unroll
+    for (int k = 0; k < RPL; ++k)
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) red[warp][k * 32 * VEC + lane * VEC + e] = acc[k][e];
+    __syncthreads();
+    for (int t = threadIdx.x; t < kPanelRows; t += kThreads) {
+      double s2 = red[0][t];
+#pragma unroll
+      for (int w = 1; w < kWarps; ++w) s2 += red[w][t];
+      rowpart[row_slot(cta, p) * kPanelRows + t] = s2;
+    }
+    __syncthreads();
+  }
+  sq = warp_sum(sq);
+  if (lane == 0) sqw[warp] = sq;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s2 = sqw[0];
+#pragma unroll
+    for (int w = 1; w < kWarps; ++w) s2 += sqw[w];
+    sqpart[cta] = s2;
+  }
+}
+
+template <int VEC>
+__global__ void __launch_bounds__(kThreads, 2) k1_primal(Buffers B, Geometry g) {
+  const DevState* st = B.st;
+  if (st->done | st->numerical_error) return;
+  const int buf = st->buf;
+  const double tau = st->step_size, omega = st->primal_weight, S = st->sum_weights;
+  const bool zero_g = st->g_is_zero != 0;
+  const bool first = !(S > 0.0);
+  // compute_next_primal_solution! uses solver_state.step_size; the averaging
+  // weight is the same solver_state.step_size (src/solver_gpu.jl:252).
+  const double s = __ddiv_rn(tau, omega);
+  const double nw = first ? 1.0 : __ddiv_rn(tau, S);
+  const double aw = first ? 1.0 : __ddiv_rn(S, __dadd_rn(S, tau));
+  primal_pass_body<VEC>(B.C, B.X[buf], B.X[buf ^ 1], B.u[buf], B.v[buf], s, nw, aw, zero_g, first,
+                        B.colpart, B.rowpart, B.sqpart, g);
+}
+
+template <int VEC>
+__global__ void __launch_bounds__(kThreads, 2)
+    k1_primal_args(const double* C, double* X, double* Xa, const double* u, const double* v, double s,
+                   double nw, double aw, int flags, double* colpart, double* rowpart, double* sqpart,
+                   Geometry g) {
+  primal_pass_body<VEC>(C, X, Xa, u, v, s, nw, aw, (flags & PDOT_PASS_ZERO_GRADIENT) != 0,
+                        (flags & PDOT_PASS_FIRST_AVERAGE) != 0, colpart, rowpart, sqpart, g);
+}
+
+// Second stage of the row sum of row i / column sum of column j.
+__device__ __forceinline__ double finish_row_sum(const Geometry& g, const double* rowpart, int64_t i) {
+  const int64_t p = i / kPanelRows, t = i - p * kPanelRows;
+  const int64_t lo = cta_of_unit(g, p * g.n), hi = cta_of_unit(g, (p + 1) * g.n - 1);
+  double s = 0.0;
+  for (int64_t c = lo; c <= hi; ++c) s += rowpart[row_slot(c, p) * kPanelRows + t];
+  return s;
+}
+__device__ __forceinline__ double finish_col_sum(const Geometry& g, const double* colpart, int64_t j) {
+  double s = 0.0;
+  for (int64_t p = 0; p < g.panels; ++p) s += colpart[p * g.n + j];
+  return s;
+}
+
+// Stand-alone stage two for pdot_primal_pass_f64: delta row/column sums and
+// the sum of squares (one extra CTA).
+__global__ void __launch_bounds__(kVecThreads) k_pass_sums(Geometry g, const double* rowpart,
+                                                           const double* colpart, const double* sqpart,
+                                                           double* drow, double* dcol, double* dsq) {
+  const int bid = blockIdx.x;
+  if (bid < g.row_blocks) {
+    const int64_t i = (int64_t)bid * kVecThreads + threadIdx.x;
+    if (i < g.m) drow[i] = finish_row_sum(g, rowpart, i);
+  } else if (bid < g.row_blocks + g.col_blocks) {
+    const int64_t j = (int64_t)(bid - g.row_blocks) * kVecThreads + threadIdx.x;
+    if (j < g.n) dcol[j] = finish_col_sum(g, colpart, j);
+  } else if (threadIdx.x < 32) {
+    double out[1];
+    warp_reduce_partials<1>(sqpart, 0, g.grid, 0u, out);
+    if (threadIdx.x == 0) *dsq = out[0];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Adaptive step-size rule and the state update on acceptance,
+// src/solver_gpu.jl:290-367 (take_step!) and :370-410 (constant step).
+// The retried candidate of a rejected attempt is identical to the first one
+// (the kernels use solver_state.step_size, not the shrunk local step), so the
+// candidate computed once is the accepted one; a rejection only adds an
+// attempt to the counters and one more application of the shrink rule.
+__device__ void step_control(DevState* st, const SolveConfig& cfg, double dot_r, double dot_c, double dx2,
+                             double dy2) {
+  const double omega = st->primal_weight;
+  const double weight = st->step_size;
+  bool accepted = true;
+  if (cfg.adaptive) {
+    const double interaction = fabs(dot_r + dot_c);
+    const double ndp = sqrt(dx2), ndd = sqrt(dy2);
+    const double movement = __dadd_rn(__dmul_rn(__dmul_rn(0.5, omega), __dmul_rn(ndp, ndp)),
+                                      __dmul_rn(__ddiv_rn(0.5, omega), __dmul_rn(ndd, ndd)));
+    double tau = st->step_size;
+    accepted = false;
+    for (int attempt = 0; attempt < 64; ++attempt) {
+      st->total_iters += 1;
+      st->kkt_passes += 1.0;
+      double limit;
+      if (interaction > 0.0) {
+        limit = __ddiv_rn(movement, interaction);
+        if (movement == 0.0) {
+          st->numerical_error = 1;
+          break;
+        }
+      } else {
+        limit = INFINITY;
+      }
+      if (tau <= limit) accepted = true;
+      const double k1 = (double)(st->total_iters + 1);
+      const double first_term = __dmul_rn(__dsub_rn(1.0, __ddiv_rn(1.0, powd(k1, cfg.reduction_exponent))), limit);
+      const double second_term = __dmul_rn(__dadd_rn(1.0, __ddiv_rn(1.0, powd(k1, cfg.growth_exponent))), tau);
+      tau = jl_min(first_term, second_term);
+      if (accepted) break;
+      // the reference loops forever on a NaN limit; stop with a numerical error
+      if (tau != tau) {
+        st->numerical_error = 1;
+        break;
+      }
+    }
+    if (!accepted) st->numerical_error = 1;
+    st->step_size = tau;
+  } else {
+    st->kkt_passes += 1.0;
+  }
+  if (accepted) {
+    st->sum_weights = st->sum_weights + weight;
+    st->avg_count += 1;
+    st->g_is_zero = 0;
+  }
+  st->iteration += 1;
+}
+
+struct DualArgs {
+  double tw, nw, aw;
+  bool first;
+};
+
+// Dual step of one entry, src/solver_gpu.jl:172-173,191,272-279 and the
+// vector averages src/saddle_point_gpu.jl:140-221.
+__device__ __forceinline__ void dual_entry(double sum_delta, double dist, double* r, double* u, double* ravg,
+                                           double* uavg, const DualArgs& A, double& dot, double& dy2) {
+  const double rr = *r;
+  const double rn = __dadd_rn(sum_delta, rr);
+  const double dr = __dsub_rn(rn, rr);
+  const double uu = *u;
+  const double un = __dadd_rn(uu, __dmul_rn(A.tw, __dadd_rn(__dsub_rn(dist, __dmul_rn(2.0, rn)), rr)));
+  const double du = __dsub_rn(un, uu);
+  dot += dr * du;
+  dy2 += du * du;
+  *r = rn;
+  *u = un;
+  *ravg = A.first ? rn : __dmul_rn(__dadd_rn(*ravg, __dmul_rn(rn, A.nw)), A.aw);
+  *uavg = A.first ? un : __dmul_rn(__dadd_rn(*uavg, __dmul_rn(un, A.nw)), A.aw);
+}
+
+__global__ void __launch_bounds__(kVecThreads) k2_dual(Buffers B, Geometry g, SolveConfig cfg) {
+  DevState* st = B.st;
+  if (st->done | st->numerical_error) return;
+  const int buf = st->buf;
+  const double tau = st->step_size, omega = st->primal_weight, S = st->sum_weights;
+  DualArgs A;
+  A.first = !(S > 0.0);
+  A.tw = __dmul_rn(tau, omega);
+  A.nw = A.first ? 1.0 : __ddiv_rn(tau, S);
+  A.aw = A.first ? 1.0 : __ddiv_rn(S, __dadd_rn(S, tau));
+  double vals[kStepSums] = {0.0, 0.0};
+  const int bid = blockIdx.x;
+  if (bid < g.row_blocks) {
+    const int64_t i = (int64_t)bid * kVecThreads + threadIdx.x;
+    if (i < g.m)
+      dual_entry(finish_row_sum(g, B.rowpart, i), B.a[i], B.r[buf] + i, B.u[buf] + i, B.r[buf ^ 1] + i,
+                 B.u[buf ^ 1] + i, A, vals[0], vals[1]);
+  } else {
+    const int64_t j = (int64_t)(bid - g.row_blocks) * kVecThreads + threadIdx.x;
+    if (j < g.n)
+      dual_entry(finish_col_sum(g, B.colpart, j), B.b[j], B.c[buf] + j, B.v[buf] + j, B.c[buf ^ 1] + j,
+                 B.v[buf ^ 1] + j, A, vals[0], vals[1]);
+  }
+  block_reduce<kStepSums>(vals, 0u, B.steppart + (int64_t)bid * kStepSums);
+  if (!elect_last_cta(&st->ticket_step)) return;
+  if (threadIdx.x < 32) {
+    double rs[kStepSums], cs[kStepSums], xs[1];
+    warp_reduce_partials<kStepSums>(B.steppart, 0, g.row_blocks, 0u, rs);
+    warp_reduce_partials<kStepSums>(B.steppart, g.row_blocks, g.col_blocks, 0u, cs);
+    warp_reduce_partials<1>(B.sqpart, 0, g.grid, 0u, xs);
+    if (threadIdx.x == 0) {
+      // interaction = dot(dr, du) + dot(dc, dv); ||[du; dv]||^2
+      step_control(st, cfg, rs[0], cs[0], xs[0], rs[1] + cs[1]);
+      st->ticket_step = 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Evaluation, matrix part: for the current point (X, G = C - u - v^T, or G = 0
+// before the first accepted step) and, when an average exists, the average
+// point, the sums <C,X>, ||X||^2, max|X|, ||min(G,0)||^2, max|min(G,0)|
+// (src/utils_gpu.jl:84,102-103,39,52,108; src/saddle_point_gpu.jl:313,325).
+enum { E_DOT = 0, E_SQX, E_MAXX, E_SQG, E_MAXG, E_AVG = 5 };
+constexpr unsigned kEvalMaxMask = (1u << E_MAXX) | (1u << E_MAXG) | (1u << (E_AVG + E_MAXX)) |
+                                  (1u << (E_AVG + E_MAXG));
+
+template <int VEC>
+__global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
+  DevState* st = B.st;
+  if (st->done) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->eval_t0_ns = globaltimer_ns();
+  constexpr int RPL = kPanelRows / (32 * VEC);
+  const int buf = st->buf;
+  const bool have_avg = st->avg_count > 0;
+  const bool zero_g = st->g_is_zero != 0;
+  const double* __restrict__ C = B.C;
+  const double* __restrict__ X = B.X[buf];
+  const double* __restrict__ Xa = B.X[buf ^ 1];
+  const double* __restrict__ u = B.u[buf];
+  const double* __restrict__ v = B.v[buf];
+  const double* __restrict__ ua = B.u[buf ^ 1];
+  const double* __restrict__ va = B.v[buf ^ 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t m = g.m, n = g.n;
+  const int64_t cta = blockIdx.x;
+  const int64_t q0 = unit_begin(g, cta), q1 = unit_begin(g, cta + 1);
+  double acc[kEvalSums];
+#pragma unroll
+  for (int k = 0; k < kEvalSums; ++k) acc[k] = 0.0;
+  for (int64_t p = q0 / n; p * n < q1; ++p) {
+    const int64_t jb = (q0 > p * n ? q0 : p * n) - p * n;
+    const int64_t je = (q1 < (p + 1) * n ? q1 : (p + 1) * n) - p * n;
+    const int64_t row0 = p * kPanelRows;
+    double ur[RPL][VEC], uar[RPL][VEC];
+    bool ok[RPL];
+#pragma unroll
+    for (int k = 0; k < RPL; ++k) {
+      const int64_t i = row0 + k * 32 * VEC + lane * VEC;
+      ok[k] = i < m;
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) {
+        ur[k][e] = ok[k] ? __ldg(u + i + e) : 0.0;
+        uar[k][e] = (ok[k] && have_avg) ? __ldg(ua + i + e) : 0.0;
+      }
+    }
+    for (int64_t j = jb + warp; j < je; j += kWarps) {
+      const double vj = __ldg(v + j);
+      const double vaj = have_avg ? __ldg(va + j) : 0.0;
+      const int64_t base = j * m + row0 + lane * VEC;
+      double cv[RPL][VEC], xv[RPL][VEC], av[RPL][VEC];
+#pragma unroll
+      for (int k = 0; k < RPL; ++k) {
+        if (ok[k]) {
+          const int64_t idx = base + k * 32 * VEC;
+          VecIO<VEC>::ldg(C + idx, cv[k]);
+          VecIO<VEC>::ldg(X + idx, xv[k]);
+          if (have_avg) VecIO<VEC>::ldg(Xa + idx, av[k]);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < RPL; ++k) {
+        if (ok[k]) {
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) {
+            const double c = cv[k][e], x = xv[k][e];
+            const double gg = zero_g ? 0.0 : __dsub_rn(__dsub_rn(c, ur[k][e]), vj);
+            const double mg = neg_part(gg);
+            acc[E_DOT] += c * x;
+            acc[E_SQX] += x * x;
+            acc[E_MAXX] = nanmax(acc[E_MAXX], fabs(x));
+            acc[E_SQG] += mg * mg;
+            acc[E_MAXG] = nanmax(acc[E_MAXG], mg);
+            if (have_avg) {
+              const double xa = av[k][e];
+              const double ga = __dsub_rn(__dsub_rn(c, uar[k][e]), vaj);
+              const double mga = neg_part(ga);
+              acc[E_AVG + E_DOT] += c * xa;
+              acc[E_AVG + E_SQX] += xa * xa;
+              acc[E_AVG + E_MAXX] = nanmax(acc[E_AVG + E_MAXX], fabs(xa));
+              acc[E_AVG + E_SQG] += mga * mga;
+              acc[E_AVG + E_MAXG] = nanmax(acc[E_AVG + E_MAXG], mga);
+            }
+          }
+        }
+      }
+    }
+  }
+  block_reduce<kEvalSums>(acc, kEvalMaxMask, B.evpart + cta * kEvalSums);
+}
+
+// Evaluation, vector part: per point, ||dist - sums||^2, max|dist - sums|,
+// <dist, dual>, ||dual||^2, max|dual| (src/utils_gpu.jl:26-27,54,94-95,115-116).
+enum { V_SQRES = 0, V_MAXRES, V_DOT, V_SQDUAL, V_MAXDUAL, V_AVG = 5 };
+constexpr unsigned kVecMaxMask = (1u << V_MAXRES) | (1u << V_MAXDUAL) | (1u << (V_AVG + V_MAXRES)) |
+                                 (1u << (V_AVG + V_MAXDUAL));
+
+struct PointSums {
+  double pobj, sq_x, max_x, sq_g, max_g;
+  double sq_src, max_src, dot_src, sq_u, max_u;
+  double sq_tgt, max_tgt, dot_tgt, sq_v, max_v;
+};
+
+__device__ __forceinline__ PointSums point_sums(const double* E, const double* R, const double* Cc, int off) {
+  PointSums P;
+  P.pobj = E[off + E_DOT];
+  P.sq_x = E[off + E_SQX];
+  P.max_x = E[off + E_MAXX];
+  P.sq_g = E[off + E_SQG];
+  P.max_g = E[off + E_MAXG];
+  P.sq_src = R[off + V_SQRES];
+  P.max_src = R[off + V_MAXRES];
+  P.dot_src = R[off + V_DOT];
+  P.sq_u = R[off + V_SQDUAL];
+  P.max_u = R[off + V_MAXDUAL];
+  P.sq_tgt = Cc[off + V_SQRES];
+  P.max_tgt = Cc[off + V_MAXRES];
+  P.dot_tgt = Cc[off + V_DOT];
+  P.sq_v = Cc[off + V_SQDUAL];
+  P.max_v = Cc[off + V_MAXDUAL];
+  return P;
+}
+
+// compute_weight_kkt_residual, src/saddle_point_gpu.jl:299-330
+__device__ __forceinline__ double weighted_kkt(double l2_pres, double l2_dres, double gap, double omega) {
+  return sqrt(omega * (l2_pres * l2_pres) + (1.0 / omega) * (l2_dres * l2_dres) + gap * gap);
+}
+
+// src/termination.jl:106-134
+__device__ bool optimality_met(const SolveConfig& cfg, const DevState* st,
+                               const pdot_convergence_information& ci) {
+  const double abs_obj = fabs(ci.primal_objective) + fabs(ci.dual_objective);
+  const double gap = fabs(ci.primal_objective - ci.dual_objective);
+  double perr, pbase, derr, dbase;
+  if (cfg.optimality_norm == PDOT_L_INF) {
+    perr = ci.l_inf_primal_residual;
+    pbase = st->linf_rhs;
+    derr = ci.l_inf_dual_residual;
+    dbase = st->linf_obj;
+  } else {
+    perr = ci.l2_primal_residual;
+    pbase = st->l2_rhs;
+    derr = ci.l2_dual_residual;
+    dbase = st->l2_obj;
+  }
+  return derr < cfg.eps_abs + cfg.eps_rel * dbase && perr < cfg.eps_abs + cfg.eps_rel * pbase &&
+         gap < cfg.eps_abs + cfg.eps_rel * abs_obj;
+}
+
+// The evaluation block of optimize(), src/solver_gpu.jl:529-696, with
+// compute_convergence_information (src/utils_gpu.jl:68-129),
+// check_termination_criteria (src/termination.jl:140-166), run_restart_scheme
+// (src/saddle_point_gpu.jl:539-696) and compute_new_primal_weight (:701-728).
+__device__ void eval_control(DevState* st, const SolveConfig& cfg, const PointSums& cur, const PointSums& avg,
+                             pdot_iteration_stats* ring, int ring_cap) {
+  const long long it = st->iteration;
+  st->kkt_passes += 2.0;
+  const bool have_avg = st->avg_count > 0;
+  const bool use_cur = st->numerical_error || !have_avg;
+  const PointSums& P = use_cur ? cur : avg;
+  const double eps_ratio = cfg.eps_abs / cfg.eps_rel;
+  const unsigned long long now = globaltimer_ns();
+
+  pdot_iteration_stats rec;
+  memset(&rec, 0, sizeof(rec));
+  pdot_convergence_information& ci = rec.convergence_information;
+  ci.candidate_type = PDOT_POINT_TYPE_AVERAGE_ITERATE;
+  ci.primal_objective = P.pobj;
+  ci.l_inf_primal_residual = nanmax(P.max_src, P.max_tgt);
+  ci.l2_primal_residual = sqrt(P.sq_src + P.sq_tgt);
+  ci.relative_l_inf_primal_residual = ci.l_inf_primal_residual / (eps_ratio + st->linf_rhs);
+  ci.relative_l2_primal_residual = ci.l2_primal_residual / (eps_ratio + st->l2_rhs);
+  ci.l_inf_primal_variable = P.max_x;
+  ci.l2_primal_variable = sqrt(P.sq_x);
+  ci.dual_objective = P.dot_src + P.dot_tgt;
+  ci.l_inf_dual_residual = P.max_g;
+  ci.l2_dual_residual = sqrt(P.sq_g);
+  ci.relative_l_inf_dual_residual = ci.l_inf_dual_residual / (eps_ratio + st->linf_obj);
+  ci.relative_l2_dual_residual = ci.l2_dual_residual / (eps_ratio + st->l2_obj);
+  // src/utils_gpu.jl:115-116 measure [u; u] (the source duals twice)
+  ci.l_inf_dual_variable = P.max_u;
+  ci.l2_dual_variable = sqrt(P.sq_u + P.sq_u);
+  ci.corrected_dual_objective = ci.l_inf_dual_residual == 0.0 ? ci.dual_objective : -INFINITY;
+  {
+    const double gap = fabs(ci.primal_objective - ci.dual_objective);
+    const double abs_obj = fabs(ci.primal_objective) + fabs(ci.dual_objective);
+    ci.relative_optimality_gap = gap / (eps_ratio + abs_obj);
+  }
+  rec.iteration_number = (int32_t)it;
+  rec.cumulative_kkt_matrix_passes = st->kkt_passes;
+  rec.cumulative_rejected_steps = 0;
+  rec.cumulative_time_sec = (double)(now - st->t_start_ns) * 1e-9;
+  rec.restart_used = PDOT_RESTART_CHOICE_UNSPECIFIED;
+  rec.step_size = st->step_size;
+  rec.primal_weight = st->primal_weight;
+  rec.time_spent_doing_basic_algorithm = rec.cumulative_time_sec - st->eval_time_sec;
+
+  const double omega = st->primal_weight, tau = st->step_size;
+  const double pnp = 1.0 / tau * omega, dnp = 1.0 / tau / omega;  // define_norms
+
+  int term = 0;
+  if (optimality_met(cfg, st, ci))
+    term = PDOT_TERMINATION_REASON_OPTIMAL;
+  else if (it >= cfg.iteration_limit)
+    term = PDOT_TERMINATION_REASON_ITERATION_LIMIT;
+  else if (rec.cumulative_kkt_matrix_passes >= cfg.kkt_matrix_pass_limit)
+    term = PDOT_TERMINATION_REASON_KKT_MATRIX_PASS_LIMIT;
+  else if (rec.cumulative_time_sec >= cfg.time_sec_limit)
+    term = PDOT_TERMINATION_REASON_TIME_LIMIT;
+  // Non-finite objectives can never meet the optimality test; the reference
+  // would iterate to the iteration limit. Stop with a numerical error.
+  if (!term && !(isfinite(ci.primal_objective) && isfinite(ci.dual_objective)))
+    term = PDOT_TERMINATION_REASON_NUMERICAL_ERROR;
+  if (st->numerical_error && !term) term = PDOT_TERMINATION_REASON_NUMERICAL_ERROR;
+
+  if (!term) {
+    int choice = PDOT_RESTART_CHOICE_NO_RESTART;
+    if (have_avg) {
+      const long long len = st->avg_count;
+      bool do_restart = (double)len >= cfg.artificial_restart_threshold * (double)(it - 1);
+      bool to_avg = false;
+      double cand = 0.0;
+      const double rp_c = sqrt(cur.sq_src + cur.sq_tgt), rd_c = sqrt(cur.sq_g);
+      const double gap_c = fabs(cur.pobj - (cur.dot_src + cur.dot_tgt));
+      const double rp_a = sqrt(avg.sq_src + avg.sq_tgt), rd_a = sqrt(avg.sq_g);
+      const double gap_a = fabs(avg.pobj - (avg.dot_src + avg.dot_tgt));
+      if (cfg.restart_scheme != PDOT_NO_RESTARTS) {
+        const double kc = weighted_kkt(rp_c, rd_c, gap_c, omega);
+        const double ka = weighted_kkt(rp_a, rd_a, gap_a, omega);
+        to_avg = cfg.restart_to_current_metric == PDOT_KKT_GREEDY ? (kc >= ka) : true;
+        cand = to_avg ? ka : kc;
+      }
+      if (!do_restart) {
+        if (cfg.restart_scheme == PDOT_ADAPTIVE_KKT) {
+          const double kl = weighted_kkt(st->last_rp, st->last_rd, st->last_gap, omega);
+          const double ratio = cand / kl;
+          if (ratio < cfg.necessary_reduction_for_restart) {
+            if (ratio < cfg.sufficient_reduction_for_restart)
+              do_restart = true;
+            else if (ratio > st->ratio_last_trial)
+              do_restart = true;
+          }
+          st->ratio_last_trial = ratio;
+        } else if (cfg.restart_scheme == PDOT_FIXED_FREQUENCY && cfg.restart_frequency_if_fixed <= len) {
+          do_restart = true;
+        }
+      }
+      if (do_restart) {
+        const PointSums& R = to_avg ? avg : cur;
+        // update_last_restart_info! measures from the previous restart point
+        // to the (already reset, zero) average: the norms of the previous point.
+        st->pdist = (sqrt(pnp) * st->last_xnorm) / sqrt(omega);
+        st->ddist = (sqrt(dnp) * st->last_ynorm) * sqrt(omega);
+        st->last_xnorm = sqrt(R.sq_x);
+        st->last_ynorm = sqrt(R.sq_u + R.sq_v);
+        st->last_rp = to_avg ? rp_a : rp_c;
+        st->last_rd = to_avg ? rd_a : rd_c;
+        st->last_gap = to_avg ? gap_a : gap_c;
+        st->last_restart_length = len;
+        if (to_avg) st->buf ^= 1;
+        st->sum_weights = 0.0;
+        st->avg_count = 0;
+        choice = to_avg ? PDOT_RESTART_CHOICE_RESTART_TO_AVERAGE : PDOT_RESTART_CHOICE_WEIGHTED_AVERAGE_RESET;
+        if (st->pdist > DBL_EPSILON && st->ddist > DBL_EPSILON) {
+          const double sm = cfg.primal_weight_update_smoothing;
+          const double est = st->ddist / st->pdist;
+          st->primal_weight = exp(sm * log(est) + (1.0 - sm) * log(omega));
+        }
+      }
+    }
+    rec.restart_used = choice;
+    st->last_restart_choice = choice;
+  } else {
+    st->done = 1;
+    st->termination_reason = term;
+    st->out_current = have_avg ? 0 : 1;
+  }
+  if (cfg.record_iteration_stats || term) {
+    ring[st->num_stats % ring_cap] = rec;
+    st->num_stats += 1;
+  }
+  st->eval_time_sec += (double)(globaltimer_ns() - st->eval_t0_ns) * 1e-9;
+}
+
+__global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, SolveConfig cfg) {
+  DevState* st = B.st;
+  if (st->done) return;
+  const int buf = st->buf;
+  const bool have_avg = st->avg_count > 0;
+  double acc[kVecSums];
+#pragma unroll
+  for (int k = 0; k < kVecSums; ++k) acc[k] = 0.0;
+  const int bid = blockIdx.x;
+  const bool is_row = bid < g.row_blocks;
+  const int64_t idx = (int64_t)(is_row ? bid : bid - g.row_blocks) * kVecThreads + threadIdx.x;
+  const int64_t len = is_row ? g.m : g.n;
+  if (idx < len) {
+    const double dist = is_row ? B.a[idx] : B.b[idx];
+    const double sc = (is_row ? B.r[buf] : B.c[buf])[idx];
+    const double dc = (is_row ? B.u[buf] : B.v[buf])[idx];
+    const double res = dist - sc;
+    acc[V_SQRES] = res * res;
+    acc[V_MAXRES] = fabs(res);
+    acc[V_DOT] = dist * dc;
+    acc[V_SQDUAL] = dc * dc;
+    acc[V_MAXDUAL] = fabs(dc);
+    if (have_avg) {
+      const double sa = (is_row ? B.r[buf ^ 1] : B.c[buf ^ 1])[idx];
+      const double da = (is_row ? B.u[buf ^ 1] : B.v[buf ^ 1])[idx];
+      const double ra = dist - sa;
+      acc[V_AVG + V_SQRES] = ra * ra;
+      acc[V_AVG + V_MAXRES] = fabs(ra);
+      acc[V_AVG + V_DOT] = dist * da;
+      acc[V_AVG + V_SQDUAL] = da * da;
+      acc[V_AVG + V_MAXDUAL] = fabs(da);
+    }
+  }
+  block_reduce<kVecSums>(acc, kVecMaxMask, B.vecpart + (int64_t)bid * kVecSums);
+  if (!elect_last_cta(&st->ticket_eval)) return;
+  if (threadIdx.x < 32) {
+    double E[kEvalSums], R[kVecSums], Cc[kVecSums];
+    warp_reduce_partials<kEvalSums>(B.evpart, 0, g.grid, kEvalMaxMask, E);
+    warp_reduce_partials<kVecSums>(B.vecpart, 0, g.row_blocks, kVecMaxMask, R);
+    warp_reduce_partials<kVecSums>(B.vecpart, g.row_blocks, g.col_blocks, kVecMaxMask, Cc);
+    if (threadIdx.x == 0) {
+      const PointSums cur = point_sums(E, R, Cc, 0);
+      const PointSums avg = point_sums(E, R, Cc, E_AVG);
+      eval_control(st, cfg, cur, avg, B.ring, B.ring_cap);
+      st->ticket_eval = 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Start of a solve: cached_ot_info (src/termination.jl:94-101) on the device,
+// the initial step size and primal weight (src/solver_gpu.jl:476-496,
+// src/saddle_point_gpu.jl:848-866) and the initial last-restart record (the
+// zero point, src/saddle_point_gpu.jl:371-393).
+template <int VEC>
+__global__ void __launch_bounds__(kThreads, 2) k0_init(Buffers B, Geometry g, SolveConfig cfg) {
+  constexpr int RPL = kPanelRows / (32 * VEC);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t m = g.m, n = g.n;
+  const int64_t cta = blockIdx.x;
+  const int64_t q0 = unit_begin(g, cta), q1 = unit_begin(g, cta + 1);
+  double acc[kNormSums] = {0.0, 0.0};  // sum C^2, max |C|
+  for (int64_t p = q0 / n; p * n < q1; ++p) {
+    const int64_t jb = (q0 > p * n ? q0 : p * n) - p * n;
+    const int64_t je = (q1 < (p + 1) * n ? q1 : (p + 1) * n) - p * n;
+    const int64_t row0 = p * kPanelRows;
+    for (int64_t j = jb + warp; j < je; j += kWarps) {
+      const int64_t base = j * m + row0 + lane * VEC;
+#pragma unroll
+      for (int k = 0; k < RPL; ++k) {
+        if (row0 + k * 32 * VEC + lane * VEC < m) {
+          double cv[VEC];
+          VecIO<VEC>::ldg(B.C + base + k * 32 * VEC, cv);
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) {
+            acc[0] += cv[e] * cv[e];
+            acc[1] = nanmax(acc[1], fabs(cv[e]));
+          }
+        }
+      }
+    }
+  }
+  block_reduce<kNormSums>(acc, 2u, B.evpart + cta * kNormSums);
+  DevState* st = B.st;
+  if (!elect_last_cta(&st->ticket_init)) return;
+  // the marginals' norms, by the whole CTA in a fixed order
+  double vacc[2] = {0.0, 0.0};
+  for (int64_t i = threadIdx.x; i < m + n; i += kThreads) {
+    const double x = i < m ? B.a[i] : B.b[i - m];
+    vacc[0] += x * x;
+    vacc[1] = nanmax(vacc[1], fabs(x));
+  }
+  __shared__ double vsum[2];
+  block_reduce<2>(vacc, 2u, vsum);
+  if (threadIdx.x < 32) {
+    double nc[kNormSums];
+    warp_reduce_partials<kNormSums>(B.evpart, 0, g.grid, 2u, nc);
+    if (threadIdx.x == 0) {
+      st->linf_obj = nc[1];
+      st->l2_obj = sqrt(nc[0]);
+      st->linf_rhs = vsum[1];
+      st->l2_rhs = sqrt(vsum[0]);
+      st->step_size = cfg.adaptive ? 1.0 : (1.0 - 0.2) / sqrt((double)(m + n));
+      if (cfg.scale_invariant_initial_primal_weight) {
+        const double rhs = sqrt(1.0) * st->l2_rhs, obj = sqrt(1.0) * st->l2_obj;
+        st->primal_weight = (obj > 0.0 && rhs > 0.0) ? cfg.primal_importance * (obj / rhs) : cfg.primal_importance;
+      } else {
+        st->primal_weight = cfg.primal_importance;
+      }
+      st->kkt_passes = 0.0;
+      st->sum_weights = 0.0;
+      st->avg_count = 0;
+      st->total_iters = 0;
+      st->iteration = 1;
+      st->last_rp = st->l2_rhs;  // ||[a - 0; b - 0]||
+      st->last_rd = 0.0;
+      st->last_gap = 0.0;
+      st->last_xnorm = 0.0;
+      st->last_ynorm = 0.0;
+      st->ratio_last_trial = 1.0;
+      st->last_restart_length = 1;
+      st->pdist = st->ddist = 0.0;
+      st->numerical_error = 0;
+      st->g_is_zero = 1;
+      st->buf = 0;
+      st->out_current = 1;
+      st->num_stats = 0;
+      st->eval_time_sec = 0.0;
+      st->done = 0;
+      st->termination_reason = 0;
+      // Non-finite data cannot be solved; the reference would iterate on NaNs.
+      if (!(isfinite(st->l2_obj) && isfinite(st->l2_rhs) && isfinite(st->linf_obj))) {
+        st->done = 1;
+        st->termination_reason = PDOT_TERMINATION_REASON_INVALID_PROBLEM;
+      }
+      st->t_start_ns = globaltimer_ns();
+      st->ticket_init = 0;
+    }
+  }
+}
+
+template <typename K>
+int blocks_per_sm(K kernel) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kThreads, 0) != cudaSuccess || nb < 1) nb = 1;
+  return nb;
+}
+
+}  // namespace
+
+Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device) {
+  Geometry g;
+  g.m = m;
+  g.n = n;
+  g.panels = (m + kPanelRows - 1) / kPanelRows;
+  g.units = g.panels * n;
+  g.vec = (vec_ok && (m % 2 == 0)) ? 2 : 1;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const int occ = g.vec == 2 ? blocks_per_sm(k1_primal<2>) : blocks_per_sm(k1_primal<1>);
+  int64_t grid = (int64_t)sms * occ;
+  if (grid > g.units) grid = g.units;
+  g.grid = (int32_t)grid;
+  g.row_blocks = (int32_t)((m + kVecThreads - 1) / kVecThreads);
+  g.col_blocks = (int32_t)((n + kVecThreads - 1) / kVecThreads);
+  return g;
+}
+
+size_t workspace_doubles(const Geometry& g) {
+  const size_t vb = (size_t)g.row_blocks + g.col_blocks;
+  return ((size_t)g.grid + g.panels) * kPanelRows  // rowpart
+         + (size_t)g.panels * g.n                   // colpart
+         + (size_t)g.grid                           // sqpart
+         + vb * kStepSums                           // steppart
+         + (size_t)g.grid * kEvalSums               // evpart
+         + vb * kVecSums;                           // vecpart
+}
+
+cudaError_t launch_init(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s) {
+  if (g.vec == 2)
+    k0_init<2><<<g.grid, kThreads, 0, s>>>(B, g, cfg);
+  else
+    k0_init<1><<<g.grid, kThreads, 0, s>>>(B, g, cfg);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s) {
+  if (g.vec == 2)
+    k1_primal<2><<<g.grid, kThreads, 0, s>>>(B, g);
+  else
+    k1_primal<1><<<g.grid, kThreads, 0, s>>>(B, g);
+  k2_dual<<<g.row_blocks + g.col_blocks, kVecThreads, 0, s>>>(B, g, cfg);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s) {
+  if (g.vec == 2)
+    k3_eval<2><<<g.grid, kThreads, 0, s>>>(B, g);
+  else
+    k3_eval<1><<<g.grid, kThreads, 0, s>>>(B, g);
+  k4_eval<<<g.row_blocks + g.col_blocks, kVecThreads, 0, s>>>(B, g, cfg);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_primal_pass(const Geometry& g, const double* C, double* X, double* Xa, const double* u,
+                               const double* v, double step_over_weight, double avg_new_weight,
+                               double avg_scale, int flags, double* drow, double* dcol, double* dsq,
+                               double* work, cudaStream_t s) {
+  double* rowpart = work;
+  double* colpart = rowpart + ((size_t)g.grid + g.panels) * kPanelRows;
+  double* sqpart = colpart + (size_t)g.panels * g.n;
+  if (g.vec == 2)
+    k1_primal_args<2><<<g.grid, kThreads, 0, s>>>(C, X, Xa, u, v, step_over_weight, avg_new_weight, avg_scale,
+                                                  flags, colpart, rowpart, sqpart, g);
+  else
+    k1_primal_args<1><<<g.grid, kThreads, 0, s>>>(C, X, Xa, u, v, step_over_weight, avg_new_weight, avg_scale,
+                                                  flags, colpart, rowpart, sqpart, g);
+  k_pass_sums<<<g.row_blocks + g.col_blocks + 1, kVecThreads, 0, s>>>(g, rowpart, colpart, sqpart, drow, dcol,
+                                                                      dsq);
+  return cudaGetLastError();
+}
+
+}  // namespace pdot

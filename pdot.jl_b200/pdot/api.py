@@ -1,0 +1,373 @@
+"""Host-side mirror of the reference's Julia API, over the C ABI of libpdot.so.
+
+Names, argument meaning and error behaviour follow MIT-Lu-Lab/PDOT.jl:
+
+    OptimalTransportProblem                src/io.jl:1-5
+    AdaptiveStepsizeParams / Constant...   src/solver_gpu.jl:2-7
+    PdhgParameters                         src/solver_gpu.jl:9-21
+    TerminationCriteria, OptimalityNorm    src/termination.jl:2-69
+    RestartParameters, RestartScheme, ...  src/saddle_point_gpu.jl:401-472
+    ConvergenceInformation, IterationStats,
+    RestartChoice, PointType,
+    TerminationReason, SolveLog            src/solve_log.jl
+    SaddlePointOutput                      src/saddle_point_gpu.jl:2-34
+    optimize(params, problem)              src/solver_gpu.jl:413-720
+
+`optimize` runs on the GPU through libpdot.so; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import enum
+import math
+from dataclasses import dataclass, field
+from typing import Optional, Union
+
+import numpy as np
+
+from . import _abi
+
+INT32_MAX = 2**31 - 1
+
+
+# ---------------------------------------------------------------- enums
+class OptimalityNorm(enum.IntEnum):  # src/termination.jl:2
+    L_INF = 0
+    L_2 = 1
+
+
+class RestartScheme(enum.IntEnum):  # src/saddle_point_gpu.jl:401
+    NO_RESTARTS = 0
+    FIXED_FREQUENCY = 1
+    ADAPTIVE_KKT = 2
+
+
+class RestartToCurrentMetric(enum.IntEnum):  # src/saddle_point_gpu.jl:408
+    NO_RESTART_TO_CURRENT = 0
+    KKT_GREEDY = 1
+
+
+class RestartChoice(enum.IntEnum):  # src/solve_log.jl:15-20
+    RESTART_CHOICE_UNSPECIFIED = 0
+    RESTART_CHOICE_NO_RESTART = 1
+    RESTART_CHOICE_WEIGHTED_AVERAGE_RESET = 2
+    RESTART_CHOICE_RESTART_TO_AVERAGE = 3
+
+
+class PointType(enum.IntEnum):  # src/solve_log.jl:35-41
+    POINT_TYPE_UNSPECIFIED = 0
+    POINT_TYPE_CURRENT_ITERATE = 1
+    POINT_TYPE_ITERATE_DIFFERENCE = 2
+    POINT_TYPE_AVERAGE_ITERATE = 3
+    POINT_TYPE_NONE = 4
+
+
+class TerminationReason(enum.IntEnum):  # src/solve_log.jl:245-254
+    TERMINATION_REASON_UNSPECIFIED = 0
+    TERMINATION_REASON_OPTIMAL = 1
+    TERMINATION_REASON_TIME_LIMIT = 2
+    TERMINATION_REASON_ITERATION_LIMIT = 3
+    TERMINATION_REASON_KKT_MATRIX_PASS_LIMIT = 4
+    TERMINATION_REASON_NUMERICAL_ERROR = 5
+    TERMINATION_REASON_INVALID_PROBLEM = 6
+    TERMINATION_REASON_OTHER = 7
+
+
+L_INF = OptimalityNorm.L_INF
+L_2 = OptimalityNorm.L_2
+NO_RESTARTS = RestartScheme.NO_RESTARTS
+FIXED_FREQUENCY = RestartScheme.FIXED_FREQUENCY
+ADAPTIVE_KKT = RestartScheme.ADAPTIVE_KKT
+NO_RESTART_TO_CURRENT = RestartToCurrentMetric.NO_RESTART_TO_CURRENT
+KKT_GREEDY = RestartToCurrentMetric.KKT_GREEDY
+
+
+def termination_reason_to_string(reason: TerminationReason) -> str:
+    """src/termination.jl:168-171: strip the TERMINATION_REASON_ prefix."""
+    return TerminationReason(reason).name[len("TERMINATION_REASON_"):]
+
+
+# ---------------------------------------------------------------- problem
+@dataclass
+class OptimalTransportProblem:
+    """src/io.jl:1-5. cost_matrix is m x n (sources x targets)."""
+
+    cost_matrix: np.ndarray
+    source_distribution: np.ndarray
+    target_distribution: np.ndarray
+
+
+# ---------------------------------------------------------------- parameters
+@dataclass
+class AdaptiveStepsizeParams:  # src/solver_gpu.jl:2-5
+    reduction_exponent: float
+    growth_exponent: float
+
+
+@dataclass
+class ConstantStepsizeParams:  # src/solver_gpu.jl:7
+    pass
+
+
+@dataclass
+class TerminationCriteria:  # src/termination.jl:5-51
+    optimality_norm: OptimalityNorm
+    eps_optimal_absolute: float
+    eps_optimal_relative: float
+    time_sec_limit: float
+    iteration_limit: int
+    kkt_matrix_pass_limit: float
+
+
+def construct_termination_criteria(
+    *,
+    optimality_norm=L_2,
+    eps_optimal_absolute,
+    eps_optimal_relative,
+    time_sec_limit=math.inf,
+    iteration_limit=INT32_MAX,
+    kkt_matrix_pass_limit=math.inf,
+) -> TerminationCriteria:
+    """src/termination.jl:53-69 (keyword-only, same defaults)."""
+    return TerminationCriteria(
+        OptimalityNorm(optimality_norm),
+        float(eps_optimal_absolute),
+        float(eps_optimal_relative),
+        float(time_sec_limit),
+        int(iteration_limit),
+        float(kkt_matrix_pass_limit),
+    )
+
+
+@dataclass
+class RestartParameters:  # src/saddle_point_gpu.jl:411-441
+    restart_scheme: RestartScheme
+    restart_to_current_metric: RestartToCurrentMetric
+    restart_frequency_if_fixed: int
+    artificial_restart_threshold: float
+    sufficient_reduction_for_restart: float
+    necessary_reduction_for_restart: float
+    primal_weight_update_smoothing: float
+
+
+def construct_restart_parameters(
+    restart_scheme,
+    restart_to_current_metric,
+    restart_frequency_if_fixed: int,
+    artificial_restart_threshold: float,
+    sufficient_reduction_for_restart: float,
+    necessary_reduction_for_restart: float,
+    primal_weight_update_smoothing: float,
+) -> RestartParameters:
+    """src/saddle_point_gpu.jl:446-472, including its assertions."""
+    assert restart_frequency_if_fixed > 1
+    assert 0.0 < artificial_restart_threshold <= 1.0
+    assert 0.0 < sufficient_reduction_for_restart <= necessary_reduction_for_restart <= 1.0
+    assert 0.0 <= primal_weight_update_smoothing <= 1.0
+    return RestartParameters(
+        RestartScheme(restart_scheme),
+        RestartToCurrentMetric(restart_to_current_metric),
+        int(restart_frequency_if_fixed),
+        float(artificial_restart_threshold),
+        float(sufficient_reduction_for_restart),
+        float(necessary_reduction_for_restart),
+        float(primal_weight_update_smoothing),
+    )
+
+
+@dataclass
+class PdhgParameters:  # src/solver_gpu.jl:9-21
+    primal_importance: float
+    scale_invariant_initial_primal_weight: bool
+    verbosity: int
+    record_iteration_stats: bool
+    termination_evaluation_frequency: int
+    termination_criteria: TerminationCriteria
+    restart_params: RestartParameters
+    step_size_policy_params: Union[AdaptiveStepsizeParams, ConstantStepsizeParams]
+
+
+# ---------------------------------------------------------------- output
+@dataclass
+class ConvergenceInformation:  # src/solve_log.jl:47-151
+    candidate_type: PointType = PointType.POINT_TYPE_UNSPECIFIED
+    primal_objective: float = 0.0
+    dual_objective: float = 0.0
+    corrected_dual_objective: float = 0.0
+    l_inf_primal_residual: float = 0.0
+    l2_primal_residual: float = 0.0
+    l_inf_dual_residual: float = 0.0
+    l2_dual_residual: float = 0.0
+    relative_l_inf_primal_residual: float = 0.0
+    relative_l2_primal_residual: float = 0.0
+    relative_l_inf_dual_residual: float = 0.0
+    relative_l2_dual_residual: float = 0.0
+    relative_optimality_gap: float = 0.0
+    l_inf_primal_variable: float = 0.0
+    l2_primal_variable: float = 0.0
+    l_inf_dual_variable: float = 0.0
+    l2_dual_variable: float = 0.0
+
+
+@dataclass
+class IterationStats:  # src/solve_log.jl:154-228
+    iteration_number: int = 0
+    convergence_information: list = field(default_factory=list)
+    cumulative_kkt_matrix_passes: float = 0.0
+    cumulative_rejected_steps: int = 0
+    cumulative_time_sec: float = 0.0
+    restart_used: RestartChoice = RestartChoice.RESTART_CHOICE_UNSPECIFIED
+    step_size: float = 0.0
+    primal_weight: float = 0.0
+    method_specific_stats: dict = field(default_factory=dict)
+
+
+@dataclass
+class SaddlePointOutput:  # src/saddle_point_gpu.jl:2-34
+    primal_solution: np.ndarray
+    dual_source_solution: np.ndarray
+    dual_target_solution: np.ndarray
+    termination_reason: TerminationReason
+    termination_string: str
+    iteration_count: int
+    iteration_stats: list
+
+
+@dataclass
+class SolveLog:  # src/solve_log.jl:256-327
+    instance_name: str = ""
+    command_line_invocation: str = ""
+    termination_reason: TerminationReason = TerminationReason.TERMINATION_REASON_UNSPECIFIED
+    termination_string: str = ""
+    iteration_count: int = 0
+    solve_time_sec: float = 0.0
+    solution_stats: IterationStats = field(default_factory=IterationStats)
+    solution_type: PointType = PointType.POINT_TYPE_UNSPECIFIED
+    iteration_stats: list = field(default_factory=list)
+
+
+# ---------------------------------------------------------------- marshalling
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ct.POINTER(ct.c_double))
+
+
+def marshal_params(params: PdhgParameters) -> _abi.PdhgParametersC:
+    tc, rp = params.termination_criteria, params.restart_params
+    c = _abi.PdhgParametersC()
+    c.primal_importance = float(params.primal_importance)
+    c.scale_invariant_initial_primal_weight = int(bool(params.scale_invariant_initial_primal_weight))
+    c.verbosity = int(params.verbosity)
+    c.record_iteration_stats = int(bool(params.record_iteration_stats))
+    c.termination_evaluation_frequency = int(params.termination_evaluation_frequency)
+    c.termination_criteria.optimality_norm = int(tc.optimality_norm)
+    c.termination_criteria.eps_optimal_absolute = float(tc.eps_optimal_absolute)
+    c.termination_criteria.eps_optimal_relative = float(tc.eps_optimal_relative)
+    c.termination_criteria.time_sec_limit = float(tc.time_sec_limit)
+    c.termination_criteria.iteration_limit = int(min(tc.iteration_limit, INT32_MAX))
+    c.termination_criteria.kkt_matrix_pass_limit = float(tc.kkt_matrix_pass_limit)
+    c.restart_params.restart_scheme = int(rp.restart_scheme)
+    c.restart_params.restart_to_current_metric = int(rp.restart_to_current_metric)
+    c.restart_params.restart_frequency_if_fixed = int(rp.restart_frequency_if_fixed)
+    c.restart_params.artificial_restart_threshold = float(rp.artificial_restart_threshold)
+    c.restart_params.sufficient_reduction_for_restart = float(rp.sufficient_reduction_for_restart)
+    c.restart_params.necessary_reduction_for_restart = float(rp.necessary_reduction_for_restart)
+    c.restart_params.primal_weight_update_smoothing = float(rp.primal_weight_update_smoothing)
+    sp = params.step_size_policy_params
+    if isinstance(sp, AdaptiveStepsizeParams):
+        c.step_size_policy = 0
+        c.reduction_exponent = float(sp.reduction_exponent)
+        c.growth_exponent = float(sp.growth_exponent)
+    elif isinstance(sp, ConstantStepsizeParams):
+        c.step_size_policy = 1
+    else:
+        raise TypeError("step_size_policy_params must be AdaptiveStepsizeParams or ConstantStepsizeParams")
+    return c
+
+
+class MarshalledProblem:
+    """Keeps the column-major host arrays alive for the duration of a call."""
+
+    def __init__(self, problem: OptimalTransportProblem):
+        C = np.asarray(problem.cost_matrix, dtype=np.float64)
+        if C.ndim != 2:
+            raise ValueError("cost_matrix must be a matrix")
+        self.C = np.asfortranarray(C)
+        self.a = np.ascontiguousarray(problem.source_distribution, dtype=np.float64).ravel()
+        self.b = np.ascontiguousarray(problem.target_distribution, dtype=np.float64).ravel()
+        m, n = self.C.shape
+        if self.a.shape[0] != m or self.b.shape[0] != n:
+            raise ValueError("distribution lengths must match the cost matrix shape")
+        self.m, self.n = m, n
+        self.c = _abi.ProblemC(m, n, _dptr(self.C), _dptr(self.a), _dptr(self.b))
+
+
+def stats_from_c(s: _abi.IterationStatsC) -> IterationStats:
+    ci = ConvergenceInformation(PointType(s.convergence_information.candidate_type))
+    for f in _abi.CONVERGENCE_FIELDS:
+        setattr(ci, f, getattr(s.convergence_information, f))
+    return IterationStats(
+        iteration_number=s.iteration_number,
+        convergence_information=[ci],
+        cumulative_kkt_matrix_passes=s.cumulative_kkt_matrix_passes,
+        cumulative_rejected_steps=s.cumulative_rejected_steps,
+        cumulative_time_sec=s.cumulative_time_sec,
+        restart_used=RestartChoice(s.restart_used),
+        step_size=s.step_size,
+        primal_weight=s.primal_weight,
+        method_specific_stats={"time_spent_doing_basic_algorithm": s.time_spent_doing_basic_algorithm},
+    )
+
+
+class OutputBuffers:
+    def __init__(self, m: int, n: int, stats_capacity: int):
+        self.X = np.zeros((m, n), dtype=np.float64, order="F")
+        self.u = np.zeros(m, dtype=np.float64)
+        self.v = np.zeros(n, dtype=np.float64)
+        self.stats = (_abi.IterationStatsC * max(stats_capacity, 1))()
+        self.c = _abi.SaddlePointOutputC()
+        self.c.primal_solution = _dptr(self.X)
+        self.c.dual_source_solution = _dptr(self.u)
+        self.c.dual_target_solution = _dptr(self.v)
+        self.c.iteration_stats = ct.cast(self.stats, ct.POINTER(_abi.IterationStatsC))
+        self.c.iteration_stats_capacity = stats_capacity
+
+    def to_output(self) -> SaddlePointOutput:
+        cnt = min(self.c.iteration_stats_count, self.c.iteration_stats_capacity)
+        stats = [stats_from_c(self.stats[k]) for k in range(cnt)]
+        if self.c.iteration_stats_count > cnt or cnt == 0:
+            # Records beyond the buffer are dropped, but the final one is kept.
+            stats.append(stats_from_c(self.c.final_stats))
+        reason = TerminationReason(self.c.termination_reason)
+        return SaddlePointOutput(
+            self.X, self.u, self.v, reason, termination_reason_to_string(reason),
+            int(self.c.iteration_count), stats,
+        )
+
+
+def stats_capacity_for(params: PdhgParameters, cap: int = 1 << 16) -> int:
+    lim = params.termination_criteria.iteration_limit
+    freq = max(int(params.termination_evaluation_frequency), 1)
+    return int(min(cap, lim // freq + 16))
+
+
+def validate(params: PdhgParameters) -> None:
+    """Raise where the reference raises: src/solver_gpu.jl:420-422."""
+    if params.primal_importance <= 0 or not math.isfinite(params.primal_importance):
+        raise ValueError("primal_importance must be positive and finite")
+
+
+# ---------------------------------------------------------------- optimize
+def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device: int = 0,
+             use_cuda_graph: bool = True) -> SaddlePointOutput:
+    """PDOT.optimize, src/solver_gpu.jl:413-720, run by libpdot.so on the GPU."""
+    validate(params)
+    lib = _abi.load()
+    mp = MarshalledProblem(problem)
+    cp = marshal_params(params)
+    opts = _abi.SolverOptionsC()
+    opts.device = device
+    opts.use_cuda_graph = 1 if use_cuda_graph else 0
+    ob = OutputBuffers(mp.m, mp.n, stats_capacity_for(params))
+    rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
+    _abi.check(lib, rc, "pdot_optimize")
+    return ob.to_output()

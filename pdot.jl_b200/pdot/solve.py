@@ -1,0 +1,146 @@
+"""Mirror of scripts/solve.jl: `solve_instance_and_output`, `warm_up`,
+`write_vector_to_file`, plus `rounding` (src/utils_gpu.jl:296-318).
+
+Compatibility fixes to the script as shipped (it does not run as written):
+`output_dir` is the `output_directory` argument (scripts/solve.jl:54,101,...),
+`time_sec_limit` is +inf (:72), the warm-up uses the caller's tolerance and its
+own termination criteria (:25-26, :39), `rounding` is the package's (:117),
+and the dual file holds [dual_source; dual_target] (:120, the struct has no
+`dual_solution` field, src/saddle_point_gpu.jl:11-12).
+"""
+from __future__ import annotations
+
+import gzip
+import json
+import math
+import os
+import sys
+from dataclasses import asdict
+
+import numpy as np
+
+from . import api
+
+
+def julia_float_str(x: float) -> str:
+    """Float64 text as Julia's `println` writes it: shortest round-trip digits,
+    scientific below 1e-4 with Julia's exponent style (0.25, 1.0e-5, 3.0).
+    Python's repr uses the same digits and the same small-number threshold."""
+    x = float(x)
+    if math.isnan(x):
+        return "NaN"
+    if math.isinf(x):
+        return "Inf" if x > 0 else "-Inf"
+    r = repr(x)
+    if "e" in r:
+        mant, ex = r.split("e")
+        if "." not in mant:
+            mant += ".0"
+        return f"{mant}e{int(ex)}"
+    if "." not in r:
+        r += ".0"
+    return r
+
+
+def write_vector_to_file(filename: str, vector) -> None:
+    """scripts/solve.jl:5-11: one value per line, matrices in column-major order."""
+    arr = np.asarray(vector)
+    flat = arr.ravel(order="F")
+    with open(filename, "w") as io:
+        for x in flat:
+            io.write(julia_float_str(x) + "\n")
+
+
+def rounding(problem: api.OptimalTransportProblem, primal_solution: np.ndarray) -> np.ndarray:
+    """src/utils_gpu.jl:296-318: make a plan feasible. Like the reference it
+    modifies `primal_solution` in place and returns it."""
+    X = primal_solution
+    a = np.asarray(problem.source_distribution, dtype=np.float64)
+    b = np.asarray(problem.target_distribution, dtype=np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        tmp = a / X.sum(axis=1)
+    tmp = np.where(np.isnan(tmp), 0.0, tmp)
+    X *= np.minimum(tmp, 1.0)[:, None]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        tmp = b / X.sum(axis=0)
+    tmp = np.where(np.isnan(tmp), 0.0, tmp)
+    X *= np.minimum(tmp, 1.0)[None, :]
+    err_r = a - X.sum(axis=1)
+    n1 = np.abs(err_r).sum()
+    if n1 != 0.0:
+        err_r = err_r / n1
+    err_c = b - X.sum(axis=0)
+    X += np.outer(err_r, err_c)
+    return X
+
+
+def default_parameters(tolerance: float = 1.0e-4, *, verbosity: int = 2,
+                       iteration_limit: int = api.INT32_MAX) -> api.PdhgParameters:
+    """The parameters scripts/solve.jl:58-86 builds."""
+    restart_params = api.construct_restart_parameters(
+        api.ADAPTIVE_KKT, api.KKT_GREEDY, 1000, 0.36, 0.1, 0.9, 0.5
+    )
+    termination_params = api.construct_termination_criteria(
+        optimality_norm=api.L_2,
+        eps_optimal_absolute=tolerance,
+        eps_optimal_relative=tolerance,
+        time_sec_limit=math.inf,
+        iteration_limit=iteration_limit,
+        kkt_matrix_pass_limit=math.inf,
+    )
+    return api.PdhgParameters(
+        1.0, False, verbosity, True, 128, termination_params, restart_params,
+        api.AdaptiveStepsizeParams(2, 1),
+    )
+
+
+def warm_up(ot: api.OptimalTransportProblem, tolerance: float = 1.0e-4) -> None:
+    """scripts/solve.jl:13-45: a 100-iteration solve, verbosity 0."""
+    params = default_parameters(tolerance, verbosity=0, iteration_limit=100)
+    api.optimize(params, ot)
+
+
+def _jsonable(obj):
+    if isinstance(obj, dict):
+        return {k: _jsonable(v) for k, v in obj.items()}
+    if isinstance(obj, list):
+        return [_jsonable(v) for v in obj]
+    if hasattr(obj, "name") and hasattr(obj, "value") and isinstance(obj, int):
+        return obj.name  # enums serialise as their names (StructTypes' StringType)
+    return obj
+
+
+def solve_log_json(log: api.SolveLog) -> str:
+    return json.dumps(_jsonable(asdict(log)), allow_nan=True)
+
+
+def solve_instance_and_output(output_directory: str, instance_name: str,
+                              instance: api.OptimalTransportProblem, *, tolerance: float = 1.0e-4):
+    """scripts/solve.jl:48-131 (README.md:26-31 signature)."""
+    os.makedirs(output_directory, exist_ok=True)
+    parameters = default_parameters(tolerance)
+    warm_up(instance, tolerance)
+    output = api.optimize(parameters, instance)
+
+    log = api.SolveLog()
+    log.instance_name = instance_name
+    log.command_line_invocation = " ".join(sys.argv)
+    log.termination_reason = output.termination_reason
+    log.termination_string = output.termination_string
+    log.iteration_count = output.iteration_count
+    log.solve_time_sec = output.iteration_stats[-1].cumulative_time_sec
+    log.solution_stats = output.iteration_stats[-1]
+    log.solution_type = api.PointType.POINT_TYPE_AVERAGE_ITERATE
+
+    with open(os.path.join(output_directory, instance_name + "_summary.json"), "w") as io:
+        io.write(solve_log_json(log))
+    log.iteration_stats = output.iteration_stats
+    with gzip.open(os.path.join(output_directory, instance_name + "_full_log.json.gz"), "wt") as io:
+        io.write(solve_log_json(log))
+    write_vector_to_file(os.path.join(output_directory, instance_name + "_primal.txt"),
+                         output.primal_solution)
+    write_vector_to_file(os.path.join(output_directory, instance_name + "_primal_rounded.txt"),
+                         rounding(instance, output.primal_solution.copy(order="F")))
+    write_vector_to_file(os.path.join(output_directory, instance_name + "_dual.txt"),
+                         np.concatenate([output.dual_source_solution, output.dual_target_solution]))
+    return output

@@ -129,7 +129,8 @@ typedef struct pdot_pdhg_parameters {
 typedef struct pdot_solver_options {
   int32_t device;                     /* CUDA device ordinal */
   int32_t use_cuda_graph;             /* 1: replay captured iteration chunks */
-  int32_t reserved[14];               /* must be zero */
+  int32_t time_kernels;               /* 1: CUDA events around every launch (direct launches) */
+  int32_t reserved[13];               /* must be zero */
 } pdot_solver_options;
 
 /* ---- output -------------------------------------------------------------- */
@@ -208,6 +209,49 @@ int pdot_optimize(const pdot_problem* problem,
  * primal_importance 1.0; record stats; evaluation every 128 iterations;
  * AdaptiveStepsizeParams(2, 1)). */
 void pdot_default_parameters(double tolerance, pdot_pdhg_parameters* params);
+
+/* ---- solver objects ------------------------------------------------------
+ * A solver holds one problem on the device and the state of optimize()'s
+ * loop, so that a caller can reuse the device copy (the warm-up solve of
+ * scripts/solve.jl:123-126 followed by the real solve) and advance the loop in
+ * pieces. pdot_optimize is create + finish + destroy. */
+typedef struct pdot_solver pdot_solver;
+
+typedef struct pdot_solver_status {
+  int64_t iteration;                  /* number of the next loop body (1 at the start) */
+  int64_t total_number_iterations;    /* solver_state.total_number_iterations */
+  int32_t done;                       /* 1 once a termination reason is set */
+  int32_t termination_reason;
+  double step_size;
+  double primal_weight;
+  double cumulative_kkt_matrix_passes;
+  int64_t iteration_stats_count;      /* records produced so far */
+  int64_t primal_passes;              /* fused primal passes run (accepted steps) */
+  int64_t primal_passes_fresh_average;/* of those, passes that started a new average */
+  /* device time per kernel family, accumulated while options->time_kernels */
+  int64_t timed_primal_passes;
+  double primal_pass_ms;
+  double dual_step_ms;
+  double evaluation_ms;
+} pdot_solver_status;
+
+/* Copies the host problem to `options->device` and prepares the loop. */
+int pdot_solver_create(const pdot_problem* problem, const pdot_pdhg_parameters* params,
+                       const pdot_solver_options* options, pdot_solver** solver);
+/* Same, but the problem's three arrays are device pointers on
+ * options->device, read in place (they must outlive the solver). */
+int pdot_solver_create_device(const pdot_problem* device_problem, const pdot_pdhg_parameters* params,
+                              const pdot_solver_options* options, pdot_solver** solver);
+/* Back to the state optimize() starts from (iteration 1, zero iterates). */
+int pdot_solver_reset(pdot_solver* solver);
+/* Runs up to `max_iterations` more loop bodies of optimize() (fewer if it
+ * terminates) and waits for them; `status` may be NULL. */
+int pdot_solver_iterate(pdot_solver* solver, int64_t max_iterations, pdot_solver_status* status);
+/* Runs to termination and fills `output` like pdot_optimize. */
+int pdot_solver_finish(pdot_solver* solver, pdot_saddle_point_output* output);
+/* The CUDA stream (cudaStream_t) all of the solver's work is issued on. */
+void* pdot_solver_stream(pdot_solver* solver);
+void pdot_solver_destroy(pdot_solver* solver);
 
 /* ---- device-level entry points of the hot path --------------------------- */
 /* These act on device memory (pointers from cudaMalloc or torch) and on the

@@ -46,6 +46,11 @@ def load():
     lib.pdot_oracle_primal_pass.argtypes = [
         ct.c_int64, ct.c_int64, P, P, P, P, P, D, D, D, ct.c_int32, P, P, P,
     ]
+    lib.pdot_oracle_time_steps.restype = ct.c_int
+    lib.pdot_oracle_time_steps.argtypes = [
+        ct.POINTER(_abi.ProblemC), ct.POINTER(_abi.PdhgParametersC), ct.c_int, ct.c_int,
+        ct.POINTER(ct.c_double),
+    ]
     lib.pdot_oracle_version.restype = ct.c_int
     _lib = lib
     return lib
@@ -83,3 +88,18 @@ def primal_pass(C, X, Xa, u, v, step_over_weight, avg_new_weight, avg_scale, fla
     lib.pdot_oracle_primal_pass(m, n, _p(C), _p(X), _p(Xa), _p(u), _p(v), step_over_weight,
                                 avg_new_weight, avg_scale, flags, _p(drow), _p(dcol), _p(dsq))
     return drow, dcol, float(dsq[0])
+
+
+def time_steps(params, problem, steps: int, num_threads: int = 0) -> float:
+    """Seconds the oracle takes for `steps` PDHG iterations (take_step! only)
+    from the initial state, with `num_threads` OpenMP threads (0 = all)."""
+    from pdot import api, _abi
+
+    lib = load()
+    mp = api.MarshalledProblem(problem)
+    cp = api.marshal_params(params)
+    sec = ct.c_double(0.0)
+    rc = lib.pdot_oracle_time_steps(ct.byref(mp.c), ct.byref(cp), int(steps), int(num_threads), ct.byref(sec))
+    if rc != 0:
+        raise _abi.PdotError(rc, f"oracle time_steps failed ({rc})")
+    return sec.value

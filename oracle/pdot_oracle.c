@@ -570,6 +570,48 @@ int pdot_oracle_validate(const pdot_problem* P, const pdot_pdhg_parameters* prm)
 
 static void* zalloc(i64 count) { return calloc((size_t)(count > 0 ? count : 1), sizeof(double)); }
 
+static void ostate_free(ostate* S) {
+  free(S->R.colbuf);
+  free(S->X); free(S->G); free(S->Xa); free(S->Ga); free(S->dX); free(S->Xl); free(S->Gl);
+  free(S->u); free(S->r); free(S->ua); free(S->ra); free(S->nu); free(S->du); free(S->dr);
+  free(S->nr); free(S->ul); free(S->rl); free(S->viol_s);
+  free(S->v); free(S->c); free(S->va); free(S->ca); free(S->nv); free(S->dv); free(S->dc);
+  free(S->nc); free(S->vl); free(S->cl); free(S->viol_t);
+  memset(S, 0, sizeof(*S));
+}
+
+/* Allocation of the reference's state (src/solver_gpu.jl:428-472,
+ * src/saddle_point_gpu.jl:70-88) and cached_ot_info (src/termination.jl:94-101). */
+static int ostate_init(ostate* S, const pdot_problem* P) {
+  memset(S, 0, sizeof(*S));
+  const i64 m = P->num_row, n = P->num_col, N = m * n;
+  S->m = m;
+  S->n = n;
+  S->C = P->cost_matrix;
+  S->a = P->source_distribution;
+  S->b = P->target_distribution;
+  S->R.m = m;
+  S->R.n = n;
+  S->R.colbuf = zalloc(n);
+  S->X = zalloc(N); S->G = zalloc(N); S->Xa = zalloc(N); S->Ga = zalloc(N);
+  S->dX = zalloc(N); S->Xl = zalloc(N); S->Gl = zalloc(N);
+  S->u = zalloc(m); S->r = zalloc(m); S->ua = zalloc(m); S->ra = zalloc(m);
+  S->nu = zalloc(m); S->du = zalloc(m); S->dr = zalloc(m); S->nr = zalloc(m);
+  S->ul = zalloc(m); S->rl = zalloc(m); S->viol_s = zalloc(m);
+  S->v = zalloc(n); S->c = zalloc(n); S->va = zalloc(n); S->ca = zalloc(n);
+  S->nv = zalloc(n); S->dv = zalloc(n); S->dc = zalloc(n); S->nc = zalloc(n);
+  S->vl = zalloc(n); S->cl = zalloc(n); S->viol_t = zalloc(n);
+  if (!S->R.colbuf || !S->X || !S->G || !S->Xa || !S->Ga || !S->dX || !S->Xl || !S->Gl) {
+    ostate_free(S);
+    return 0;
+  }
+  S->linf_obj = mat_nrminf(&S->R, S->C);
+  S->linf_rhs = cat_nrminf(S->a, m, S->b, n);
+  S->l2_obj = mat_nrm2(&S->R, S->C);
+  S->l2_rhs = cat_nrm2(S->a, m, S->b, n);
+  return 1;
+}
+
 /* ---- src/solver_gpu.jl:413-720  optimize ----------------------------- */
 int pdot_oracle_optimize(const pdot_problem* P, const pdot_pdhg_parameters* prm,
                          pdot_saddle_point_output* out, int num_threads) {
@@ -582,32 +624,8 @@ int pdot_oracle_optimize(const pdot_problem* P, const pdot_pdhg_parameters* prm,
 #endif
   ostate St;
   ostate* S = &St;
-  memset(S, 0, sizeof(*S));
   const i64 m = P->num_row, n = P->num_col, N = m * n;
-  S->m = m;
-  S->n = n;
-  S->C = P->cost_matrix;
-  S->a = P->source_distribution;
-  S->b = P->target_distribution;
-  S->R.m = m;
-  S->R.n = n;
-  S->R.colbuf = zalloc(n);
-
-  /* cached_ot_info, src/termination.jl:94-101 */
-  S->linf_obj = mat_nrminf(&S->R, S->C);
-  S->linf_rhs = cat_nrminf(S->a, m, S->b, n);
-  S->l2_obj = mat_nrm2(&S->R, S->C);
-  S->l2_rhs = cat_nrm2(S->a, m, S->b, n);
-
-  S->X = zalloc(N); S->G = zalloc(N); S->Xa = zalloc(N); S->Ga = zalloc(N);
-  S->dX = zalloc(N); S->Xl = zalloc(N); S->Gl = zalloc(N);
-  S->u = zalloc(m); S->r = zalloc(m); S->ua = zalloc(m); S->ra = zalloc(m);
-  S->nu = zalloc(m); S->du = zalloc(m); S->dr = zalloc(m); S->nr = zalloc(m);
-  S->ul = zalloc(m); S->rl = zalloc(m); S->viol_s = zalloc(m);
-  S->v = zalloc(n); S->c = zalloc(n); S->va = zalloc(n); S->ca = zalloc(n);
-  S->nv = zalloc(n); S->dv = zalloc(n); S->dc = zalloc(n); S->nc = zalloc(n);
-  S->vl = zalloc(n); S->cl = zalloc(n); S->viol_t = zalloc(n);
-  if (!S->X || !S->G || !S->Xa || !S->Ga || !S->dX || !S->Xl || !S->Gl) {
+  if (!ostate_init(S, P)) {
     rc = PDOT_ERR_OUT_OF_MEMORY;
     goto cleanup;
   }
@@ -708,12 +726,7 @@ int pdot_oracle_optimize(const pdot_problem* P, const pdot_pdhg_parameters* prm,
   rc = PDOT_OK;
 
 cleanup:
-  free(S->R.colbuf);
-  free(S->X); free(S->G); free(S->Xa); free(S->Ga); free(S->dX); free(S->Xl); free(S->Gl);
-  free(S->u); free(S->r); free(S->ua); free(S->ra); free(S->nu); free(S->du); free(S->dr);
-  free(S->nr); free(S->ul); free(S->rl); free(S->viol_s);
-  free(S->v); free(S->c); free(S->va); free(S->ca); free(S->nv); free(S->dv); free(S->dc);
-  free(S->nc); free(S->vl); free(S->cl); free(S->viol_t);
+  ostate_free(S);
   return rc;
 }
 
@@ -759,6 +772,38 @@ void pdot_oracle_primal_pass(i64 m, i64 n, const double* C, double* X, double* X
   *dsq = s;
   free(colsq);
   free(d);
+}
+
+/*
+ * CPU baseline timing: `steps` iterations of take_step! (the per-iteration
+ * work of optimize()'s loop, src/solver_gpu.jl:290-367) from the initial
+ * state, with all OpenMP threads; returns the elapsed seconds (evaluations,
+ * one per termination_evaluation_frequency iterations, are not included).
+ */
+int pdot_oracle_time_steps(const pdot_problem* P, const pdot_pdhg_parameters* prm, int steps,
+                           int num_threads, double* seconds) {
+  int rc = pdot_oracle_validate(P, prm);
+  if (rc != PDOT_OK) return rc;
+#ifdef _OPENMP
+  if (num_threads > 0) omp_set_num_threads(num_threads);
+#else
+  (void)num_threads;
+#endif
+  ostate St;
+  ostate* S = &St;
+  if (!ostate_init(S, P)) return PDOT_ERR_OUT_OF_MEMORY;
+  S->step_size = prm->step_size_policy == PDOT_STEP_SIZE_ADAPTIVE ? 1.0 : 0.8 / sqrt((double)(S->m + S->n));
+  S->primal_weight = prm->primal_importance;
+  const double t0 = now_sec();
+  for (int k = 0; k < steps; ++k) {
+    if (prm->step_size_policy == PDOT_STEP_SIZE_ADAPTIVE)
+      take_step_adaptive(S, prm->reduction_exponent, prm->growth_exponent);
+    else
+      take_step_constant(S);
+  }
+  *seconds = now_sec() - t0;
+  ostate_free(S);
+  return PDOT_OK;
 }
 
 int pdot_oracle_version(void) { return PDOT_ABI_VERSION; }

@@ -83,6 +83,8 @@ struct DevState {
   unsigned long long eval_t0_ns;
   double eval_time_sec;      // device time spent in evaluations
   long long num_stats;       // iteration-stats records written
+  long long primal_passes;   // fused primal passes that ran
+  long long fresh_passes;    // of those, passes that started a new average
   int numerical_error;
   int g_is_zero;             // the stored gradient is still its initial 0
   int done;
@@ -140,6 +142,8 @@ Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device);
 size_t workspace_doubles(const Geometry& g);
 
 cudaError_t launch_init(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
+cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s);
+cudaError_t launch_dual(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
 cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
 cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
 

@@ -131,22 +131,56 @@ pdot::SolveConfig make_config(const pdot_pdhg_parameters& p) {
   return c;
 }
 
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+int64_t pass_workspace_bytes(const pdot::Geometry& g) {
+  return (int64_t)((((size_t)g.grid + g.panels) * pdot::kPanelRows + (size_t)g.panels * g.n + g.grid) *
+                   sizeof(double));
+}
+
 constexpr int kRingCap = 4096;
 constexpr int kInFlight = 2;
 
-// Device memory and launch state of one solve.
-class Solve {
+enum TimedKind { kTimedPrimal = 0, kTimedDual = 1, kTimedEval = 2 };
+
+struct TimedLaunch {
+  cudaEvent_t start, stop;
+  int kind;
+};
+
+// Device memory and launch state of one problem and its optimize() loop.
+class Solver {
  public:
-  Solve(int device, int64_t m, int64_t n) : device_(device) {
-    CK(cudaSetDevice(device));
-    g_ = pdot::make_geometry(m, n, 1, device);
+  Solver(const pdot_problem& P, bool device_inputs, const pdot_pdhg_parameters& prm,
+         const pdot_solver_options* opt)
+      : device_(opt ? opt->device : 0),
+        use_graph_(opt ? opt->use_cuda_graph != 0 : true),
+        time_kernels_(opt ? opt->time_kernels != 0 : false),
+        params_(prm) {
+    CK(cudaSetDevice(device_));
+    const int64_t m = P.num_row, n = P.num_col;
+    g_ = pdot::make_geometry(m, n, 1, device_);
+    if (device_inputs && !(aligned16(P.cost_matrix))) g_ = pdot::make_geometry(m, n, 0, device_);
     const size_t N = (size_t)m * (size_t)n;
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-    alloc(&C_, N);
+    if (device_inputs) {
+      C_ = P.cost_matrix;
+      a_ = P.source_distribution;
+      b_ = P.target_distribution;
+    } else {
+      double *C = nullptr, *a = nullptr, *b = nullptr;
+      alloc(&C, N);
+      alloc(&a, m);
+      alloc(&b, n);
+      CK(cudaMemcpyAsync(C, P.cost_matrix, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
+      CK(cudaMemcpyAsync(a, P.source_distribution, m * sizeof(double), cudaMemcpyHostToDevice, stream_));
+      CK(cudaMemcpyAsync(b, P.target_distribution, n * sizeof(double), cudaMemcpyHostToDevice, stream_));
+      C_ = C;
+      a_ = a;
+      b_ = b;
+    }
     alloc(&X_[0], N);
     alloc(&X_[1], N);
-    alloc(&a_, m);
-    alloc(&b_, n);
     for (int k = 0; k < 2; ++k) {
       alloc(&u_[k], m);
       alloc(&r_[k], m);
@@ -192,80 +226,96 @@ class Solve {
     B_.ring = ring_;
     B_.ring_cap = kRingCap;
     B_.st = st_;
+
+    cfg_ = make_config(prm);
+    freq_ = prm.termination_evaluation_frequency;
+    limit_ = prm.termination_criteria.iteration_limit;
+    if (use_graph_ && !time_kernels_) capture_regular_chunk();
+    reset();
   }
 
-  ~Solve() {
-    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  ~Solver() {
     if (stream_) cudaStreamSynchronize(stream_);
-    for (int k = 0; k < kInFlight; ++k)
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    for (int k = 0; k < kInFlight; ++k) {
       if (ev_[k]) cudaEventDestroy(ev_[k]);
+      for (TimedLaunch& t : timed_[k]) {
+        cudaEventDestroy(t.start);
+        cudaEventDestroy(t.stop);
+      }
+    }
+    for (TimedLaunch& t : spare_) {
+      cudaEventDestroy(t.start);
+      cudaEventDestroy(t.stop);
+    }
     if (host_status_) cudaFreeHost(host_status_);
     for (void* p : allocs_) cudaFree(p);
     if (stream_) cudaStreamDestroy(stream_);
   }
 
-  void upload(const pdot_problem& P) {
+  cudaStream_t stream() const { return stream_; }
+
+  // CuPdhgSolverState starts at zero (src/solver_gpu.jl:428-441); the average
+  // halves need no clearing: the first accepted step overwrites them.
+  void reset() {
+    CK(cudaSetDevice(device_));
+    CK(cudaStreamSynchronize(stream_));
     const size_t N = (size_t)g_.m * (size_t)g_.n;
-    CK(cudaMemcpyAsync(C_, P.cost_matrix, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(a_, P.source_distribution, g_.m * sizeof(double), cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(b_, P.target_distribution, g_.n * sizeof(double), cudaMemcpyHostToDevice, stream_));
-    // CuPdhgSolverState starts at zero (src/solver_gpu.jl:428-441); the
-    // average halves need no clearing: the first accepted step overwrites them.
     CK(cudaMemsetAsync(X_[0], 0, N * sizeof(double), stream_));
     CK(cudaMemsetAsync(u_[0], 0, g_.m * sizeof(double), stream_));
     CK(cudaMemsetAsync(r_[0], 0, g_.m * sizeof(double), stream_));
     CK(cudaMemsetAsync(v_[0], 0, g_.n * sizeof(double), stream_));
     CK(cudaMemsetAsync(c_[0], 0, g_.n * sizeof(double), stream_));
     CK(cudaMemsetAsync(st_, 0, sizeof(pdot::DevState), stream_));
+    CK(pdot::launch_init(B_, g_, cfg_, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(&status_, st_, sizeof(status_), cudaMemcpyDeviceToHost));
+    host_it_ = 1;
+    drained_ = 0;
+    records_.clear();
+    primal_ms_ = dual_ms_ = eval_ms_ = 0.0;
+    timed_primal_ = 0;
   }
 
-  void run(const pdot_pdhg_parameters& prm, bool use_graph, pdot_saddle_point_output* out) {
-    cfg_ = make_config(prm);
-    freq_ = prm.termination_evaluation_frequency;
-    limit_ = prm.termination_criteria.iteration_limit;
-    CK(pdot::launch_init(B_, g_, cfg_, stream_));
-    if (use_graph) capture_regular_chunk();
-
-    long long host_it = 1;
-    long long drained = 0;
+  void iterate(int64_t max_iterations) {
+    CK(cudaSetDevice(device_));
+    int64_t remaining = max_iterations;
     int issued = 0, completed = 0;
-    std::vector<pdot_iteration_stats> records;
-    pdot::DevState s{};
-    // keep kInFlight chunks queued; stop when the device reports `done`
-    for (;;) {
-      while (issued - completed < kInFlight) {
-        enqueue_chunk(host_it, use_graph);
-        CK(cudaMemcpyAsync(&host_status_[issued % kInFlight], st_, sizeof(pdot::DevState),
-                           cudaMemcpyDeviceToHost, stream_));
-        CK(cudaEventRecord(ev_[issued % kInFlight], stream_));
+    while (!status_.done && (remaining > 0 || issued > completed)) {
+      while (issued - completed < kInFlight && remaining > 0 && !status_.done) {
+        const int slot = issued % kInFlight;
+        remaining -= enqueue_chunk(remaining, slot);
+        CK(cudaMemcpyAsync(&host_status_[slot], st_, sizeof(pdot::DevState), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaEventRecord(ev_[slot], stream_));
         ++issued;
       }
-      CK(cudaEventSynchronize(ev_[completed % kInFlight]));
-      s = host_status_[completed % kInFlight];
+      const int slot = completed % kInFlight;
+      CK(cudaEventSynchronize(ev_[slot]));
+      status_ = host_status_[slot];
+      collect_timings(slot);
       ++completed;
-      drain(s, drained, records);
-      if (s.done) break;
-      if (s.numerical_error) {
+      drain();
+      if (status_.done) break;
+      if (status_.numerical_error) {
         // The step kernels stop once a numerical error is flagged; the next
         // evaluation terminates (src/solver_gpu.jl:529-533,594-596).
-        CK(cudaStreamSynchronize(stream_));
-        CK(cudaMemcpy(&s, st_, sizeof(s), cudaMemcpyDeviceToHost));
-        if (!s.done) {
+        sync_all(issued, completed);
+        if (!status_.done) {
           CK(pdot::launch_eval(B_, g_, cfg_, stream_));
           CK(cudaStreamSynchronize(stream_));
-          CK(cudaMemcpy(&s, st_, sizeof(s), cudaMemcpyDeviceToHost));
+          CK(cudaMemcpy(&status_, st_, sizeof(status_), cudaMemcpyDeviceToHost));
+          drain();
         }
-        drain(s, drained, records);
         break;
       }
     }
-    CK(cudaStreamSynchronize(stream_));
-    CK(cudaMemcpy(&s, st_, sizeof(s), cudaMemcpyDeviceToHost));
-    drain(s, drained, records);
-    if (!s.done) fail(PDOT_ERR_CUDA, "solver stopped without a termination reason");
+    sync_all(issued, completed);
+  }
 
+  void finish(pdot_saddle_point_output* out) {
+    while (!status_.done) iterate(int64_t(1) << 40);
     // gpu_to_cpu!, src/io.jl:41-53 (average, or current if no average exists)
-    const int xb = s.out_current ? s.buf : (s.buf ^ 1);
+    const int xb = status_.out_current ? status_.buf : (status_.buf ^ 1);
     const size_t N = (size_t)g_.m * (size_t)g_.n;
     if (out->primal_solution)
       CK(cudaMemcpy(out->primal_solution, X_[xb], N * sizeof(double), cudaMemcpyDeviceToHost));
@@ -273,20 +323,38 @@ class Solve {
       CK(cudaMemcpy(out->dual_source_solution, u_[xb], g_.m * sizeof(double), cudaMemcpyDeviceToHost));
     if (out->dual_target_solution)
       CK(cudaMemcpy(out->dual_target_solution, v_[xb], g_.n * sizeof(double), cudaMemcpyDeviceToHost));
-    out->termination_reason = s.termination_reason;
-    out->iteration_count = (int32_t)(s.iteration - 1);
-    out->iteration_stats_count = (int64_t)records.size();
+    out->termination_reason = status_.termination_reason;
+    out->iteration_count = (int32_t)(status_.iteration - 1);
+    out->iteration_stats_count = (int64_t)records_.size();
     if (out->iteration_stats) {
-      const int64_t k = std::min<int64_t>((int64_t)records.size(), out->iteration_stats_capacity);
-      for (int64_t i = 0; i < k; ++i) out->iteration_stats[i] = records[i];
+      const int64_t k = std::min<int64_t>((int64_t)records_.size(), out->iteration_stats_capacity);
+      for (int64_t i = 0; i < k; ++i) out->iteration_stats[i] = records_[i];
     }
     memset(&out->final_stats, 0, sizeof(out->final_stats));
-    if (!records.empty()) {
-      out->final_stats = records.back();
-      out->solve_time_sec = records.back().cumulative_time_sec;
+    if (!records_.empty()) {
+      out->final_stats = records_.back();
+      out->solve_time_sec = records_.back().cumulative_time_sec;
     } else {
       out->solve_time_sec = 0.0;  // invalid problem: no evaluation ran
     }
+  }
+
+  void fill_status(pdot_solver_status* s) const {
+    memset(s, 0, sizeof(*s));
+    s->iteration = status_.iteration;
+    s->total_number_iterations = status_.total_iters;
+    s->done = status_.done;
+    s->termination_reason = status_.termination_reason;
+    s->step_size = status_.step_size;
+    s->primal_weight = status_.primal_weight;
+    s->cumulative_kkt_matrix_passes = status_.kkt_passes;
+    s->iteration_stats_count = (int64_t)records_.size();
+    s->primal_passes = status_.primal_passes;
+    s->primal_passes_fresh_average = status_.fresh_passes;
+    s->timed_primal_passes = timed_primal_;
+    s->primal_pass_ms = primal_ms_;
+    s->dual_step_ms = dual_ms_;
+    s->evaluation_ms = eval_ms_;
   }
 
  private:
@@ -303,30 +371,87 @@ class Solve {
   // A chunk starting here may be the captured graph: evaluation at its first
   // iteration only, and no forced evaluation (iteration_limit + 1) inside.
   bool regular_start(long long it) const {
-    if (it <= 10 || (it - 1) % freq_ != 0) return false;
+    if (!graph_exec_ || it <= 10 || (it - 1) % freq_ != 0) return false;
     for (long long k = it + 1; k < it + freq_; ++k)
       if (is_eval(k)) return false;
     return true;
   }
 
-  void enqueue_iteration(long long it) {
-    if (is_eval(it)) CK(pdot::launch_eval(B_, g_, cfg_, stream_));
-    CK(pdot::launch_step(B_, g_, cfg_, stream_));
+  TimedLaunch take_timer(int kind) {
+    TimedLaunch t;
+    if (!spare_.empty()) {
+      t = spare_.back();
+      spare_.pop_back();
+    } else {
+      CK(cudaEventCreate(&t.start));
+      CK(cudaEventCreate(&t.stop));
+    }
+    t.kind = kind;
+    return t;
   }
 
-  void enqueue_chunk(long long& it, bool use_graph) {
-    if (use_graph && graph_exec_ && regular_start(it)) {
-      CK(cudaGraphLaunch(graph_exec_, stream_));
-      it += freq_;
+  template <typename L>
+  void timed(int slot, int kind, L&& launch) {
+    if (!time_kernels_) {
+      CK(launch());
       return;
     }
-    // direct launches up to the next regular chunk (at most freq iterations)
-    long long k = 0;
+    TimedLaunch t = take_timer(kind);
+    CK(cudaEventRecord(t.start, stream_));
+    CK(launch());
+    CK(cudaEventRecord(t.stop, stream_));
+    timed_[slot].push_back(t);
+  }
+
+  void enqueue_iteration(long long it, int slot) {
+    if (is_eval(it)) timed(slot, kTimedEval, [&] { return pdot::launch_eval(B_, g_, cfg_, stream_); });
+    timed(slot, kTimedPrimal, [&] { return pdot::launch_primal(B_, g_, stream_); });
+    timed(slot, kTimedDual, [&] { return pdot::launch_dual(B_, g_, cfg_, stream_); });
+  }
+
+  // Enqueues up to `budget` loop bodies starting at host_it_; returns how many.
+  int64_t enqueue_chunk(int64_t budget, int slot) {
+    if (regular_start(host_it_) && budget >= freq_) {
+      CK(cudaGraphLaunch(graph_exec_, stream_));
+      host_it_ += freq_;
+      return freq_;
+    }
+    int64_t k = 0;
     do {
-      enqueue_iteration(it);
-      ++it;
+      enqueue_iteration(host_it_, slot);
+      ++host_it_;
       ++k;
-    } while (k < freq_ && !(use_graph && graph_exec_ && regular_start(it)));
+    } while (k < freq_ && k < budget && !regular_start(host_it_));
+    return k;
+  }
+
+  void collect_timings(int slot) {
+    for (TimedLaunch& t : timed_[slot]) {
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, t.start, t.stop));
+      if (t.kind == kTimedPrimal) {
+        primal_ms_ += ms;
+        ++timed_primal_;
+      } else if (t.kind == kTimedDual) {
+        dual_ms_ += ms;
+      } else {
+        eval_ms_ += ms;
+      }
+      spare_.push_back(t);
+    }
+    timed_[slot].clear();
+  }
+
+  void sync_all(int issued, int& completed) {
+    while (completed < issued) {
+      const int slot = completed % kInFlight;
+      CK(cudaEventSynchronize(ev_[slot]));
+      collect_timings(slot);
+      ++completed;
+    }
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(&status_, st_, sizeof(status_), cudaMemcpyDeviceToHost));
+    drain();
   }
 
   void capture_regular_chunk() {
@@ -342,30 +467,37 @@ class Solve {
     CK(e3);
   }
 
-  void drain(const pdot::DevState& s, long long& drained, std::vector<pdot_iteration_stats>& recs) {
-    const long long total = s.num_stats;
-    if (total <= drained) return;
-    if (total - drained > kRingCap) fail(PDOT_ERR_CUDA, "iteration-stats ring overflow");
-    std::vector<pdot_iteration_stats> tmp((size_t)(total - drained));
-    for (long long k = drained; k < total; ++k) {
-      CK(cudaMemcpy(&tmp[(size_t)(k - drained)], ring_ + (k % kRingCap), sizeof(pdot_iteration_stats),
-                    cudaMemcpyDeviceToHost));
+  void drain() {
+    const long long total = status_.num_stats;
+    if (total <= drained_) return;
+    if (total - drained_ > kRingCap) fail(PDOT_ERR_CUDA, "iteration-stats ring overflow");
+    for (long long k = drained_; k < total; ++k) {
+      pdot_iteration_stats rec;
+      CK(cudaMemcpy(&rec, ring_ + (k % kRingCap), sizeof(rec), cudaMemcpyDeviceToHost));
+      records_.push_back(rec);
     }
-    recs.insert(recs.end(), tmp.begin(), tmp.end());
-    drained = total;
+    drained_ = total;
   }
 
   int device_;
+  bool use_graph_, time_kernels_;
+  pdot_pdhg_parameters params_;
   pdot::Geometry g_{};
   pdot::SolveConfig cfg_{};
   long long freq_ = 128, limit_ = 0;
+  long long host_it_ = 1, drained_ = 0;
   cudaStream_t stream_ = nullptr;
   cudaEvent_t ev_[kInFlight] = {};
   cudaGraphExec_t graph_exec_ = nullptr;
+  std::vector<TimedLaunch> timed_[kInFlight];
+  std::vector<TimedLaunch> spare_;
+  double primal_ms_ = 0.0, dual_ms_ = 0.0, eval_ms_ = 0.0;
+  long long timed_primal_ = 0;
   std::vector<void*> allocs_;
-  double* C_ = nullptr;
+  const double* C_ = nullptr;
+  const double* a_ = nullptr;
+  const double* b_ = nullptr;
   double* X_[2] = {};
-  double *a_ = nullptr, *b_ = nullptr;
   double* u_[2] = {};
   double* v_[2] = {};
   double* r_[2] = {};
@@ -374,15 +506,11 @@ class Solve {
   pdot::DevState* st_ = nullptr;
   pdot_iteration_stats* ring_ = nullptr;
   pdot::DevState* host_status_ = nullptr;
+  pdot::DevState status_{};
+  std::vector<pdot_iteration_stats> records_;
   pdot::Buffers B_{};
 };
 
-bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
-
-int64_t pass_workspace_bytes(const pdot::Geometry& g) {
-  return (int64_t)((((size_t)g.grid + g.panels) * pdot::kPanelRows + (size_t)g.panels * g.n + g.grid) *
-                   sizeof(double));
-}
 
 }  // namespace
 
@@ -423,13 +551,67 @@ int pdot_optimize(const pdot_problem* problem, const pdot_pdhg_parameters* param
   return guarded([&] {
     validate(problem, params);
     if (!output) fail(PDOT_ERR_INVALID_ARGUMENT, "null output");
-    const int device = options ? options->device : 0;
-    const bool use_graph = options ? options->use_cuda_graph != 0 : true;
-    require_sm100(device);
-    Solve solve(device, problem->num_row, problem->num_col);
-    solve.upload(*problem);
-    solve.run(*params, use_graph, output);
+    require_sm100(options ? options->device : 0);
+    Solver solver(*problem, false, *params, options);
+    solver.finish(output);
   });
+}
+
+struct pdot_solver {
+  Solver* impl;
+};
+
+static int create_solver(const pdot_problem* problem, const pdot_pdhg_parameters* params,
+                         const pdot_solver_options* options, pdot_solver** out, bool device_inputs) {
+  return guarded([&] {
+    validate(problem, params);
+    if (!out) fail(PDOT_ERR_INVALID_ARGUMENT, "null solver handle");
+    *out = nullptr;
+    require_sm100(options ? options->device : 0);
+    Solver* s = new Solver(*problem, device_inputs, *params, options);
+    *out = new pdot_solver{s};
+  });
+}
+
+int pdot_solver_create(const pdot_problem* problem, const pdot_pdhg_parameters* params,
+                       const pdot_solver_options* options, pdot_solver** solver) {
+  return create_solver(problem, params, options, solver, false);
+}
+
+int pdot_solver_create_device(const pdot_problem* device_problem, const pdot_pdhg_parameters* params,
+                              const pdot_solver_options* options, pdot_solver** solver) {
+  return create_solver(device_problem, params, options, solver, true);
+}
+
+int pdot_solver_reset(pdot_solver* solver) {
+  return guarded([&] {
+    if (!solver) fail(PDOT_ERR_INVALID_ARGUMENT, "null solver");
+    solver->impl->reset();
+  });
+}
+
+int pdot_solver_iterate(pdot_solver* solver, int64_t max_iterations, pdot_solver_status* status) {
+  return guarded([&] {
+    if (!solver) fail(PDOT_ERR_INVALID_ARGUMENT, "null solver");
+    if (max_iterations < 0) fail(PDOT_ERR_INVALID_ARGUMENT, "negative iteration count");
+    solver->impl->iterate(max_iterations);
+    if (status) solver->impl->fill_status(status);
+  });
+}
+
+int pdot_solver_finish(pdot_solver* solver, pdot_saddle_point_output* output) {
+  return guarded([&] {
+    if (!solver || !output) fail(PDOT_ERR_INVALID_ARGUMENT, "null solver or output");
+    solver->impl->finish(output);
+  });
+}
+
+void* pdot_solver_stream(pdot_solver* solver) { return solver ? (void*)solver->impl->stream() : nullptr; }
+
+void pdot_solver_destroy(pdot_solver* solver) {
+  if (!solver) return;
+  delete solver->impl;
+  delete solver;
 }
 
 int64_t pdot_primal_pass_workspace_bytes(int64_t m, int64_t n) {

@@ -317,6 +317,7 @@ __device__ void step_control(DevState* st, const SolveConfig& cfg, double dot_r,
                              double dy2) {
   const double omega = st->primal_weight;
   const double weight = st->step_size;
+  const bool fresh = !(st->sum_weights > 0.0);
   bool accepted = true;
   if (cfg.adaptive) {
     const double interaction = fabs(dot_r + dot_c);
@@ -360,6 +361,8 @@ __device__ void step_control(DevState* st, const SolveConfig& cfg, double dot_r,
     st->avg_count += 1;
     st->g_is_zero = 0;
   }
+  st->primal_passes += 1;
+  st->fresh_passes += fresh ? 1 : 0;
   st->iteration += 1;
 }
 
@@ -837,6 +840,8 @@ __global__ void __launch_bounds__(kThreads, 2) k0_init(Buffers B, Geometry g, So
       st->buf = 0;
       st->out_current = 1;
       st->num_stats = 0;
+      st->primal_passes = 0;
+      st->fresh_passes = 0;
       st->eval_time_sec = 0.0;
       st->done = 0;
       st->termination_reason = 0;
@@ -896,13 +901,23 @@ cudaError_t launch_init(const Buffers& B, const Geometry& g, const SolveConfig& 
   return cudaGetLastError();
 }
 
-cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s) {
+cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s) {
   if (g.vec == 2)
     k1_primal<2><<<g.grid, kThreads, 0, s>>>(B, g);
   else
     k1_primal<1><<<g.grid, kThreads, 0, s>>>(B, g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dual(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s) {
   k2_dual<<<g.row_blocks + g.col_blocks, kVecThreads, 0, s>>>(B, g, cfg);
   return cudaGetLastError();
+}
+
+cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s) {
+  cudaError_t e = launch_primal(B, g, s);
+  if (e != cudaSuccess) return e;
+  return launch_dual(B, g, cfg, s);
 }
 
 cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s) {

@@ -26,6 +26,7 @@ from .api import (  # noqa: F401
     RestartToCurrentMetric,
     SaddlePointOutput,
     SolveLog,
+    Solver,
     TerminationCriteria,
     TerminationReason,
     construct_restart_parameters,

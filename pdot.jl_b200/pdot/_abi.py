@@ -72,7 +72,27 @@ class SolverOptionsC(ct.Structure):
     _fields_ = [
         ("device", ct.c_int32),
         ("use_cuda_graph", ct.c_int32),
-        ("reserved", ct.c_int32 * 14),
+        ("time_kernels", ct.c_int32),
+        ("reserved", ct.c_int32 * 13),
+    ]
+
+
+class SolverStatusC(ct.Structure):
+    _fields_ = [
+        ("iteration", ct.c_int64),
+        ("total_number_iterations", ct.c_int64),
+        ("done", ct.c_int32),
+        ("termination_reason", ct.c_int32),
+        ("step_size", ct.c_double),
+        ("primal_weight", ct.c_double),
+        ("cumulative_kkt_matrix_passes", ct.c_double),
+        ("iteration_stats_count", ct.c_int64),
+        ("primal_passes", ct.c_int64),
+        ("primal_passes_fresh_average", ct.c_int64),
+        ("timed_primal_passes", ct.c_int64),
+        ("primal_pass_ms", ct.c_double),
+        ("dual_step_ms", ct.c_double),
+        ("evaluation_ms", ct.c_double),
     ]
 
 
@@ -153,6 +173,19 @@ SIGNATURES = {
          ct.POINTER(SaddlePointOutputC)],
     ),
     "pdot_default_parameters": (None, [_D, ct.POINTER(PdhgParametersC)]),
+    "pdot_solver_create": (
+        ct.c_int,
+        [ct.POINTER(ProblemC), ct.POINTER(PdhgParametersC), ct.POINTER(SolverOptionsC), ct.POINTER(_P)],
+    ),
+    "pdot_solver_create_device": (
+        ct.c_int,
+        [ct.POINTER(ProblemC), ct.POINTER(PdhgParametersC), ct.POINTER(SolverOptionsC), ct.POINTER(_P)],
+    ),
+    "pdot_solver_reset": (ct.c_int, [_P]),
+    "pdot_solver_iterate": (ct.c_int, [_P, _I64, ct.POINTER(SolverStatusC)]),
+    "pdot_solver_finish": (ct.c_int, [_P, ct.POINTER(SaddlePointOutputC)]),
+    "pdot_solver_stream": (_P, [_P]),
+    "pdot_solver_destroy": (None, [_P]),
     "pdot_primal_pass_workspace_bytes": (_I64, [_I64, _I64]),
     "pdot_primal_pass_f64": (
         ct.c_int,

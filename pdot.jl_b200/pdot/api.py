@@ -357,6 +357,14 @@ def validate(params: PdhgParameters) -> None:
 
 
 # ---------------------------------------------------------------- optimize
+def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False) -> _abi.SolverOptionsC:
+    opts = _abi.SolverOptionsC()
+    opts.device = device
+    opts.use_cuda_graph = 1 if use_cuda_graph else 0
+    opts.time_kernels = 1 if time_kernels else 0
+    return opts
+
+
 def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device: int = 0,
              use_cuda_graph: bool = True) -> SaddlePointOutput:
     """PDOT.optimize, src/solver_gpu.jl:413-720, run by libpdot.so on the GPU."""
@@ -364,10 +372,75 @@ def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device
     lib = _abi.load()
     mp = MarshalledProblem(problem)
     cp = marshal_params(params)
-    opts = _abi.SolverOptionsC()
-    opts.device = device
-    opts.use_cuda_graph = 1 if use_cuda_graph else 0
+    opts = _options(device, use_cuda_graph)
     ob = OutputBuffers(mp.m, mp.n, stats_capacity_for(params))
     rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
     _abi.check(lib, rc, "pdot_optimize")
     return ob.to_output()
+
+
+class Solver:
+    """A problem resident on the GPU plus the state of optimize()'s loop
+    (pdot_solver in include/pdot.h). `problem` is an OptimalTransportProblem
+    (copied to the device), or `device_problem` a tuple (m, n, cost_ptr,
+    source_ptr, target_ptr) of device pointers read in place."""
+
+    def __init__(self, params: PdhgParameters, problem: Optional[OptimalTransportProblem] = None, *,
+                 device_problem=None, device: int = 0, use_cuda_graph: bool = True,
+                 time_kernels: bool = False):
+        validate(params)
+        self._lib = _abi.load()
+        self._params = params
+        self._cp = marshal_params(params)
+        opts = _options(device, use_cuda_graph, time_kernels)
+        handle = ct.c_void_p()
+        if device_problem is not None:
+            m, n, cptr, aptr, bptr = device_problem
+            pc = _abi.ProblemC(m, n, ct.cast(ct.c_void_p(cptr), ct.POINTER(ct.c_double)),
+                               ct.cast(ct.c_void_p(aptr), ct.POINTER(ct.c_double)),
+                               ct.cast(ct.c_void_p(bptr), ct.POINTER(ct.c_double)))
+            rc = self._lib.pdot_solver_create_device(ct.byref(pc), ct.byref(self._cp), ct.byref(opts),
+                                                     ct.byref(handle))
+            self.m, self.n = m, n
+        else:
+            mp = MarshalledProblem(problem)
+            rc = self._lib.pdot_solver_create(ct.byref(mp.c), ct.byref(self._cp), ct.byref(opts),
+                                              ct.byref(handle))
+            self.m, self.n = mp.m, mp.n
+        _abi.check(self._lib, rc, "pdot_solver_create")
+        self._h = handle
+
+    def reset(self) -> None:
+        _abi.check(self._lib, self._lib.pdot_solver_reset(self._h), "pdot_solver_reset")
+
+    def iterate(self, iterations: int) -> dict:
+        st = _abi.SolverStatusC()
+        _abi.check(self._lib, self._lib.pdot_solver_iterate(self._h, int(iterations), ct.byref(st)),
+                   "pdot_solver_iterate")
+        return {f: getattr(st, f) for f, _ in st._fields_}
+
+    def finish(self) -> SaddlePointOutput:
+        ob = OutputBuffers(self.m, self.n, stats_capacity_for(self._params))
+        _abi.check(self._lib, self._lib.pdot_solver_finish(self._h, ct.byref(ob.c)), "pdot_solver_finish")
+        return ob.to_output()
+
+    @property
+    def stream(self) -> int:
+        return int(self._lib.pdot_solver_stream(self._h) or 0)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.pdot_solver_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

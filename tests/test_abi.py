@@ -48,6 +48,7 @@ STRUCTS = {
     "pdot_restart_parameters": _abi.RestartParametersC,
     "pdot_pdhg_parameters": _abi.PdhgParametersC,
     "pdot_solver_options": _abi.SolverOptionsC,
+    "pdot_solver_status": _abi.SolverStatusC,
     "pdot_convergence_information": _abi.ConvergenceInformationC,
     "pdot_iteration_stats": _abi.IterationStatsC,
     "pdot_saddle_point_output": _abi.SaddlePointOutputC,

@@ -281,6 +281,24 @@ int pdot_primal_pass_f64(int64_t m, int64_t n,
                          double* delta_row_sum, double* delta_col_sum, double* delta_sq_norm,
                          void* workspace, int64_t workspace_bytes, void* stream);
 
+/* The same fused primal pass for callers that cannot allocate device memory
+ * (a host framework that hands out its whole memory budget from its own pool,
+ * or a latency-critical loop that cannot afford cudaMalloc's implicit device
+ * synchronisation). It has no counterpart in the reference. Its scratch is a
+ * fixed PDOT_NOALLOC_SCRATCH_BYTES array inside the library (held by every GPU
+ * that loads it until exit), so the call allocates nothing; sizes whose
+ * scratch would exceed it return PDOT_ERR_TOO_LARGE. The first call on a
+ * device looks up the array's device address: make it before any stream
+ * capture. Calls share the array: calls that overlap on the GPU race. */
+#define PDOT_NOALLOC_SCRATCH_BYTES (16u << 20)
+int pdot_primal_pass_f64_noalloc(int64_t m, int64_t n,
+                                 const double* cost, double* primal, double* primal_avg,
+                                 const double* dual_source, const double* dual_target,
+                                 double step_over_weight, double avg_new_weight, double avg_scale,
+                                 int32_t flags,
+                                 double* delta_row_sum, double* delta_col_sum, double* delta_sq_norm,
+                                 void* stream);
+
 #ifdef __cplusplus
 }
 #endif

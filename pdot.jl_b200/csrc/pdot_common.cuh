@@ -147,6 +147,9 @@ cudaError_t launch_dual(const Buffers& B, const Geometry& g, const SolveConfig& 
 cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
 cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
 
+// Sets the thread-local text pdot_last_error() returns (pdot_host.cu).
+void set_last_error(const char* msg);
+
 // Stand-alone primal pass on caller buffers (pdot_primal_pass_f64).
 cudaError_t launch_primal_pass(const Geometry& g, const double* C, double* X, double* Xa,
                                const double* u, const double* v, double step_over_weight,

@@ -48,6 +48,14 @@ void check_cuda(cudaError_t e, const char* what, int line) {
 }
 #define CK(x) check_cuda((x), #x, __LINE__)
 
+}  // namespace
+
+namespace pdot {
+void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+}  // namespace pdot
+
+namespace {
+
 template <typename F>
 int guarded(F&& f) {
   try {

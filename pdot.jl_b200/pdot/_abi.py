@@ -26,6 +26,8 @@ PDOT_ERR_OUT_OF_MEMORY = -3
 PDOT_ERR_NO_DEVICE = -4
 PDOT_ERR_TOO_LARGE = -5
 
+NOALLOC_SCRATCH_BYTES = 16 << 20
+
 PDOT_PASS_ZERO_GRADIENT = 1
 PDOT_PASS_FIRST_AVERAGE = 2
 
@@ -187,6 +189,10 @@ SIGNATURES = {
     "pdot_solver_stream": (_P, [_P]),
     "pdot_solver_destroy": (None, [_P]),
     "pdot_primal_pass_workspace_bytes": (_I64, [_I64, _I64]),
+    "pdot_primal_pass_f64_noalloc": (
+        ct.c_int,
+        [_I64, _I64, _P, _P, _P, _P, _P, _D, _D, _D, _I32, _P, _P, _P, _P],
+    ),
     "pdot_primal_pass_f64": (
         ct.c_int,
         [_I64, _I64, _P, _P, _P, _P, _P, _D, _D, _D, _I32, _P, _P, _P, _P, _I64, _P],

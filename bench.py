@@ -28,6 +28,8 @@ import subprocess
 import sys
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 for _p in (os.path.join(ROOT, "pdot.jl_b200"), os.path.join(ROOT, "oracle")):
     if _p not in sys.path:
@@ -53,6 +55,11 @@ def parse():
     ap.add_argument("--n", type=int, default=N_COLS)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ttk", action="store_true", help="skip the time-to-KKT solve")
+    ap.add_argument("--no-mp", action="store_true", help="skip the mixed-precision variants")
+    ap.add_argument("--precision", choices=["f64", "f32"], default="f64",
+                    help="plan precision of the primary workload (f64: the drop-in)")
+    ap.add_argument("--cost", choices=["f64", "f32", "bf16", "sqeuclid"], default=None,
+                    help="cost source of the primary workload (default: f64, or f32 with --precision f32)")
     return ap.parse_args()
 
 
@@ -254,8 +261,102 @@ def run_reference(args, world, rank):
     return line
 
 
+def fp64_kkt_device(Ct, a, b, X_t, u, v):
+    """Relative L2 KKT error of a solution on the FP64 problem, on the device.
+    Ct is the (n, m) row-major view of C; X_t the plan in the same layout."""
+    import torch
+
+    pres = torch.sqrt(((a - X_t.sum(dim=0)) ** 2).sum() + ((b - X_t.sum(dim=1)) ** 2).sum()).item()
+    G = Ct - u[None, :] - v[:, None]
+    dres = torch.linalg.vector_norm(torch.clamp(G, max=0.0)).item()
+    del G
+    pobj = float((Ct * X_t).sum().item())
+    dobj = float((a @ u + b @ v).item())
+    rp = pres / (1 + math.sqrt(float((a @ a + b @ b).item())))
+    rd = dres / (1 + torch.linalg.vector_norm(Ct).item())
+    rg = abs(pobj - dobj) / (1 + abs(pobj) + abs(dobj))
+    return {"primal_objective": pobj, "relative_l2_primal_residual": rp, "relative_l2_dual_residual": rd,
+            "relative_optimality_gap": rg, "relative_kkt": max(rp, rd, rg)}
+
+
+def time_iterations(solver, warmup, steps, device):
+    import torch
+
+    s0 = solver.iterate(warmup)
+    stream = torch.cuda.ExternalStream(solver.stream, device=device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    s1 = solver.iterate(steps)
+    e1.record(stream)
+    e1.synchronize()
+    return s1["iteration"] - s0["iteration"], e0.elapsed_time(e1), s0, s1
+
+
+def run_mixed(args, params, m, n, Ct, a, b, xs_d, ys_d, device, local, fp64_obj):
+    """Mixed-precision variants: FP32 plan with the cost from FP32 or BF16
+    storage or computed from FP32 coordinates (16 B per entry)."""
+    import torch
+
+    import pdot
+
+    N = m * n
+    out = {}
+    dev_problem = (m, n, Ct.data_ptr(), a.data_ptr(), b.data_ptr())
+    pts = (xs_d.data_ptr(), ys_d.data_ptr(), xs_d.shape[1])
+    bytes_per_entry = {"sqeuclid": 16.0, "f32": 20.0, "bf16": 18.0}
+    for cost in ("sqeuclid", "f32", "bf16"):
+        kw = {"points": pts} if cost == "sqeuclid" else {}
+        prob = (m, n, 0, a.data_ptr(), b.data_ptr()) if cost == "sqeuclid" else dev_problem
+        solver = pdot.Solver(params, device_problem=prob, device=local, precision="f32", cost=cost, **kw)
+        iters, ms, _, _ = time_iterations(solver, args.warmup, args.steps, device)
+        entry = {"iters_per_sec": iters / (ms / 1000.0), "ms_per_iter": ms / max(iters, 1)}
+        if cost == "sqeuclid" and not args.no_ttk:
+            solver.reset()
+            stream = torch.cuda.ExternalStream(solver.stream, device=device)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            res = solver.finish()
+            e1.record(stream)
+            e1.synchronize()
+            X_t = torch.from_numpy(np.ascontiguousarray(res.primal_solution.T)).to(device)
+            u = torch.from_numpy(res.dual_source_solution).to(device)
+            v = torch.from_numpy(res.dual_target_solution).to(device)
+            k64 = fp64_kkt_device(Ct, a, b, X_t, u, v)
+            del X_t
+            entry["time_to_kkt"] = {"seconds": e0.elapsed_time(e1) / 1000.0, "iterations": res.iteration_count,
+                                    "termination": res.termination_string,
+                                    "internal_relative_gap":
+                                        res.iteration_stats[-1].convergence_information[0].relative_optimality_gap,
+                                    "fp64_evaluation": k64,
+                                    "objective_vs_fp64_solve": (k64["primal_objective"] - fp64_obj) / fp64_obj
+                                    if fp64_obj else None}
+        solver.close()
+        if cost == "sqeuclid":
+            ts = pdot.Solver(params, device_problem=prob, device=local, use_cuda_graph=False, time_kernels=True,
+                             precision="f32", cost=cost, **kw)
+            t0 = ts.iterate(args.warmup)
+            t1 = ts.iterate(min(args.steps, 200))
+            ts.close()
+            passes = t1["primal_passes"] - t0["primal_passes"]
+            fresh = t1["primal_passes_fresh_average"] - t0["primal_passes_fresh_average"]
+            k1_ms = t1["primal_pass_ms"] - t0["primal_pass_ms"]
+            launches = t1["timed_primal_passes"] - t0["timed_primal_passes"]
+            alg = N * (16.0 * (passes - fresh) + 12.0 * fresh) / max(passes, 1)
+            avg_s = k1_ms / 1000.0 / max(launches, 1)
+            peak, _ = read_peak()
+            entry["roofline"] = {"achieved": alg / avg_s / 1e9, "peak": peak, "unit": "GB/s",
+                                 "frac": alg / avg_s / 1e9 / peak, "algorithmic_bytes_per_launch": alg,
+                                 "avg_launch_ms": avg_s * 1000.0}
+        entry["bytes_per_entry"] = bytes_per_entry[cost]
+        out[cost] = entry
+    return out
+
+
 def run_ours(args, world, rank, local):
-    import numpy as np
     import torch
 
     import pdot
@@ -269,12 +370,26 @@ def run_ours(args, world, rank, local):
     a = torch.from_numpy(a_h).to(device)
     b = torch.from_numpy(b_h).to(device)
     torch.cuda.synchronize()
-    dev_problem = (m, n, Ct.data_ptr(), a.data_ptr(), b.data_ptr())
     params = pdot.default_parameters(TOL)
     params.termination_criteria.time_sec_limit = 300.0
+    precision = args.precision
+    cost = args.cost or ("f64" if precision == "f64" else "f32")
+    variant = {"precision": precision, "cost": cost}
+    xs_d = torch.from_numpy(xs.astype(np.float32)).to(device)
+    ys_d = torch.from_numpy(ys.astype(np.float32)).to(device)
+    if cost == "sqeuclid":
+        dev_problem = (m, n, 0, a.data_ptr(), b.data_ptr())
+        variant["points"] = (xs_d.data_ptr(), ys_d.data_ptr(), xs.shape[1])
+    else:
+        dev_problem = (m, n, Ct.data_ptr(), a.data_ptr(), b.data_ptr())
+    # algorithmic bytes per entry of the fused pass: read cost, plan, average;
+    # write plan, average (the average is not read after a reset)
+    xb = 8.0 if precision == "f64" else 4.0
+    cb = {"f64": 8.0, "f32": 4.0, "bf16": 2.0, "sqeuclid": 0.0}[cost]
+    full_bytes, fresh_bytes = cb + 4 * xb, cb + 3 * xb
 
     # ---- timed region: K iterations, problem resident, CUDA graphs ----
-    solver = pdot.Solver(params, device_problem=dev_problem, device=local)
+    solver = pdot.Solver(params, device_problem=dev_problem, device=local, **variant)
     s0 = solver.iterate(args.warmup)
     stream = torch.cuda.ExternalStream(solver.stream, device=device)
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -317,7 +432,7 @@ def run_ours(args, world, rank, local):
 
     # ---- per-launch kernel times (CUDA events around every launch) ----
     tsolver = pdot.Solver(params, device_problem=dev_problem, device=local, use_cuda_graph=False,
-                          time_kernels=True)
+                          time_kernels=True, **variant)
     t0 = tsolver.iterate(args.warmup)
     t1 = tsolver.iterate(args.steps)
     tsolver.close()
@@ -328,9 +443,7 @@ def run_ours(args, world, rank, local):
     k1_ms = t1["primal_pass_ms"] - t0["primal_pass_ms"]
     region_kernel_ms = (t1["primal_pass_ms"] + t1["dual_step_ms"] + t1["evaluation_ms"]
                         - t0["primal_pass_ms"] - t0["dual_step_ms"] - t0["evaluation_ms"])
-    # algorithmic bytes: read C, X, Xavg and write X, Xavg (8 B each in FP64);
-    # a pass that starts a new average does not read Xavg
-    alg_bytes = N * (40.0 * (passes - fresh) + 32.0 * fresh)
+    alg_bytes = N * (full_bytes * (passes - fresh) + fresh_bytes * fresh)
     per_launch_bytes = alg_bytes / max(passes, 1)
     k1_avg_s = k1_ms / 1000.0 / max(k1_launches, 1)
     achieved = per_launch_bytes / k1_avg_s / 1e9
@@ -342,23 +455,34 @@ def run_ours(args, world, rank, local):
     if not args.no_e2e:
         C_host = torch.empty((n, m), dtype=torch.float64, pin_memory=True)
         C_host.copy_(Ct)
-        prob = pdot.OptimalTransportProblem(C_host.numpy().T, a_h, b_h)
+        ekw = {"precision": precision, "cost": cost}
+        if cost == "sqeuclid":
+            prob = pdot.OptimalTransportProblem(None, a_h, b_h)
+            ekw["points"] = (xs.astype(np.float32), ys.astype(np.float32))
+        else:
+            prob = pdot.OptimalTransportProblem(C_host.numpy().T, a_h, b_h)
         eparams = pdot.default_parameters(TOL, iteration_limit=args.steps)
         torch.cuda.synchronize()
         barrier(world)
         w0 = time.perf_counter()
-        out = pdot.optimize(eparams, prob, device=local)
+        out = pdot.optimize(eparams, prob, device=local, **ekw)
         torch.cuda.synchronize()
         w1 = time.perf_counter()
         e_sec = max_over_ranks(w1 - w0, world, device)
         vec_bytes = 8 * (m + n)
+        h2d = (8 * (m + n) * xs.shape[1] // 2 if cost == "sqeuclid" else 8 * N) + vec_bytes
         e2e = {"value": world * out.iteration_count / e_sec, "unit": UNIT,
-               "h2d_bytes_per_step": (8 * N + vec_bytes) / max(out.iteration_count, 1),
+               "h2d_bytes_per_step": h2d / max(out.iteration_count, 1),
                "d2h_bytes_per_step": (8 * N + vec_bytes) / max(out.iteration_count, 1),
                "iterations_per_call": out.iteration_count, "seconds_per_call": e_sec,
                "note": "one pdot.optimize call: H2D of C, a, b from pinned memory, the solve, "
                        "D2H of the returned plan and duals; bytes amortised per iteration"}
         del C_host
+
+    mixed = None
+    if not args.no_mp and precision == "f64":
+        fp64_obj = ttk["primal_objective"] if ttk else None
+        mixed = run_mixed(args, params, m, n, Ct, a, b, xs_d, ys_d, device, local, fp64_obj)
 
     cpu = None
     if rank == 0 and world == 1:
@@ -368,20 +492,23 @@ def run_ours(args, world, rank, local):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": iters,
         "warmup": args.warmup, "ms_per_step": ms / max(iters, 1), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"PDHG-OT m={m} n={n} gauss-mixture(8, sigma 0.05) sq-euclid/max FP64 drop-in, "
-                               f"reference script parameters, tol {TOL}",
+        "scaling": "weak", "vs_baseline": None, "dtype": precision, "data": "synthetic",
+        "config": {"workload": f"PDHG-OT m={m} n={n} gauss-mixture(8, sigma 0.05) sq-euclid/max, "
+                               + ("FP64 drop-in" if precision == "f64" else f"FP32 plan, {cost} cost")
+                               + f", reference script parameters, tol {TOL}",
                    "l2": "inputs larger than L2 (C, X, Xavg = 7.2 GB), no flush",
                    "parallelism": "replicas" if world > 1 else "1 GPU",
                    "cuda_graph_chunks": True},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "k1_primal (fused primal pass)",
+                     "algorithmic_bytes_per_entry": full_bytes,
                      "algorithmic_bytes_per_launch": per_launch_bytes,
                      "avg_launch_ms": k1_avg_s * 1000.0, "launches_timed": k1_launches,
                      "share_of_kernel_time": k1_ms / region_kernel_ms if region_kernel_ms > 0 else None},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk.summary(), "time_to_kkt": ttk,
+        "mixed_precision": mixed,
     }
     return line
 

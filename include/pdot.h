@@ -81,7 +81,8 @@ enum { PDOT_STEP_SIZE_ADAPTIVE = 0, PDOT_STEP_SIZE_CONSTANT = 1 };
 typedef struct pdot_problem {
   int64_t num_row;                    /* m, number of sources */
   int64_t num_col;                    /* n, number of targets */
-  const double* cost_matrix;          /* m*n, column-major, ld = m (host memory) */
+  const double* cost_matrix;          /* m*n, column-major, ld = m (host memory);
+                                       * NULL with PDOT_COST_SQEUCLID_POINTS */
   const double* source_distribution;  /* m (host memory) */
   const double* target_distribution;  /* n (host memory) */
 } pdot_problem;
@@ -125,12 +126,28 @@ typedef struct pdot_pdhg_parameters {
 } pdot_pdhg_parameters;
 
 /* Options of this implementation that have no counterpart in the reference.
- * Pass NULL for the defaults (device 0, FP64 drop-in, CUDA graphs on). */
+ * Pass NULL for the defaults: device 0, the FP64 drop-in, CUDA graphs on. */
+enum { PDOT_PRECISION_F64 = 0, PDOT_PRECISION_F32 = 1 };
+enum {
+  PDOT_COST_F64 = 0,              /* the problem's FP64 cost matrix, as given */
+  PDOT_COST_F32 = 1,              /* stored in FP32 (converted on the device) */
+  PDOT_COST_BF16 = 2,             /* stored in BF16 (converted on the device) */
+  PDOT_COST_SQEUCLID_POINTS = 3   /* C_ij = scale*||x_i - y_j||^2 computed on the fly
+                                   * from FP32 coordinates; cost_matrix may be NULL */
+};
 typedef struct pdot_solver_options {
   int32_t device;                     /* CUDA device ordinal */
   int32_t use_cuda_graph;             /* 1: replay captured iteration chunks */
   int32_t time_kernels;               /* 1: CUDA events around every launch (direct launches) */
-  int32_t reserved[13];               /* must be zero */
+  int32_t plan_precision;             /* PDOT_PRECISION_F64 (drop-in) or _F32 (mixed precision) */
+  int32_t cost_storage;               /* PDOT_COST_*; anything but F64 needs plan_precision F32 */
+  int32_t point_dim;                  /* 1..4, for PDOT_COST_SQEUCLID_POINTS */
+  const float* source_points;         /* m x point_dim, row-major (same memory kind as the problem) */
+  const float* target_points;         /* n x point_dim, row-major */
+  double cost_scale;                  /* > 0: the scale; <= 0: 1 / max_ij ||x_i - y_j||^2 */
+  const double* warm_dual_source;     /* m initial source duals, or NULL (zero start) */
+  const double* warm_dual_target;     /* n initial target duals, or NULL */
+  int32_t reserved[8];                /* must be zero */
 } pdot_solver_options;
 
 /* ---- output -------------------------------------------------------------- */

@@ -1,10 +1,12 @@
 // pdot_common.cuh — shared declarations of the sm_100a PDHG-for-OT solver.
 //
 // Data layout in HBM (one solve):
-//   C          m x n FP64, column-major (entry (i,j) at i + j*m), read-only
-//   X[2]       two m x n FP64 plans: X[buf] is the current iterate, X[1-buf]
-//              the running weighted average. A restart to the average flips
-//              `buf`, so restarts copy nothing.
+//   C          m x n, column-major (entry (i,j) at i + j*m), read-only; FP64
+//              in the drop-in, FP32 or BF16 in mixed precision, or absent when
+//              the squared-Euclidean cost is computed from FP32 coordinates
+//   X[2]       two m x n plans (FP64 drop-in, FP32 mixed precision): X[buf] is
+//              the current iterate, X[1-buf] the running weighted average. A
+//              restart to the average flips `buf`, so restarts copy nothing.
 //   u[2] v[2]  source/target duals (current / average), FP64
 //   r[2] c[2]  row / column sums of the plan (current / average), FP64
 //   partials   per-CTA and per-(panel, column) partial sums; reductions are
@@ -40,10 +42,25 @@ struct Geometry {
   int64_t panels;      // P = ceil(m / kPanelRows)
   int64_t units;       // U = P * n
   int32_t grid;        // CTAs of the matrix passes (<= U)
-  int32_t vec;         // 2: 16-byte loads (m even), 1: scalar loads
+  int32_t vec;         // rows per lane load: 16 B / sizeof(plan element), or 1
   int32_t row_blocks;  // CTAs of the vector passes covering m
   int32_t col_blocks;  // CTAs of the vector passes covering n
+  int32_t plan_f32;    // 1: FP32 plan and average, 0: FP64
+  int32_t cost_kind;   // PDOT_COST_F64 / _F32 / _BF16, or kCostSqBase + point dim
 };
+
+// Where the cost entries come from.
+struct CostSource {
+  const void* C;       // PDOT_COST_F64 / F32 / BF16 storage
+  const float* xs;     // PDOT_COST_SQEUCLID_POINTS: m x dim source points
+  const float* ys;     // n x dim target points
+  int dim;             // 1..kMaxPointDim
+};
+constexpr int kMaxPointDim = 4;
+// Internal cost kinds: the PDOT_COST_* values, and kCostSqBase + dim for the
+// coordinate cost (the point dimension is a compile-time constant of the kernels).
+constexpr int kCostSqBase = 10;
+__host__ __device__ constexpr bool is_sq_cost(int kind) { return kind > kCostSqBase; }
 
 __host__ __device__ __forceinline__ int64_t unit_begin(const Geometry& g, int64_t cta) {
   return cta * g.units / g.grid;
@@ -78,6 +95,7 @@ struct DevState {
   double pdist, ddist;       // distances moved in the last restart period
   // cached_ot_info, termination.jl:87-92
   double linf_obj, linf_rhs, l2_obj, l2_rhs;
+  double cost_scale;         // PDOT_COST_SQEUCLID_POINTS: C = scale * ||x - y||^2
   // timing (globaltimer ns)
   unsigned long long t_start_ns;
   unsigned long long eval_t0_ns;
@@ -115,13 +133,15 @@ struct SolveConfig {
   int record_iteration_stats;
   int scale_invariant_initial_primal_weight;
   double primal_importance;
+  double cost_scale;         // given scale (> 0) or 0: normalise by the max
+  int warm_start;            // duals were given: the stored gradient is C - u - v
 };
 
 struct Buffers {
-  const double* C;
+  CostSource cost;
   const double* a;
   const double* b;
-  double* X[2];
+  void* X[2];        // double (FP64 plan) or float (FP32 plan)
   double* u[2];
   double* v[2];
   double* r[2];
@@ -138,7 +158,8 @@ struct Buffers {
 };
 
 // ---- launchers (pdot_kernels.cu) ----------------------------------------
-Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device);
+Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device, int plan_f32 = 0,
+                       int cost_kind = PDOT_COST_F64);
 size_t workspace_doubles(const Geometry& g);
 
 cudaError_t launch_init(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
@@ -146,6 +167,11 @@ cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s);
 cudaError_t launch_dual(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
 cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
 cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
+
+// Conversions used by the host: FP64 cost to its stored precision, and an
+// FP32 plan widened to FP64 for the caller.
+cudaError_t launch_convert_cost(const double* src, void* dst, int cost_kind, size_t count, cudaStream_t s);
+cudaError_t launch_widen(const float* src, double* dst, size_t count, cudaStream_t s);
 
 // Sets the thread-local text pdot_last_error() returns (pdot_host.cu).
 void set_last_error(const char* msg);

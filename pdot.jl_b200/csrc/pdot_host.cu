@@ -93,8 +93,7 @@ void validate(const pdot_problem* P, const pdot_pdhg_parameters* prm) {
   if (!P || !prm) fail(PDOT_ERR_INVALID_ARGUMENT, "null problem or parameters");
   if (P->num_row < 1 || P->num_col < 1) fail(PDOT_ERR_INVALID_ARGUMENT, "empty problem (%lld x %lld)",
                                              (long long)P->num_row, (long long)P->num_col);
-  if (!P->cost_matrix || !P->source_distribution || !P->target_distribution)
-    fail(PDOT_ERR_INVALID_ARGUMENT, "null problem array");
+  if (!P->source_distribution || !P->target_distribution) fail(PDOT_ERR_INVALID_ARGUMENT, "null problem array");
   if (!(prm->primal_importance > 0) || !std::isfinite(prm->primal_importance))
     fail(PDOT_ERR_INVALID_ARGUMENT, "primal_importance must be positive and finite");
   const pdot_restart_parameters& rp = prm->restart_params;
@@ -112,6 +111,58 @@ void validate(const pdot_problem* P, const pdot_pdhg_parameters* prm) {
     fail(PDOT_ERR_INVALID_ARGUMENT, "termination_evaluation_frequency must be positive");
   if (prm->step_size_policy != PDOT_STEP_SIZE_ADAPTIVE && prm->step_size_policy != PDOT_STEP_SIZE_CONSTANT)
     fail(PDOT_ERR_INVALID_ARGUMENT, "unknown step_size_policy %d", prm->step_size_policy);
+}
+
+// Options of this implementation (include/pdot.h: pdot_solver_options).
+struct Variant {
+  int device = 0;
+  bool use_graph = true, time_kernels = false;
+  int plan_f32 = 0;
+  int cost_kind = PDOT_COST_F64;
+  int point_dim = 0;
+  const float* xs = nullptr;
+  const float* ys = nullptr;
+  double cost_scale = 0.0;
+  const double* warm_u = nullptr;
+  const double* warm_v = nullptr;
+};
+
+Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
+  Variant v;
+  if (!o) {
+    if (!P.cost_matrix) fail(PDOT_ERR_INVALID_ARGUMENT, "null cost matrix");
+    return v;
+  }
+  v.device = o->device;
+  v.use_graph = o->use_cuda_graph != 0;
+  v.time_kernels = o->time_kernels != 0;
+  if (o->plan_precision != PDOT_PRECISION_F64 && o->plan_precision != PDOT_PRECISION_F32)
+    fail(PDOT_ERR_INVALID_ARGUMENT, "unknown plan_precision %d", o->plan_precision);
+  v.plan_f32 = o->plan_precision == PDOT_PRECISION_F32;
+  v.cost_kind = o->cost_storage;
+  if (v.cost_kind < PDOT_COST_F64 || v.cost_kind > PDOT_COST_SQEUCLID_POINTS)
+    fail(PDOT_ERR_INVALID_ARGUMENT, "unknown cost_storage %d", v.cost_kind);
+  if (v.plan_f32 == (v.cost_kind == PDOT_COST_F64))
+    fail(PDOT_ERR_INVALID_ARGUMENT,
+         "the FP64 plan runs with the FP64 cost; an FP32 plan runs with FP32, BF16 or coordinate costs");
+  if (v.cost_kind == PDOT_COST_SQEUCLID_POINTS) {
+    if (o->point_dim < 1 || o->point_dim > pdot::kMaxPointDim)
+      fail(PDOT_ERR_INVALID_ARGUMENT, "point_dim must be 1..%d", pdot::kMaxPointDim);
+    if (!o->source_points || !o->target_points) fail(PDOT_ERR_INVALID_ARGUMENT, "null point coordinates");
+    v.point_dim = o->point_dim;
+    v.xs = o->source_points;
+    v.ys = o->target_points;
+    v.cost_scale = o->cost_scale > 0.0 ? o->cost_scale : 0.0;
+  } else if (!P.cost_matrix) {
+    fail(PDOT_ERR_INVALID_ARGUMENT, "null cost matrix");
+  }
+  if ((o->warm_dual_source == nullptr) != (o->warm_dual_target == nullptr))
+    fail(PDOT_ERR_INVALID_ARGUMENT, "give both warm-start dual vectors or neither");
+  v.warm_u = o->warm_dual_source;
+  v.warm_v = o->warm_dual_target;
+  for (int k = 0; k < 8; ++k)
+    if (o->reserved[k] != 0) fail(PDOT_ERR_INVALID_ARGUMENT, "reserved option fields must be zero");
+  return v;
 }
 
 pdot::SolveConfig make_config(const pdot_pdhg_parameters& p) {
@@ -161,34 +212,91 @@ class Solver {
  public:
   Solver(const pdot_problem& P, bool device_inputs, const pdot_pdhg_parameters& prm,
          const pdot_solver_options* opt)
-      : device_(opt ? opt->device : 0),
-        use_graph_(opt ? opt->use_cuda_graph != 0 : true),
-        time_kernels_(opt ? opt->time_kernels != 0 : false),
-        params_(prm) {
+      : params_(prm) {
+    const Variant var = read_options(P, opt);
+    device_ = var.device;
+    use_graph_ = var.use_graph;
+    time_kernels_ = var.time_kernels;
     CK(cudaSetDevice(device_));
     const int64_t m = P.num_row, n = P.num_col;
-    g_ = pdot::make_geometry(m, n, 1, device_);
-    if (device_inputs && !(aligned16(P.cost_matrix))) g_ = pdot::make_geometry(m, n, 0, device_);
     const size_t N = (size_t)m * (size_t)n;
+    const size_t xbytes = var.plan_f32 ? sizeof(float) : sizeof(double);
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+
+    // the cost: as given (FP64), converted to FP32 / BF16 on the device, or
+    // coordinates for the on-the-fly squared-Euclidean cost
+    bool cost_aligned = true;
+    if (var.cost_kind == PDOT_COST_SQEUCLID_POINTS) {
+      const size_t d = (size_t)var.point_dim;
+      if (device_inputs) {
+        cost_.xs = var.xs;
+        cost_.ys = var.ys;
+      } else {
+        float *xs = nullptr, *ys = nullptr;
+        alloc(&xs, (size_t)m * d);
+        alloc(&ys, (size_t)n * d);
+        CK(cudaMemcpyAsync(xs, var.xs, (size_t)m * d * sizeof(float), cudaMemcpyHostToDevice, stream_));
+        CK(cudaMemcpyAsync(ys, var.ys, (size_t)n * d * sizeof(float), cudaMemcpyHostToDevice, stream_));
+        cost_.xs = xs;
+        cost_.ys = ys;
+      }
+      cost_.dim = var.point_dim;
+      cost_.C = nullptr;
+    } else if (var.cost_kind == PDOT_COST_F64) {
+      if (device_inputs) {
+        cost_.C = P.cost_matrix;
+        cost_aligned = aligned16(P.cost_matrix);
+      } else {
+        double* C = nullptr;
+        alloc(&C, N);
+        CK(cudaMemcpyAsync(C, P.cost_matrix, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        cost_.C = C;
+      }
+    } else {
+      const size_t cbytes = var.cost_kind == PDOT_COST_F32 ? 4 : 2;
+      void* Cs = nullptr;
+      CK(cudaMalloc(&Cs, std::max<size_t>(N, 1) * cbytes));
+      allocs_.push_back(Cs);
+      const double* src = P.cost_matrix;
+      void* tmp = nullptr;
+      if (!device_inputs) {
+        CK(cudaMalloc(&tmp, N * sizeof(double)));
+        CK(cudaMemcpyAsync(tmp, P.cost_matrix, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        src = static_cast<const double*>(tmp);
+      }
+      CK(pdot::launch_convert_cost(src, Cs, var.cost_kind, N, stream_));
+      CK(cudaStreamSynchronize(stream_));
+      if (tmp) CK(cudaFree(tmp));
+      cost_.C = Cs;
+    }
+    const int kind = var.cost_kind == PDOT_COST_SQEUCLID_POINTS ? pdot::kCostSqBase + var.point_dim : var.cost_kind;
+    g_ = pdot::make_geometry(m, n, cost_aligned ? 1 : 0, device_, var.plan_f32, kind);
     if (device_inputs) {
-      C_ = P.cost_matrix;
       a_ = P.source_distribution;
       b_ = P.target_distribution;
     } else {
-      double *C = nullptr, *a = nullptr, *b = nullptr;
-      alloc(&C, N);
+      double *a = nullptr, *b = nullptr;
       alloc(&a, m);
       alloc(&b, n);
-      CK(cudaMemcpyAsync(C, P.cost_matrix, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
       CK(cudaMemcpyAsync(a, P.source_distribution, m * sizeof(double), cudaMemcpyHostToDevice, stream_));
       CK(cudaMemcpyAsync(b, P.target_distribution, n * sizeof(double), cudaMemcpyHostToDevice, stream_));
-      C_ = C;
       a_ = a;
       b_ = b;
     }
-    alloc(&X_[0], N);
-    alloc(&X_[1], N);
+    if (var.warm_u) {
+      alloc(&warm_u_, m);
+      alloc(&warm_v_, n);
+      const cudaMemcpyKind kind = device_inputs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+      CK(cudaMemcpyAsync(warm_u_, var.warm_u, m * sizeof(double), kind, stream_));
+      CK(cudaMemcpyAsync(warm_v_, var.warm_v, n * sizeof(double), kind, stream_));
+    }
+    void* xp = nullptr;
+    for (int k = 0; k < 2; ++k) {
+      CK(cudaMalloc(&xp, std::max<size_t>(N, 1) * xbytes));
+      allocs_.push_back(xp);
+      X_[k] = xp;
+    }
+    xbytes_ = xbytes;
     for (int k = 0; k < 2; ++k) {
       alloc(&u_[k], m);
       alloc(&r_[k], m);
@@ -207,7 +315,7 @@ class Solver {
     host_status_ = static_cast<pdot::DevState*>(p);
     for (int k = 0; k < kInFlight; ++k) CK(cudaEventCreateWithFlags(&ev_[k], cudaEventDisableTiming));
 
-    B_.C = C_;
+    B_.cost = cost_;
     B_.a = a_;
     B_.b = b_;
     for (int k = 0; k < 2; ++k) {
@@ -236,6 +344,8 @@ class Solver {
     B_.st = st_;
 
     cfg_ = make_config(prm);
+    cfg_.cost_scale = var.cost_scale;
+    cfg_.warm_start = warm_u_ != nullptr;
     freq_ = prm.termination_evaluation_frequency;
     limit_ = prm.termination_criteria.iteration_limit;
     if (use_graph_ && !time_kernels_) capture_regular_chunk();
@@ -269,10 +379,15 @@ class Solver {
     CK(cudaSetDevice(device_));
     CK(cudaStreamSynchronize(stream_));
     const size_t N = (size_t)g_.m * (size_t)g_.n;
-    CK(cudaMemsetAsync(X_[0], 0, N * sizeof(double), stream_));
-    CK(cudaMemsetAsync(u_[0], 0, g_.m * sizeof(double), stream_));
+    CK(cudaMemsetAsync(X_[0], 0, N * xbytes_, stream_));
+    if (warm_u_) {
+      CK(cudaMemcpyAsync(u_[0], warm_u_, g_.m * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+      CK(cudaMemcpyAsync(v_[0], warm_v_, g_.n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    } else {
+      CK(cudaMemsetAsync(u_[0], 0, g_.m * sizeof(double), stream_));
+      CK(cudaMemsetAsync(v_[0], 0, g_.n * sizeof(double), stream_));
+    }
     CK(cudaMemsetAsync(r_[0], 0, g_.m * sizeof(double), stream_));
-    CK(cudaMemsetAsync(v_[0], 0, g_.n * sizeof(double), stream_));
     CK(cudaMemsetAsync(c_[0], 0, g_.n * sizeof(double), stream_));
     CK(cudaMemsetAsync(st_, 0, sizeof(pdot::DevState), stream_));
     CK(pdot::launch_init(B_, g_, cfg_, stream_));
@@ -325,8 +440,24 @@ class Solver {
     // gpu_to_cpu!, src/io.jl:41-53 (average, or current if no average exists)
     const int xb = status_.out_current ? status_.buf : (status_.buf ^ 1);
     const size_t N = (size_t)g_.m * (size_t)g_.n;
-    if (out->primal_solution)
-      CK(cudaMemcpy(out->primal_solution, X_[xb], N * sizeof(double), cudaMemcpyDeviceToHost));
+    if (out->primal_solution) {
+      if (!g_.plan_f32) {
+        CK(cudaMemcpy(out->primal_solution, X_[xb], N * sizeof(double), cudaMemcpyDeviceToHost));
+      } else {
+        // widen the FP32 plan in chunks through a small device buffer
+        const size_t chunk = std::min<size_t>(N, size_t(1) << 24);
+        double* tmp = nullptr;
+        CK(cudaMalloc(&tmp, std::max<size_t>(chunk, 1) * sizeof(double)));
+        for (size_t off = 0; off < N; off += chunk) {
+          const size_t cnt = std::min(chunk, N - off);
+          CK(pdot::launch_widen(static_cast<const float*>(X_[xb]) + off, tmp, cnt, stream_));
+          CK(cudaMemcpyAsync(out->primal_solution + off, tmp, cnt * sizeof(double), cudaMemcpyDeviceToHost,
+                             stream_));
+        }
+        CK(cudaStreamSynchronize(stream_));
+        CK(cudaFree(tmp));
+      }
+    }
     if (out->dual_source_solution)
       CK(cudaMemcpy(out->dual_source_solution, u_[xb], g_.m * sizeof(double), cudaMemcpyDeviceToHost));
     if (out->dual_target_solution)
@@ -487,8 +618,8 @@ class Solver {
     drained_ = total;
   }
 
-  int device_;
-  bool use_graph_, time_kernels_;
+  int device_ = 0;
+  bool use_graph_ = true, time_kernels_ = false;
   pdot_pdhg_parameters params_;
   pdot::Geometry g_{};
   pdot::SolveConfig cfg_{};
@@ -502,10 +633,13 @@ class Solver {
   double primal_ms_ = 0.0, dual_ms_ = 0.0, eval_ms_ = 0.0;
   long long timed_primal_ = 0;
   std::vector<void*> allocs_;
-  const double* C_ = nullptr;
+  pdot::CostSource cost_{};
   const double* a_ = nullptr;
   const double* b_ = nullptr;
-  double* X_[2] = {};
+  double* warm_u_ = nullptr;
+  double* warm_v_ = nullptr;
+  void* X_[2] = {};
+  size_t xbytes_ = sizeof(double);
   double* u_[2] = {};
   double* v_[2] = {};
   double* r_[2] = {};
@@ -559,6 +693,7 @@ int pdot_optimize(const pdot_problem* problem, const pdot_pdhg_parameters* param
   return guarded([&] {
     validate(problem, params);
     if (!output) fail(PDOT_ERR_INVALID_ARGUMENT, "null output");
+    read_options(*problem, options);
     require_sm100(options ? options->device : 0);
     Solver solver(*problem, false, *params, options);
     solver.finish(output);
@@ -575,6 +710,7 @@ static int create_solver(const pdot_problem* problem, const pdot_pdhg_parameters
     validate(problem, params);
     if (!out) fail(PDOT_ERR_INVALID_ARGUMENT, "null solver handle");
     *out = nullptr;
+    read_options(*problem, options);
     require_sm100(options ? options->device : 0);
     Solver* s = new Solver(*problem, device_inputs, *params, options);
     *out = new pdot_solver{s};

@@ -19,8 +19,18 @@
 // reference's operation order (no fused multiply-add), so the projected step,
 // the plan update and the averages round exactly as the reference's Julia code
 // does; only the order of the sums differs.
+//
+// The matrix kernels are templates over the plan element (double for the FP64
+// drop-in, float for mixed precision), the cost source (FP64 / FP32 / BF16
+// storage, or the squared-Euclidean cost computed from FP32 coordinates) and
+// the rows each lane loads at once (16 bytes of plan, or 1 on the scalar path
+// for odd sizes and unaligned buffers). Per-entry arithmetic is FP64 in every
+// variant; an FP32 plan is rounded once when stored, and the step entering the
+// row/column sums is taken between the stored values, so the FP64 sums track
+// the stored plan exactly.
 #include <cfloat>
 #include <cmath>
+#include <cuda_bf16.h>
 
 #include "pdot_common.cuh"
 
@@ -122,80 +132,248 @@ __device__ __forceinline__ bool elect_last_cta(unsigned int* ticket) {
   return last;
 }
 
-template <int VEC>
-struct VecIO;
+// ---- vector loads and stores of R consecutive rows (R*sizeof(T) bytes) -------
+// Values stay in their storage type in registers and are widened to FP64 at use.
+template <int BYTES>
+struct VecWord;
 template <>
-struct VecIO<1> {
-  static __device__ __forceinline__ void ld(const double* p, double (&v)[1]) { v[0] = *p; }
-  static __device__ __forceinline__ void ldg(const double* p, double (&v)[1]) { v[0] = __ldg(p); }
-  static __device__ __forceinline__ void st(double* p, const double (&v)[1]) { *p = v[0]; }
+struct VecWord<16> {
+  using type = uint4;
 };
 template <>
-struct VecIO<2> {
-  static __device__ __forceinline__ void ld(const double* p, double (&v)[2]) {
-    const double2 t = *reinterpret_cast<const double2*>(p);
+struct VecWord<8> {
+  using type = uint2;
+};
+template <>
+struct VecWord<4> {
+  using type = unsigned int;
+};
+template <>
+struct VecWord<2> {
+  using type = unsigned short;
+};
+
+template <typename T, int R>
+__device__ __forceinline__ void vld(const T* p, T (&v)[R]) {
+  if constexpr (R == 1) {
+    v[0] = *p;
+  } else if constexpr (sizeof(T) == 8) {
+#pragma unroll
+    for (int h = 0; h < R / 2; ++h) {
+      const double2 t = reinterpret_cast<const double2*>(p)[h];
+      v[2 * h] = t.x;
+      v[2 * h + 1] = t.y;
+    }
+  } else if constexpr (sizeof(T) == 4 && R == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
     v[0] = t.x;
     v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+  } else {
+    using W = typename VecWord<sizeof(T) * R>::type;
+    const W w = *reinterpret_cast<const W*>(p);
+    memcpy(v, &w, sizeof(W));
   }
-  static __device__ __forceinline__ void ldg(const double* p, double (&v)[2]) {
-    const double2 t = __ldg(reinterpret_cast<const double2*>(p));
+}
+template <typename T, int R>
+__device__ __forceinline__ void vldg(const T* p, T (&v)[R]) {
+  if constexpr (R == 1) {
+    v[0] = __ldg(p);
+  } else if constexpr (sizeof(T) == 8) {
+#pragma unroll
+    for (int h = 0; h < R / 2; ++h) {
+      const double2 t = __ldg(reinterpret_cast<const double2*>(p) + h);
+      v[2 * h] = t.x;
+      v[2 * h + 1] = t.y;
+    }
+  } else if constexpr (sizeof(T) == 4 && R == 4) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
     v[0] = t.x;
     v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+  } else {
+    using W = typename VecWord<sizeof(T) * R>::type;
+    const W w = __ldg(reinterpret_cast<const W*>(p));
+    memcpy(v, &w, sizeof(W));
   }
-  static __device__ __forceinline__ void st(double* p, const double (&v)[2]) {
-    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+}
+template <typename T, int R>
+__device__ __forceinline__ void vst(T* p, const T (&v)[R]) {
+  if constexpr (R == 1) {
+    *p = v[0];
+  } else if constexpr (sizeof(T) == 8) {
+#pragma unroll
+    for (int h = 0; h < R / 2; ++h) reinterpret_cast<double2*>(p)[h] = make_double2(v[2 * h], v[2 * h + 1]);
+  } else if constexpr (sizeof(T) == 4 && R == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+    using W = typename VecWord<sizeof(T) * R>::type;
+    W w;
+    memcpy(&w, v, sizeof(W));
+    *reinterpret_cast<W*>(p) = w;
+  }
+}
+
+__device__ __forceinline__ double widen(double x) { return x; }
+__device__ __forceinline__ double widen(float x) { return (double)x; }
+__device__ __forceinline__ double widen(__nv_bfloat16 x) { return (double)__bfloat162float(x); }
+
+// Round an FP64 value to the plan's storage type.
+template <typename TX>
+__device__ __forceinline__ TX narrow(double x);
+template <>
+__device__ __forceinline__ double narrow<double>(double x) {
+  return x;
+}
+template <>
+__device__ __forceinline__ float narrow<float>(double x) {
+  return __double2float_rn(x);
+}
+
+// ---- cost sources ------------------------------------------------------------
+// panel(): once per panel (per-lane row data); column(): once per column
+// (warp-uniform data); get(): the R cost entries of lane rows k at index idx,
+// in the source's value type (value_t).
+//
+// C_ij = scale * ||x_i - y_j||^2 in FP32 from DIM-dimensional coordinates;
+// nothing of C is read from memory.
+template <int CK, int R, int RPL>
+struct CostReader {
+  static constexpr int DIM = CK - kCostSqBase;
+  static_assert(DIM >= 1 && DIM <= kMaxPointDim, "coordinate cost kinds only");
+  using value_t = float;
+  const float* __restrict__ xs;
+  const float* __restrict__ ys;
+  float scale;
+  float xr[RPL][R][DIM];
+  float yr[DIM];
+  __device__ __forceinline__ CostReader(const CostSource& s, float scl) : xs(s.xs), ys(s.ys), scale(scl) {}
+  __device__ __forceinline__ void panel(int64_t row0, int lane, int64_t m, const bool (&ok)[RPL]) {
+#pragma unroll
+    for (int k = 0; k < RPL; ++k)
+#pragma unroll
+      for (int e = 0; e < R; ++e) {
+        const int64_t i = row0 + k * 32 * R + lane * R + e;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) xr[k][e][d] = (ok[k] && i < m) ? __ldg(xs + i * DIM + d) : 0.0f;
+      }
+  }
+  __device__ __forceinline__ void column(int64_t j) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) yr[d] = __ldg(ys + j * DIM + d);
+  }
+  __device__ __forceinline__ void get(int64_t, int k, float (&c)[R]) const {
+#pragma unroll
+    for (int e = 0; e < R; ++e) {
+      float acc = 0.0f;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        const float t = xr[k][e][d] - yr[d];
+        acc = acc + t * t;
+      }
+      c[e] = acc * scale;
+    }
   }
 };
+
+template <typename T, int R, int RPL>
+struct StoredCost {
+  using value_t = T;
+  const T* __restrict__ C;
+  __device__ __forceinline__ StoredCost(const CostSource& s, float) : C(static_cast<const T*>(s.C)) {}
+  __device__ __forceinline__ void panel(int64_t, int, int64_t, const bool (&)[RPL]) {}
+  __device__ __forceinline__ void column(int64_t) {}
+  __device__ __forceinline__ void get(int64_t idx, int, T (&c)[R]) const { vldg<T, R>(C + idx, c); }
+};
+template <int R, int RPL>
+struct CostReader<PDOT_COST_F64, R, RPL> : StoredCost<double, R, RPL> {
+  using StoredCost<double, R, RPL>::StoredCost;
+};
+template <int R, int RPL>
+struct CostReader<PDOT_COST_F32, R, RPL> : StoredCost<float, R, RPL> {
+  using StoredCost<float, R, RPL>::StoredCost;
+};
+template <int R, int RPL>
+struct CostReader<PDOT_COST_BF16, R, RPL> : StoredCost<__nv_bfloat16, R, RPL> {
+  using StoredCost<__nv_bfloat16, R, RPL>::StoredCost;
+};
+
+// One entry of the primal pass (see the fused pass below). With an FP32 plan
+// the new value is rounded to its stored precision first and the step d is
+// taken between stored values.
+template <typename TX>
+__device__ __forceinline__ void primal_entry(double c, double ui, double vj, double s, double nw, double aw,
+                                             bool zero_g, bool first, TX& xs, TX& xas, double& d) {
+  const double x = widen(xs);
+  const double gg = zero_g ? 0.0 : __dsub_rn(__dsub_rn(c, ui), vj);
+  const double t = jl_max0(__dsub_rn(x, __dmul_rn(s, gg)));
+  double xn;
+  if constexpr (sizeof(TX) == 8) {
+    d = __dsub_rn(t, x);
+    xn = __dadd_rn(x, d);
+  } else {
+    xn = (double)__double2float_rn(t);
+    d = __dsub_rn(xn, x);
+  }
+  xs = narrow<TX>(xn);
+  xas = narrow<TX>(first ? xn : __dmul_rn(__dadd_rn(widen(xas), __dmul_rn(xn, nw)), aw));
+}
 
 // ---------------------------------------------------------------------------
 // The fused primal pass. Per entry (src/solver_gpu.jl:139-141,242,249-250;
 // src/saddle_point_gpu.jl:129-130):
 //   g  = (C - u_i) - v_j ;  t = max(X - s*g, 0) ;  d = t - X ;  X' = X + d
 //   Xavg' = (Xavg + X'*nw)*aw      (Xavg' = X' after a reset of the average)
-template <int VEC>
-__device__ __forceinline__ void primal_pass_body(const double* __restrict__ C, double* __restrict__ X,
-                                                 double* __restrict__ Xa, const double* __restrict__ u,
+template <typename TX, int CK, int R>
+__device__ __forceinline__ void primal_pass_body(const CostSource& csrc, float scale, TX* __restrict__ X,
+                                                 TX* __restrict__ Xa, const double* __restrict__ u,
                                                  const double* __restrict__ v, const double s,
                                                  const double nw, const double aw, const bool zero_g,
                                                  const bool first, double* __restrict__ colpart,
                                                  double* __restrict__ rowpart, double* __restrict__ sqpart,
                                                  const Geometry g) {
-  constexpr int RPL = kPanelRows / (32 * VEC);
+  constexpr int RPL = kPanelRows / (32 * R);
   __shared__ double red[kWarps][kPanelRows];
   __shared__ double sqw[kWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t m = g.m, n = g.n;
   const int64_t cta = blockIdx.x;
   const int64_t q0 = unit_begin(g, cta), q1 = unit_begin(g, cta + 1);
+  CostReader<CK, R, RPL> cost(csrc, scale);
   double sq = 0.0;
   for (int64_t p = q0 / n; p * n < q1; ++p) {
     const int64_t jb = (q0 > p * n ? q0 : p * n) - p * n;
     const int64_t je = (q1 < (p + 1) * n ? q1 : (p + 1) * n) - p * n;
     const int64_t row0 = p * kPanelRows;
-    double acc[RPL][VEC];
-    double ur[RPL][VEC];
+    double acc[RPL][R];
+    double ur[RPL][R];
     bool ok[RPL];
 #pragma unroll
     for (int k = 0; k < RPL; ++k) {
-      const int64_t i = row0 + k * 32 * VEC + lane * VEC;
+      const int64_t i = row0 + k * 32 * R + lane * R;
       ok[k] = i < m;
 #pragma unroll
-      for (int e = 0; e < VEC; ++e) {
+      for (int e = 0; e < R; ++e) {
         acc[k][e] = 0.0;
         ur[k][e] = (ok[k] && !zero_g) ? __ldg(u + i + e) : 0.0;
       }
     }
+    cost.panel(row0, lane, m, ok);
     for (int64_t j = jb + warp; j < je; j += kWarps) {
       const double vj = zero_g ? 0.0 : __ldg(v + j);
-      const int64_t base = j * m + row0 + lane * VEC;
-      double cv[RPL][VEC], xv[RPL][VEC], av[RPL][VEC];
+      cost.column(j);
+      const int64_t base = j * m + row0 + lane * R;
+      typename CostReader<CK, R, RPL>::value_t cv[RPL][R];
+      TX xv[RPL][R], av[RPL][R];
 #pragma unroll
       for (int k = 0; k < RPL; ++k) {
         if (ok[k]) {
-          const int64_t idx = base + k * 32 * VEC;
-          VecIO<VEC>::ldg(C + idx, cv[k]);
-          VecIO<VEC>::ld(X + idx, xv[k]);
-          if (!first) VecIO<VEC>::ld(Xa + idx, av[k]);
+          const int64_t idx = base + k * 32 * R;
+          cost.get(idx, k, cv[k]);
+          vld<TX, R>(X + idx, xv[k]);
+          if (!first) vld<TX, R>(Xa + idx, av[k]);
         }
       }
       double cs = 0.0;
@@ -203,20 +381,16 @@ __device__ __forceinline__ void primal_pass_body(const double* __restrict__ C, d
       for (int k = 0; k < RPL; ++k) {
         if (ok[k]) {
 #pragma unroll
-          for (int e = 0; e < VEC; ++e) {
-            const double gg = zero_g ? 0.0 : __dsub_rn(__dsub_rn(cv[k][e], ur[k][e]), vj);
-            const double t = jl_max0(__dsub_rn(xv[k][e], __dmul_rn(s, gg)));
-            const double d = __dsub_rn(t, xv[k][e]);
-            const double xn = __dadd_rn(xv[k][e], d);
-            xv[k][e] = xn;
-            av[k][e] = first ? xn : __dmul_rn(__dadd_rn(av[k][e], __dmul_rn(xn, nw)), aw);
+          for (int e = 0; e < R; ++e) {
+            double d;
+            primal_entry<TX>(widen(cv[k][e]), ur[k][e], vj, s, nw, aw, zero_g, first, xv[k][e], av[k][e], d);
             acc[k][e] += d;
             cs += d;
             sq += d * d;
           }
-          const int64_t idx = base + k * 32 * VEC;
-          VecIO<VEC>::st(X + idx, xv[k]);
-          VecIO<VEC>::st(Xa + idx, av[k]);
+          const int64_t idx = base + k * 32 * R;
+          vst<TX, R>(X + idx, xv[k]);
+          vst<TX, R>(Xa + idx, av[k]);
         }
       }
       cs = warp_sum(cs);
@@ -226,7 +400,7 @@ __device__ __forceinline__ void primal_pass_body(const double* __restrict__ C, d
 #pragma unroll
     for (int k = 0; k < RPL; ++k)
 #pragma unroll
-      for (int e = 0; e < VEC; ++e) red[warp][k * 32 * VEC + lane * VEC + e] = acc[k][e];
+      for (int e = 0; e < R; ++e) red[warp][k * 32 * R + lane * R + e] = acc[k][e];
     __syncthreads();
     for (int t = threadIdx.x; t < kPanelRows; t += kThreads) {
       double s2 = red[0][t];
@@ -247,7 +421,7 @@ __device__ __forceinline__ void primal_pass_body(const double* __restrict__ C, d
   }
 }
 
-template <int VEC>
+template <typename TX, int CK, int R>
 __global__ void __launch_bounds__(kThreads, 2) k1_primal(Buffers B, Geometry g) {
   const DevState* st = B.st;
   if (st->done | st->numerical_error) return;
@@ -260,17 +434,23 @@ __global__ void __launch_bounds__(kThreads, 2) k1_primal(Buffers B, Geometry g) 
   const double s = __ddiv_rn(tau, omega);
   const double nw = first ? 1.0 : __ddiv_rn(tau, S);
   const double aw = first ? 1.0 : __ddiv_rn(S, __dadd_rn(S, tau));
-  primal_pass_body<VEC>(B.C, B.X[buf], B.X[buf ^ 1], B.u[buf], B.v[buf], s, nw, aw, zero_g, first,
-                        B.colpart, B.rowpart, B.sqpart, g);
+  primal_pass_body<TX, CK, R>(B.cost, (float)st->cost_scale, static_cast<TX*>(B.X[buf]),
+                              static_cast<TX*>(B.X[buf ^ 1]), B.u[buf], B.v[buf], s, nw, aw, zero_g, first,
+                              B.colpart, B.rowpart, B.sqpart, g);
 }
 
-template <int VEC>
+template <int R>
 __global__ void __launch_bounds__(kThreads, 2)
     k1_primal_args(const double* C, double* X, double* Xa, const double* u, const double* v, double s,
                    double nw, double aw, int flags, double* colpart, double* rowpart, double* sqpart,
                    Geometry g) {
-  primal_pass_body<VEC>(C, X, Xa, u, v, s, nw, aw, (flags & PDOT_PASS_ZERO_GRADIENT) != 0,
-                        (flags & PDOT_PASS_FIRST_AVERAGE) != 0, colpart, rowpart, sqpart, g);
+  CostSource cs;
+  cs.C = C;
+  cs.xs = cs.ys = nullptr;
+  cs.dim = 0;
+  primal_pass_body<double, PDOT_COST_F64, R>(cs, 1.0f, X, Xa, u, v, s, nw, aw,
+                                             (flags & PDOT_PASS_ZERO_GRADIENT) != 0,
+                                             (flags & PDOT_PASS_FIRST_AVERAGE) != 0, colpart, rowpart, sqpart, g);
 }
 
 // Second stage of the row sum of row i / column sum of column j.
@@ -436,18 +616,18 @@ enum { E_DOT = 0, E_SQX, E_MAXX, E_SQG, E_MAXG, E_AVG = 5 };
 constexpr unsigned kEvalMaxMask = (1u << E_MAXX) | (1u << E_MAXG) | (1u << (E_AVG + E_MAXX)) |
                                   (1u << (E_AVG + E_MAXG));
 
-template <int VEC>
+template <typename TX, int CK, int R>
 __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
   DevState* st = B.st;
   if (st->done) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) st->eval_t0_ns = globaltimer_ns();
-  constexpr int RPL = kPanelRows / (32 * VEC);
+  constexpr int RPL = kPanelRows / (32 * R);
   const int buf = st->buf;
   const bool have_avg = st->avg_count > 0;
   const bool zero_g = st->g_is_zero != 0;
-  const double* __restrict__ C = B.C;
-  const double* __restrict__ X = B.X[buf];
-  const double* __restrict__ Xa = B.X[buf ^ 1];
+  CostReader<CK, R, RPL> cost(B.cost, (float)st->cost_scale);
+  const TX* __restrict__ X = static_cast<const TX*>(B.X[buf]);
+  const TX* __restrict__ Xa = static_cast<const TX*>(B.X[buf ^ 1]);
   const double* __restrict__ u = B.u[buf];
   const double* __restrict__ v = B.v[buf];
   const double* __restrict__ ua = B.u[buf ^ 1];
@@ -463,38 +643,41 @@ __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
     const int64_t jb = (q0 > p * n ? q0 : p * n) - p * n;
     const int64_t je = (q1 < (p + 1) * n ? q1 : (p + 1) * n) - p * n;
     const int64_t row0 = p * kPanelRows;
-    double ur[RPL][VEC], uar[RPL][VEC];
+    double ur[RPL][R], uar[RPL][R];
     bool ok[RPL];
 #pragma unroll
     for (int k = 0; k < RPL; ++k) {
-      const int64_t i = row0 + k * 32 * VEC + lane * VEC;
+      const int64_t i = row0 + k * 32 * R + lane * R;
       ok[k] = i < m;
 #pragma unroll
-      for (int e = 0; e < VEC; ++e) {
+      for (int e = 0; e < R; ++e) {
         ur[k][e] = ok[k] ? __ldg(u + i + e) : 0.0;
         uar[k][e] = (ok[k] && have_avg) ? __ldg(ua + i + e) : 0.0;
       }
     }
+    cost.panel(row0, lane, m, ok);
     for (int64_t j = jb + warp; j < je; j += kWarps) {
       const double vj = __ldg(v + j);
       const double vaj = have_avg ? __ldg(va + j) : 0.0;
-      const int64_t base = j * m + row0 + lane * VEC;
-      double cv[RPL][VEC], xv[RPL][VEC], av[RPL][VEC];
+      cost.column(j);
+      const int64_t base = j * m + row0 + lane * R;
+      typename CostReader<CK, R, RPL>::value_t cv[RPL][R];
+      TX xv[RPL][R], av[RPL][R];
 #pragma unroll
       for (int k = 0; k < RPL; ++k) {
         if (ok[k]) {
-          const int64_t idx = base + k * 32 * VEC;
-          VecIO<VEC>::ldg(C + idx, cv[k]);
-          VecIO<VEC>::ldg(X + idx, xv[k]);
-          if (have_avg) VecIO<VEC>::ldg(Xa + idx, av[k]);
+          const int64_t idx = base + k * 32 * R;
+          cost.get(idx, k, cv[k]);
+          vldg<TX, R>(X + idx, xv[k]);
+          if (have_avg) vldg<TX, R>(Xa + idx, av[k]);
         }
       }
 #pragma unroll
       for (int k = 0; k < RPL; ++k) {
         if (ok[k]) {
 #pragma unroll
-          for (int e = 0; e < VEC; ++e) {
-            const double c = cv[k][e], x = xv[k][e];
+          for (int e = 0; e < R; ++e) {
+            const double c = widen(cv[k][e]), x = widen(xv[k][e]);
             const double gg = zero_g ? 0.0 : __dsub_rn(__dsub_rn(c, ur[k][e]), vj);
             const double mg = neg_part(gg);
             acc[E_DOT] += c * x;
@@ -503,7 +686,7 @@ __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
             acc[E_SQG] += mg * mg;
             acc[E_MAXG] = nanmax(acc[E_MAXG], mg);
             if (have_avg) {
-              const double xa = av[k][e];
+              const double xa = widen(av[k][e]);
               const double ga = __dsub_rn(__dsub_rn(c, uar[k][e]), vaj);
               const double mga = neg_part(ga);
               acc[E_AVG + E_DOT] += c * xa;
@@ -767,29 +950,37 @@ __global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, So
 // the initial step size and primal weight (src/solver_gpu.jl:476-496,
 // src/saddle_point_gpu.jl:848-866) and the initial last-restart record (the
 // zero point, src/saddle_point_gpu.jl:371-393).
-template <int VEC>
+template <typename TX, int CK, int R>
 __global__ void __launch_bounds__(kThreads, 2) k0_init(Buffers B, Geometry g, SolveConfig cfg) {
-  constexpr int RPL = kPanelRows / (32 * VEC);
+  constexpr int RPL = kPanelRows / (32 * R);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t m = g.m, n = g.n;
   const int64_t cta = blockIdx.x;
   const int64_t q0 = unit_begin(g, cta), q1 = unit_begin(g, cta + 1);
+  // the coordinate cost is reduced unscaled; the scale is known only at the end
+  CostReader<CK, R, RPL> cost(B.cost, 1.0f);
   double acc[kNormSums] = {0.0, 0.0};  // sum C^2, max |C|
   for (int64_t p = q0 / n; p * n < q1; ++p) {
     const int64_t jb = (q0 > p * n ? q0 : p * n) - p * n;
     const int64_t je = (q1 < (p + 1) * n ? q1 : (p + 1) * n) - p * n;
     const int64_t row0 = p * kPanelRows;
+    bool ok[RPL];
+#pragma unroll
+    for (int k = 0; k < RPL; ++k) ok[k] = row0 + k * 32 * R + lane * R < m;
+    cost.panel(row0, lane, m, ok);
     for (int64_t j = jb + warp; j < je; j += kWarps) {
-      const int64_t base = j * m + row0 + lane * VEC;
+      cost.column(j);
+      const int64_t base = j * m + row0 + lane * R;
 #pragma unroll
       for (int k = 0; k < RPL; ++k) {
-        if (row0 + k * 32 * VEC + lane * VEC < m) {
-          double cv[VEC];
-          VecIO<VEC>::ldg(B.C + base + k * 32 * VEC, cv);
+        if (ok[k]) {
+          typename CostReader<CK, R, RPL>::value_t cv[R];
+          cost.get(base + k * 32 * R, k, cv);
 #pragma unroll
-          for (int e = 0; e < VEC; ++e) {
-            acc[0] += cv[e] * cv[e];
-            acc[1] = nanmax(acc[1], fabs(cv[e]));
+          for (int e = 0; e < R; ++e) {
+            const double c = widen(cv[e]);
+            acc[0] += c * c;
+            acc[1] = nanmax(acc[1], fabs(c));
           }
         }
       }
@@ -811,6 +1002,13 @@ __global__ void __launch_bounds__(kThreads, 2) k0_init(Buffers B, Geometry g, So
     double nc[kNormSums];
     warp_reduce_partials<kNormSums>(B.evpart, 0, g.grid, 2u, nc);
     if (threadIdx.x == 0) {
+      double scale = 1.0;
+      if (is_sq_cost(CK)) {
+        scale = cfg.cost_scale > 0.0 ? cfg.cost_scale : (nc[1] > 0.0 ? 1.0 / nc[1] : 1.0);
+        nc[0] *= scale * scale;
+        nc[1] *= scale;
+      }
+      st->cost_scale = scale;
       st->linf_obj = nc[1];
       st->l2_obj = sqrt(nc[0]);
       st->linf_rhs = vsum[1];
@@ -836,7 +1034,9 @@ __global__ void __launch_bounds__(kThreads, 2) k0_init(Buffers B, Geometry g, So
       st->last_restart_length = 1;
       st->pdist = st->ddist = 0.0;
       st->numerical_error = 0;
-      st->g_is_zero = 1;
+      // the stored gradient starts at 0 (src/solver_gpu.jl:434); after a warm
+      // start it is C - u - v from the first step on
+      st->g_is_zero = cfg.warm_start ? 0 : 1;
       st->buf = 0;
       st->out_current = 1;
       st->num_stats = 0;
@@ -863,18 +1063,65 @@ int blocks_per_sm(K kernel) {
   return nb;
 }
 
+// FP32 storage of an FP64 cost, and an FP32 plan widened for the caller.
+__global__ void k_convert_cost(const double* __restrict__ src, void* __restrict__ dst, int kind, size_t count) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+    if (kind == PDOT_COST_F32)
+      static_cast<float*>(dst)[i] = __double2float_rn(src[i]);
+    else
+      static_cast<__nv_bfloat16*>(dst)[i] = __double2bfloat16(src[i]);
+  }
+}
+__global__ void k_widen(const float* __restrict__ src, double* __restrict__ dst, size_t count) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+
 }  // namespace
 
-Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device) {
+// Expands to the kernel variant of geometry `g`:
+//   plan FP64 + cost FP64, or plan FP32 + cost FP32 / BF16 / coordinates,
+//   each with the 16-byte load path (R = 16 / sizeof(plan)) or R = 1.
+#define PDOT_VARIANT(g, KERNEL, LAUNCH)                                                   \
+  do {                                                                                     \
+    if (!(g).plan_f32) {                                                                   \
+      if ((g).vec > 1) { auto kfn = KERNEL<double, PDOT_COST_F64, 2>; LAUNCH; }            \
+      else { auto kfn = KERNEL<double, PDOT_COST_F64, 1>; LAUNCH; }                        \
+    } else if ((g).cost_kind == PDOT_COST_F32) {                                           \
+      if ((g).vec > 1) { auto kfn = KERNEL<float, PDOT_COST_F32, 4>; LAUNCH; }             \
+      else { auto kfn = KERNEL<float, PDOT_COST_F32, 1>; LAUNCH; }                         \
+    } else if ((g).cost_kind == PDOT_COST_BF16) {                                          \
+      if ((g).vec > 1) { auto kfn = KERNEL<float, PDOT_COST_BF16, 4>; LAUNCH; }            \
+      else { auto kfn = KERNEL<float, PDOT_COST_BF16, 1>; LAUNCH; }                        \
+    } else if ((g).cost_kind == kCostSqBase + 1) {                                         \
+      if ((g).vec > 1) { auto kfn = KERNEL<float, kCostSqBase + 1, 4>; LAUNCH; }           \
+      else { auto kfn = KERNEL<float, kCostSqBase + 1, 1>; LAUNCH; }                       \
+    } else if ((g).cost_kind == kCostSqBase + 2) {                                         \
+      if ((g).vec > 1) { auto kfn = KERNEL<float, kCostSqBase + 2, 4>; LAUNCH; }           \
+      else { auto kfn = KERNEL<float, kCostSqBase + 2, 1>; LAUNCH; }                       \
+    } else if ((g).cost_kind == kCostSqBase + 3) {                                         \
+      if ((g).vec > 1) { auto kfn = KERNEL<float, kCostSqBase + 3, 4>; LAUNCH; }           \
+      else { auto kfn = KERNEL<float, kCostSqBase + 3, 1>; LAUNCH; }                       \
+    } else {                                                                               \
+      if ((g).vec > 1) { auto kfn = KERNEL<float, kCostSqBase + 4, 4>; LAUNCH; }           \
+      else { auto kfn = KERNEL<float, kCostSqBase + 4, 1>; LAUNCH; }                       \
+    }                                                                                      \
+  } while (0)
+
+Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device, int plan_f32, int cost_kind) {
   Geometry g;
   g.m = m;
   g.n = n;
+  g.plan_f32 = plan_f32 ? 1 : 0;
+  g.cost_kind = cost_kind;
   g.panels = (m + kPanelRows - 1) / kPanelRows;
   g.units = g.panels * n;
-  g.vec = (vec_ok && (m % 2 == 0)) ? 2 : 1;
+  const int R = g.plan_f32 ? 4 : 2;
+  g.vec = (vec_ok && (m % R == 0)) ? R : 1;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  const int occ = g.vec == 2 ? blocks_per_sm(k1_primal<2>) : blocks_per_sm(k1_primal<1>);
+  int occ = 1;
+  PDOT_VARIANT(g, k1_primal, occ = blocks_per_sm(kfn));
   int64_t grid = (int64_t)sms * occ;
   if (grid > g.units) grid = g.units;
   g.grid = (int32_t)grid;
@@ -894,18 +1141,12 @@ size_t workspace_doubles(const Geometry& g) {
 }
 
 cudaError_t launch_init(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s) {
-  if (g.vec == 2)
-    k0_init<2><<<g.grid, kThreads, 0, s>>>(B, g, cfg);
-  else
-    k0_init<1><<<g.grid, kThreads, 0, s>>>(B, g, cfg);
+  PDOT_VARIANT(g, k0_init, (kfn<<<g.grid, kThreads, 0, s>>>(B, g, cfg)));
   return cudaGetLastError();
 }
 
 cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s) {
-  if (g.vec == 2)
-    k1_primal<2><<<g.grid, kThreads, 0, s>>>(B, g);
-  else
-    k1_primal<1><<<g.grid, kThreads, 0, s>>>(B, g);
+  PDOT_VARIANT(g, k1_primal, (kfn<<<g.grid, kThreads, 0, s>>>(B, g)));
   return cudaGetLastError();
 }
 
@@ -921,10 +1162,7 @@ cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& 
 }
 
 cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s) {
-  if (g.vec == 2)
-    k3_eval<2><<<g.grid, kThreads, 0, s>>>(B, g);
-  else
-    k3_eval<1><<<g.grid, kThreads, 0, s>>>(B, g);
+  PDOT_VARIANT(g, k3_eval, (kfn<<<g.grid, kThreads, 0, s>>>(B, g)));
   k4_eval<<<g.row_blocks + g.col_blocks, kVecThreads, 0, s>>>(B, g, cfg);
   return cudaGetLastError();
 }
@@ -936,7 +1174,7 @@ cudaError_t launch_primal_pass(const Geometry& g, const double* C, double* X, do
   double* rowpart = work;
   double* colpart = rowpart + ((size_t)g.grid + g.panels) * kPanelRows;
   double* sqpart = colpart + (size_t)g.panels * g.n;
-  if (g.vec == 2)
+  if (g.vec > 1)
     k1_primal_args<2><<<g.grid, kThreads, 0, s>>>(C, X, Xa, u, v, step_over_weight, avg_new_weight, avg_scale,
                                                   flags, colpart, rowpart, sqpart, g);
   else
@@ -944,6 +1182,16 @@ cudaError_t launch_primal_pass(const Geometry& g, const double* C, double* X, do
                                                   flags, colpart, rowpart, sqpart, g);
   k_pass_sums<<<g.row_blocks + g.col_blocks + 1, kVecThreads, 0, s>>>(g, rowpart, colpart, sqpart, drow, dcol,
                                                                       dsq);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_convert_cost(const double* src, void* dst, int cost_kind, size_t count, cudaStream_t s) {
+  k_convert_cost<<<4 * 148, 256, 0, s>>>(src, dst, cost_kind, count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_widen(const float* src, double* dst, size_t count, cudaStream_t s) {
+  k_widen<<<4 * 148, 256, 0, s>>>(src, dst, count);
   return cudaGetLastError();
 }
 

@@ -70,12 +70,28 @@ class PdhgParametersC(ct.Structure):
     ]
 
 
+PRECISION_F64 = 0
+PRECISION_F32 = 1
+COST_F64 = 0
+COST_F32 = 1
+COST_BF16 = 2
+COST_SQEUCLID_POINTS = 3
+
+
 class SolverOptionsC(ct.Structure):
     _fields_ = [
         ("device", ct.c_int32),
         ("use_cuda_graph", ct.c_int32),
         ("time_kernels", ct.c_int32),
-        ("reserved", ct.c_int32 * 13),
+        ("plan_precision", ct.c_int32),
+        ("cost_storage", ct.c_int32),
+        ("point_dim", ct.c_int32),
+        ("source_points", ct.POINTER(ct.c_float)),
+        ("target_points", ct.POINTER(ct.c_float)),
+        ("cost_scale", ct.c_double),
+        ("warm_dual_source", ct.POINTER(ct.c_double)),
+        ("warm_dual_target", ct.POINTER(ct.c_double)),
+        ("reserved", ct.c_int32 * 8),
     ]
 
 

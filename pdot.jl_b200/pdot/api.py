@@ -285,20 +285,26 @@ def marshal_params(params: PdhgParameters) -> _abi.PdhgParametersC:
 
 
 class MarshalledProblem:
-    """Keeps the column-major host arrays alive for the duration of a call."""
+    """Keeps the column-major host arrays alive for the duration of a call.
+    A problem whose cost comes from coordinates may have cost_matrix None."""
 
     def __init__(self, problem: OptimalTransportProblem):
-        C = np.asarray(problem.cost_matrix, dtype=np.float64)
-        if C.ndim != 2:
-            raise ValueError("cost_matrix must be a matrix")
-        self.C = np.asfortranarray(C)
         self.a = np.ascontiguousarray(problem.source_distribution, dtype=np.float64).ravel()
         self.b = np.ascontiguousarray(problem.target_distribution, dtype=np.float64).ravel()
-        m, n = self.C.shape
-        if self.a.shape[0] != m or self.b.shape[0] != n:
-            raise ValueError("distribution lengths must match the cost matrix shape")
+        m, n = self.a.shape[0], self.b.shape[0]
+        if problem.cost_matrix is None:
+            self.C = None
+            cptr = None
+        else:
+            C = np.asarray(problem.cost_matrix, dtype=np.float64)
+            if C.ndim != 2:
+                raise ValueError("cost_matrix must be a matrix")
+            self.C = np.asfortranarray(C)
+            if self.C.shape != (m, n):
+                raise ValueError("distribution lengths must match the cost matrix shape")
+            cptr = _dptr(self.C)
         self.m, self.n = m, n
-        self.c = _abi.ProblemC(m, n, _dptr(self.C), _dptr(self.a), _dptr(self.b))
+        self.c = _abi.ProblemC(m, n, cptr, _dptr(self.a), _dptr(self.b))
 
 
 def stats_from_c(s: _abi.IterationStatsC) -> IterationStats:
@@ -357,22 +363,77 @@ def validate(params: PdhgParameters) -> None:
 
 
 # ---------------------------------------------------------------- optimize
-def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False) -> _abi.SolverOptionsC:
+_PRECISIONS = {"f64": _abi.PRECISION_F64, "f32": _abi.PRECISION_F32}
+_COSTS = {"f64": _abi.COST_F64, "f32": _abi.COST_F32, "bf16": _abi.COST_BF16,
+          "sqeuclid": _abi.COST_SQEUCLID_POINTS}
+
+
+def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, precision: str = "f64",
+             cost: Optional[str] = None, points=None, cost_scale: Optional[float] = None, warm_start=None,
+             device_pointers: bool = False):
+    """Build pdot_solver_options. Returns (options, objects to keep alive).
+
+    precision  "f64" (the drop-in) or "f32" (mixed precision: FP32 plan)
+    cost       "f64", "f32", "bf16" or "sqeuclid" (from `points`); defaults to
+               "f64" for an FP64 plan and "f32" for an FP32 plan
+    points     (xs, ys) coordinate arrays (m x d, n x d) for "sqeuclid"; with
+               device_pointers, (xs_ptr, ys_ptr, d)
+    warm_start (u0, v0) initial duals; with device_pointers, (u_ptr, v_ptr)
+    """
+    keep = []
     opts = _abi.SolverOptionsC()
     opts.device = device
     opts.use_cuda_graph = 1 if use_cuda_graph else 0
     opts.time_kernels = 1 if time_kernels else 0
-    return opts
+    opts.plan_precision = _PRECISIONS[precision]
+    if cost is None:
+        cost = "f64" if precision == "f64" else "f32"
+    opts.cost_storage = _COSTS[cost]
+    if cost == "sqeuclid":
+        if points is None:
+            raise ValueError("the sqeuclid cost needs point coordinates")
+        if device_pointers:
+            xs_ptr, ys_ptr, dim = points
+            opts.source_points = ct.cast(ct.c_void_p(xs_ptr), ct.POINTER(ct.c_float))
+            opts.target_points = ct.cast(ct.c_void_p(ys_ptr), ct.POINTER(ct.c_float))
+        else:
+            xs = np.ascontiguousarray(points[0], dtype=np.float32)
+            ys = np.ascontiguousarray(points[1], dtype=np.float32)
+            if xs.ndim == 1:
+                xs, ys = xs[:, None], ys[:, None]
+            dim = xs.shape[1]
+            keep += [xs, ys]
+            opts.source_points = xs.ctypes.data_as(ct.POINTER(ct.c_float))
+            opts.target_points = ys.ctypes.data_as(ct.POINTER(ct.c_float))
+        opts.point_dim = int(dim)
+        opts.cost_scale = float(cost_scale) if cost_scale else 0.0
+    if warm_start is not None:
+        if device_pointers:
+            opts.warm_dual_source = ct.cast(ct.c_void_p(warm_start[0]), ct.POINTER(ct.c_double))
+            opts.warm_dual_target = ct.cast(ct.c_void_p(warm_start[1]), ct.POINTER(ct.c_double))
+        else:
+            u0 = np.ascontiguousarray(warm_start[0], dtype=np.float64)
+            v0 = np.ascontiguousarray(warm_start[1], dtype=np.float64)
+            keep += [u0, v0]
+            opts.warm_dual_source = _dptr(u0)
+            opts.warm_dual_target = _dptr(v0)
+    return opts, keep
 
 
 def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device: int = 0,
-             use_cuda_graph: bool = True) -> SaddlePointOutput:
-    """PDOT.optimize, src/solver_gpu.jl:413-720, run by libpdot.so on the GPU."""
+             use_cuda_graph: bool = True, precision: str = "f64", cost: Optional[str] = None, points=None,
+             cost_scale: Optional[float] = None, warm_start=None) -> SaddlePointOutput:
+    """PDOT.optimize, src/solver_gpu.jl:413-720, run by libpdot.so on the GPU.
+
+    The keyword options beyond `device` select this implementation's mixed
+    precision (FP32 plan; FP32/BF16/coordinate cost) and a warm start from
+    given duals; the defaults are the FP64 drop-in."""
     validate(params)
     lib = _abi.load()
     mp = MarshalledProblem(problem)
     cp = marshal_params(params)
-    opts = _options(device, use_cuda_graph)
+    opts, _keep = _options(device, use_cuda_graph, precision=precision, cost=cost, points=points,
+                           cost_scale=cost_scale, warm_start=warm_start)
     ob = OutputBuffers(mp.m, mp.n, stats_capacity_for(params))
     rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
     _abi.check(lib, rc, "pdot_optimize")
@@ -387,16 +448,19 @@ class Solver:
 
     def __init__(self, params: PdhgParameters, problem: Optional[OptimalTransportProblem] = None, *,
                  device_problem=None, device: int = 0, use_cuda_graph: bool = True,
-                 time_kernels: bool = False):
+                 time_kernels: bool = False, precision: str = "f64", cost: Optional[str] = None,
+                 points=None, cost_scale: Optional[float] = None, warm_start=None):
         validate(params)
         self._lib = _abi.load()
         self._params = params
         self._cp = marshal_params(params)
-        opts = _options(device, use_cuda_graph, time_kernels)
+        opts, self._keep = _options(device, use_cuda_graph, time_kernels, precision=precision, cost=cost,
+                                    points=points, cost_scale=cost_scale, warm_start=warm_start,
+                                    device_pointers=device_problem is not None)
         handle = ct.c_void_p()
         if device_problem is not None:
             m, n, cptr, aptr, bptr = device_problem
-            pc = _abi.ProblemC(m, n, ct.cast(ct.c_void_p(cptr), ct.POINTER(ct.c_double)),
+            pc = _abi.ProblemC(m, n, ct.cast(ct.c_void_p(cptr or 0), ct.POINTER(ct.c_double)),
                                ct.cast(ct.c_void_p(aptr), ct.POINTER(ct.c_double)),
                                ct.cast(ct.c_void_p(bptr), ct.POINTER(ct.c_double)))
             rc = self._lib.pdot_solver_create_device(ct.byref(pc), ct.byref(self._cp), ct.byref(opts),

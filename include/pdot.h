@@ -135,6 +135,12 @@ enum {
   PDOT_COST_SQEUCLID_POINTS = 3   /* C_ij = scale*||x_i - y_j||^2 computed on the fly
                                    * from FP32 coordinates; cost_matrix may be NULL */
 };
+/* How the fused primal pass reads its operands: with direct 16-byte vector
+ * loads, or staged through shared memory by bulk copies with an mbarrier per
+ * stage (where the buffers are 16-byte aligned). PDOT_PASS_AUTO picks the one
+ * measured faster on B200: staged for BF16 and coordinate costs, direct for
+ * FP64 and FP32 costs. */
+enum { PDOT_PASS_AUTO = 0, PDOT_PASS_STAGED = 1, PDOT_PASS_DIRECT = 2 };
 typedef struct pdot_solver_options {
   int32_t device;                     /* CUDA device ordinal */
   int32_t use_cuda_graph;             /* 1: replay captured iteration chunks */
@@ -147,7 +153,8 @@ typedef struct pdot_solver_options {
   double cost_scale;                  /* > 0: the scale; <= 0: 1 / max_ij ||x_i - y_j||^2 */
   const double* warm_dual_source;     /* m initial source duals, or NULL (zero start) */
   const double* warm_dual_target;     /* n initial target duals, or NULL */
-  int32_t reserved[8];                /* must be zero */
+  int32_t primal_pass;                /* PDOT_PASS_AUTO, _STAGED or _DIRECT */
+  int32_t reserved[7];                /* must be zero */
 } pdot_solver_options;
 
 /* ---- output -------------------------------------------------------------- */

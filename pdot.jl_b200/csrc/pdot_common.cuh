@@ -47,6 +47,8 @@ struct Geometry {
   int32_t col_blocks;  // CTAs of the vector passes covering n
   int32_t plan_f32;    // 1: FP32 plan and average, 0: FP64
   int32_t cost_kind;   // PDOT_COST_F64 / _F32 / _BF16, or kCostSqBase + point dim
+  int32_t tma;         // 1: the fused pass stages its operands with bulk copies
+  int32_t tma_smem;    // dynamic shared memory of the staged pass (bytes)
 };
 
 // Where the cost entries come from.
@@ -110,10 +112,11 @@ struct DevState {
   int buf;                   // which half of each pair is the current iterate
   int out_current;           // at termination: 1 = return current, 0 = average
   int last_restart_choice;
+  int kernel_error;          // non-zero: a bounded wait in a kernel timed out
   unsigned int ticket_step;  // last-CTA tickets
   unsigned int ticket_eval;
   unsigned int ticket_init;
-  int pad_[2];
+  int pad_[1];
 };
 
 // Parameters of one solve, passed by value to the control kernels.
@@ -158,8 +161,10 @@ struct Buffers {
 };
 
 // ---- launchers (pdot_kernels.cu) ----------------------------------------
+// vec_ok: the cost and plan buffers are 16-byte aligned (vector and staged
+// paths allowed); staged_ok: the fused pass may use the bulk-copy staging.
 Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device, int plan_f32 = 0,
-                       int cost_kind = PDOT_COST_F64);
+                       int cost_kind = PDOT_COST_F64, int staged_ok = 0);
 size_t workspace_doubles(const Geometry& g);
 
 cudaError_t launch_init(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);

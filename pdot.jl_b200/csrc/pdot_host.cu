@@ -125,6 +125,7 @@ struct Variant {
   double cost_scale = 0.0;
   const double* warm_u = nullptr;
   const double* warm_v = nullptr;
+  int staged = 2;  // 0 direct, 1 staged, 2 automatic
 };
 
 Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
@@ -160,7 +161,10 @@ Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
     fail(PDOT_ERR_INVALID_ARGUMENT, "give both warm-start dual vectors or neither");
   v.warm_u = o->warm_dual_source;
   v.warm_v = o->warm_dual_target;
-  for (int k = 0; k < 8; ++k)
+  if (o->primal_pass != PDOT_PASS_AUTO && o->primal_pass != PDOT_PASS_STAGED && o->primal_pass != PDOT_PASS_DIRECT)
+    fail(PDOT_ERR_INVALID_ARGUMENT, "unknown primal_pass %d", o->primal_pass);
+  v.staged = o->primal_pass == PDOT_PASS_STAGED ? 1 : (o->primal_pass == PDOT_PASS_DIRECT ? 0 : 2);
+  for (int k = 0; k < 7; ++k)
     if (o->reserved[k] != 0) fail(PDOT_ERR_INVALID_ARGUMENT, "reserved option fields must be zero");
   return v;
 }
@@ -270,7 +274,7 @@ class Solver {
       cost_.C = Cs;
     }
     const int kind = var.cost_kind == PDOT_COST_SQEUCLID_POINTS ? pdot::kCostSqBase + var.point_dim : var.cost_kind;
-    g_ = pdot::make_geometry(m, n, cost_aligned ? 1 : 0, device_, var.plan_f32, kind);
+    g_ = pdot::make_geometry(m, n, cost_aligned ? 1 : 0, device_, var.plan_f32, kind, var.staged);
     if (device_inputs) {
       a_ = P.source_distribution;
       b_ = P.target_distribution;
@@ -418,6 +422,11 @@ class Solver {
       collect_timings(slot);
       ++completed;
       drain();
+      if (status_.kernel_error) {
+        sync_all(issued, completed);
+        fail(PDOT_ERR_CUDA, "a bounded wait in the fused primal pass timed out (kernel_error %d)",
+             status_.kernel_error);
+      }
       if (status_.done) break;
       if (status_.numerical_error) {
         // The step kernels stop once a numerical error is flagged; the next

@@ -453,6 +453,252 @@ __global__ void __launch_bounds__(kThreads, 2)
                                              (flags & PDOT_PASS_FIRST_AVERAGE) != 0, colpart, rowpart, sqpart, g);
 }
 
+// ---------------------------------------------------------------------------
+// The fused primal pass with bulk-copy staging. Each warp keeps an S-stage
+// ring in shared memory; lane 0 issues cp.async.bulk copies of the cost, plan
+// and average segments of its next units (one mbarrier per stage, completed by
+// the copies' byte count), so the bytes in flight no longer depend on the
+// registers a lane can hold. Results are written straight to global memory.
+// Every wait is bounded: on a timeout the kernel records kernel_error, waits
+// (bounded) for the copies it still has in flight and returns.
+constexpr int kSpinLimit = 1 << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+  for (int it = 0; it < kSpinLimit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// The units of warp w inside [q0, q1): column w, w+8, ... of each panel segment.
+struct UnitCursor {
+  int64_t p, j, je, q1, n;
+  bool valid;
+  __device__ __forceinline__ void init(int64_t q0, int64_t q1_, int64_t n_, int w) {
+    q1 = q1_;
+    n = n_;
+    p = q0 / n;
+    const int64_t jb = (q0 > p * n ? q0 : p * n) - p * n;
+    je = (q1 < (p + 1) * n ? q1 : (p + 1) * n) - p * n;
+    j = jb + w;
+    valid = true;
+    normalize(w);
+  }
+  __device__ __forceinline__ void normalize(int w) {
+    while (j >= je) {
+      ++p;
+      if (p * n >= q1) {
+        valid = false;
+        return;
+      }
+      je = (q1 < (p + 1) * n ? q1 : (p + 1) * n) - p * n;
+      j = w;
+    }
+  }
+  __device__ __forceinline__ void advance(int w) {
+    j += kWarps;
+    normalize(w);
+  }
+};
+
+template <typename TX, int CK>
+struct StagedLayout {
+  static constexpr bool kSq = is_sq_cost(CK);
+  using TC = typename CostReader<CK, 16 / sizeof(TX), kPanelRows / (32 * (16 / sizeof(TX)))>::value_t;
+  static constexpr int kCBytes = kSq ? 0 : kPanelRows * (int)sizeof(TC);
+  static constexpr int kXBytes = kPanelRows * (int)sizeof(TX);
+  static constexpr int kStageBytes = kCBytes + 2 * kXBytes;
+  // stages per warp: two CTAs (16 warps) per SM fit in shared memory
+  static constexpr int S0 = (96 * 1024) / (kWarps * kStageBytes);
+  static constexpr int S = S0 > 6 ? 6 : (S0 < 2 ? 2 : S0);
+  static constexpr int kRingBytes = kWarps * S * kStageBytes;
+  static constexpr int kSmem = kRingBytes + kWarps * S * 8;  // plus the mbarriers
+};
+
+template <typename TX, int CK>
+__global__ void __launch_bounds__(kThreads, 2) k1_primal_staged(Buffers B, Geometry g) {
+  using L = StagedLayout<TX, CK>;
+  constexpr int R = 16 / sizeof(TX);
+  constexpr int RPL = kPanelRows / (32 * R);
+  constexpr int S = L::S;
+  using TC = typename L::TC;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ double red[kWarps][kPanelRows];
+  __shared__ double sqw[kWarps];
+  DevState* st = B.st;
+  if (st->done | st->numerical_error) return;
+  const int buf = st->buf;
+  const double tau = st->step_size, omega = st->primal_weight, Ssum = st->sum_weights;
+  const bool zero_g = st->g_is_zero != 0;
+  const bool first = !(Ssum > 0.0);
+  const double s = __ddiv_rn(tau, omega);
+  const double nw = first ? 1.0 : __ddiv_rn(tau, Ssum);
+  const double aw = first ? 1.0 : __ddiv_rn(Ssum, __dadd_rn(Ssum, tau));
+  TX* __restrict__ X = static_cast<TX*>(B.X[buf]);
+  TX* __restrict__ Xa = static_cast<TX*>(B.X[buf ^ 1]);
+  const double* __restrict__ u = B.u[buf];
+  const double* __restrict__ v = B.v[buf];
+  const TC* __restrict__ Cg = static_cast<const TC*>(B.cost.C);
+  CostReader<CK, R, RPL> cost(B.cost, (float)st->cost_scale);
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t m = g.m, n = g.n;
+  const int64_t cta = blockIdx.x;
+  const int64_t q0 = unit_begin(g, cta), q1 = unit_begin(g, cta + 1);
+  unsigned char* ring = smem + (size_t)warp * S * L::kStageBytes;
+  const uint32_t bar0 = smem_u32(smem + L::kRingBytes) + (uint32_t)(warp * S * 8);
+  if (lane == 0) {
+    for (int k = 0; k < S; ++k) mbar_init(bar0 + 8 * k, 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+
+  // lane 0 fills stage k with unit (p, j)
+  auto issue = [&](int64_t p, int64_t j, int k) {
+    const int64_t row0 = p * kPanelRows;
+    const int64_t rows = (m - row0) < kPanelRows ? (m - row0) : kPanelRows;
+    const uint32_t xb = (uint32_t)(rows * sizeof(TX));
+    const uint32_t cb = L::kSq ? 0u : (uint32_t)(rows * sizeof(TC));
+    const uint32_t bar = bar0 + 8 * k;
+    unsigned char* stg = ring + (size_t)k * L::kStageBytes;
+    const int64_t off = j * m + row0;
+    mbar_expect_tx(bar, cb + xb + (first ? 0u : xb));
+    if (!L::kSq) bulk_g2s(smem_u32(stg), Cg + off, cb, bar);
+    bulk_g2s(smem_u32(stg + L::kCBytes), X + off, xb, bar);
+    if (!first) bulk_g2s(smem_u32(stg + L::kCBytes + L::kXBytes), Xa + off, xb, bar);
+  };
+
+  UnitCursor prod, cons;
+  prod.init(q0, q1, n, warp);
+  cons.init(q0, q1, n, warp);
+  long long issued = 0, consumed = 0;
+  for (int k = 0; k < S && prod.valid; ++k) {
+    if (lane == 0) issue(prod.p, prod.j, k);
+    prod.advance(warp);
+    ++issued;
+  }
+  bool failed = false;
+  double sq = 0.0;
+  for (int64_t p = q0 / n; p * n < q1; ++p) {
+    const int64_t row0 = p * kPanelRows;
+    double acc[RPL][R];
+    double ur[RPL][R];
+    bool ok[RPL];
+#pragma unroll
+    for (int k = 0; k < RPL; ++k) {
+      const int64_t i = row0 + k * 32 * R + lane * R;
+      ok[k] = i < m;
+#pragma unroll
+      for (int e = 0; e < R; ++e) {
+        acc[k][e] = 0.0;
+        ur[k][e] = (ok[k] && !zero_g) ? __ldg(u + i + e) : 0.0;
+      }
+    }
+    cost.panel(row0, lane, m, ok);
+    while (!failed && cons.valid && cons.p == p) {
+      const int64_t j = cons.j;
+      const int stage = (int)(consumed % S);
+      const uint32_t parity = (uint32_t)((consumed / S) & 1);
+      if (!mbar_wait_bounded(bar0 + 8 * stage, parity)) {
+        failed = true;
+        break;
+      }
+      const unsigned char* stg = ring + (size_t)stage * L::kStageBytes;
+      const TC* sC = reinterpret_cast<const TC*>(stg);
+      const TX* sX = reinterpret_cast<const TX*>(stg + L::kCBytes);
+      const TX* sXa = reinterpret_cast<const TX*>(stg + L::kCBytes + L::kXBytes);
+      const double vj = zero_g ? 0.0 : __ldg(v + j);
+      cost.column(j);
+      const int64_t base = j * m + row0 + lane * R;
+      double cs = 0.0;
+#pragma unroll
+      for (int k = 0; k < RPL; ++k) {
+        if (ok[k]) {
+          const int r = k * 32 * R + lane * R;
+          typename CostReader<CK, R, RPL>::value_t cv[R];
+          if constexpr (L::kSq)
+            cost.get(0, k, cv);
+          else
+            vld<TC, R>(sC + r, cv);
+          TX xv[R], av[R];
+          vld<TX, R>(sX + r, xv);
+          if (!first) vld<TX, R>(sXa + r, av);
+#pragma unroll
+          for (int e = 0; e < R; ++e) {
+            double d;
+            primal_entry<TX>(widen(cv[e]), ur[k][e], vj, s, nw, aw, zero_g, first, xv[e], av[e], d);
+            acc[k][e] += d;
+            cs += d;
+            sq += d * d;
+          }
+          vst<TX, R>(X + base + k * 32 * R, xv);
+          vst<TX, R>(Xa + base + k * 32 * R, av);
+        }
+      }
+      cs = warp_sum(cs);
+      if (lane == 0) B.colpart[p * n + j] = cs;
+      __syncwarp();
+      ++consumed;
+      cons.advance(warp);
+      if (prod.valid) {
+        if (lane == 0) issue(prod.p, prod.j, stage);
+        prod.advance(warp);
+        ++issued;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < RPL; ++k)
+#pragma unroll
+      for (int e = 0; e < R; ++e) red[warp][k * 32 * R + lane * R + e] = acc[k][e];
+    __syncthreads();
+    for (int t = threadIdx.x; t < kPanelRows; t += kThreads) {
+      double s2 = red[0][t];
+#pragma unroll
+      for (int w = 1; w < kWarps; ++w) s2 += red[w][t];
+      B.rowpart[row_slot(cta, p) * kPanelRows + t] = s2;
+    }
+    __syncthreads();
+  }
+  if (failed) {
+    // drain the copies still in flight (bounded) before the shared memory goes away
+    if (lane == 0) atomicExch(&st->kernel_error, 1);
+    for (long long c = consumed; c < issued; ++c)
+      mbar_wait_bounded(bar0 + 8 * (int)(c % S), (uint32_t)((c / S) & 1));
+  }
+  sq = warp_sum(sq);
+  if (lane == 0) sqw[warp] = sq;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s2 = sqw[0];
+#pragma unroll
+    for (int w = 1; w < kWarps; ++w) s2 += sqw[w];
+    B.sqpart[cta] = s2;
+  }
+}
+
 // Second stage of the row sum of row i / column sum of column j.
 __device__ __forceinline__ double finish_row_sum(const Geometry& g, const double* rowpart, int64_t i) {
   const int64_t p = i / kPanelRows, t = i - p * kPanelRows;
@@ -1108,7 +1354,26 @@ __global__ void k_widen(const float* __restrict__ src, double* __restrict__ dst,
     }                                                                                      \
   } while (0)
 
-Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device, int plan_f32, int cost_kind) {
+// The staged fused pass exists for the 16-byte path of every variant.
+#define PDOT_STAGED_VARIANT(g, LAUNCH)                                                              \
+  do {                                                                                            \
+    if (!(g).plan_f32) { auto kfn = k1_primal_staged<double, PDOT_COST_F64>;                     \
+      constexpr int smem = StagedLayout<double, PDOT_COST_F64>::kSmem; LAUNCH; }                 \
+    else if ((g).cost_kind == PDOT_COST_F32) { auto kfn = k1_primal_staged<float, PDOT_COST_F32>; \
+      constexpr int smem = StagedLayout<float, PDOT_COST_F32>::kSmem; LAUNCH; }                  \
+    else if ((g).cost_kind == PDOT_COST_BF16) { auto kfn = k1_primal_staged<float, PDOT_COST_BF16>; \
+      constexpr int smem = StagedLayout<float, PDOT_COST_BF16>::kSmem; LAUNCH; }                 \
+    else if ((g).cost_kind == kCostSqBase + 1) { auto kfn = k1_primal_staged<float, kCostSqBase + 1>; \
+      constexpr int smem = StagedLayout<float, kCostSqBase + 1>::kSmem; LAUNCH; }                \
+    else if ((g).cost_kind == kCostSqBase + 2) { auto kfn = k1_primal_staged<float, kCostSqBase + 2>; \
+      constexpr int smem = StagedLayout<float, kCostSqBase + 2>::kSmem; LAUNCH; }                \
+    else if ((g).cost_kind == kCostSqBase + 3) { auto kfn = k1_primal_staged<float, kCostSqBase + 3>; \
+      constexpr int smem = StagedLayout<float, kCostSqBase + 3>::kSmem; LAUNCH; }                \
+    else { auto kfn = k1_primal_staged<float, kCostSqBase + 4>;                                   \
+      constexpr int smem = StagedLayout<float, kCostSqBase + 4>::kSmem; LAUNCH; }                \
+  } while (0)
+
+Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device, int plan_f32, int cost_kind, int staged_ok) {
   Geometry g;
   g.m = m;
   g.n = n;
@@ -1120,8 +1385,26 @@ Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device, int plan_f3
   g.vec = (vec_ok && (m % R == 0)) ? R : 1;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  // The staged pass needs 16-byte aligned segments: the vector path, and for a
+  // BF16 cost m divisible by 8 (8 two-byte entries per 16 bytes). staged_ok:
+  // 0 never, 1 always, 2 where it measured faster on B200 (BF16 and coordinate
+  // costs, whose direct loads keep too few bytes in flight per warp).
+  const bool want = staged_ok == 1 || (staged_ok == 2 && (cost_kind == PDOT_COST_BF16 || is_sq_cost(cost_kind)));
+  g.tma = (want && g.vec > 1 && !(cost_kind == PDOT_COST_BF16 && m % 8 != 0)) ? 1 : 0;
+  g.tma_smem = 0;
   int occ = 1;
-  PDOT_VARIANT(g, k1_primal, occ = blocks_per_sm(kfn));
+  if (g.tma) {
+    PDOT_STAGED_VARIANT(g, {
+      g.tma_smem = smem;
+      if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, kThreads, smem) != cudaSuccess || occ < 1) {
+        cudaGetLastError();
+        g.tma = 0;
+        occ = 1;
+      }
+    });
+  }
+  if (!g.tma) PDOT_VARIANT(g, k1_primal, occ = blocks_per_sm(kfn));
   int64_t grid = (int64_t)sms * occ;
   if (grid > g.units) grid = g.units;
   g.grid = (int32_t)grid;
@@ -1146,7 +1429,10 @@ cudaError_t launch_init(const Buffers& B, const Geometry& g, const SolveConfig& 
 }
 
 cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s) {
-  PDOT_VARIANT(g, k1_primal, (kfn<<<g.grid, kThreads, 0, s>>>(B, g)));
+  if (g.tma)
+    PDOT_STAGED_VARIANT(g, (kfn<<<g.grid, kThreads, smem, s>>>(B, g)));
+  else
+    PDOT_VARIANT(g, k1_primal, (kfn<<<g.grid, kThreads, 0, s>>>(B, g)));
   return cudaGetLastError();
 }
 

@@ -76,6 +76,9 @@ COST_F64 = 0
 COST_F32 = 1
 COST_BF16 = 2
 COST_SQEUCLID_POINTS = 3
+PASS_AUTO = 0
+PASS_STAGED = 1
+PASS_DIRECT = 2
 
 
 class SolverOptionsC(ct.Structure):
@@ -91,7 +94,8 @@ class SolverOptionsC(ct.Structure):
         ("cost_scale", ct.c_double),
         ("warm_dual_source", ct.POINTER(ct.c_double)),
         ("warm_dual_target", ct.POINTER(ct.c_double)),
-        ("reserved", ct.c_int32 * 8),
+        ("primal_pass", ct.c_int32),
+        ("reserved", ct.c_int32 * 7),
     ]
 
 

@@ -370,7 +370,7 @@ _COSTS = {"f64": _abi.COST_F64, "f32": _abi.COST_F32, "bf16": _abi.COST_BF16,
 
 def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, precision: str = "f64",
              cost: Optional[str] = None, points=None, cost_scale: Optional[float] = None, warm_start=None,
-             device_pointers: bool = False):
+             device_pointers: bool = False, primal_pass: str = "auto"):
     """Build pdot_solver_options. Returns (options, objects to keep alive).
 
     precision  "f64" (the drop-in) or "f32" (mixed precision: FP32 plan)
@@ -389,6 +389,7 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
     if cost is None:
         cost = "f64" if precision == "f64" else "f32"
     opts.cost_storage = _COSTS[cost]
+    opts.primal_pass = {"auto": _abi.PASS_AUTO, "staged": _abi.PASS_STAGED, "direct": _abi.PASS_DIRECT}[primal_pass]
     if cost == "sqeuclid":
         if points is None:
             raise ValueError("the sqeuclid cost needs point coordinates")
@@ -422,7 +423,7 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
 
 def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device: int = 0,
              use_cuda_graph: bool = True, precision: str = "f64", cost: Optional[str] = None, points=None,
-             cost_scale: Optional[float] = None, warm_start=None) -> SaddlePointOutput:
+             cost_scale: Optional[float] = None, warm_start=None, primal_pass: str = "auto") -> SaddlePointOutput:
     """PDOT.optimize, src/solver_gpu.jl:413-720, run by libpdot.so on the GPU.
 
     The keyword options beyond `device` select this implementation's mixed
@@ -433,7 +434,7 @@ def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device
     mp = MarshalledProblem(problem)
     cp = marshal_params(params)
     opts, _keep = _options(device, use_cuda_graph, precision=precision, cost=cost, points=points,
-                           cost_scale=cost_scale, warm_start=warm_start)
+                           cost_scale=cost_scale, warm_start=warm_start, primal_pass=primal_pass)
     ob = OutputBuffers(mp.m, mp.n, stats_capacity_for(params))
     rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
     _abi.check(lib, rc, "pdot_optimize")
@@ -449,14 +450,14 @@ class Solver:
     def __init__(self, params: PdhgParameters, problem: Optional[OptimalTransportProblem] = None, *,
                  device_problem=None, device: int = 0, use_cuda_graph: bool = True,
                  time_kernels: bool = False, precision: str = "f64", cost: Optional[str] = None,
-                 points=None, cost_scale: Optional[float] = None, warm_start=None):
+                 points=None, cost_scale: Optional[float] = None, warm_start=None, primal_pass: str = "auto"):
         validate(params)
         self._lib = _abi.load()
         self._params = params
         self._cp = marshal_params(params)
         opts, self._keep = _options(device, use_cuda_graph, time_kernels, precision=precision, cost=cost,
                                     points=points, cost_scale=cost_scale, warm_start=warm_start,
-                                    device_pointers=device_problem is not None)
+                                    device_pointers=device_problem is not None, primal_pass=primal_pass)
         handle = ct.c_void_p()
         if device_problem is not None:
             m, n, cptr, aptr, bptr = device_problem

@@ -305,6 +305,26 @@ int pdot_primal_pass_f64(int64_t m, int64_t n,
                          double* delta_row_sum, double* delta_col_sum, double* delta_sq_norm,
                          void* workspace, int64_t workspace_bytes, void* stream);
 
+/* ---- passes around a solve ------------------------------------------------ */
+
+/* The feasibility rounding of a plan, src/utils_gpu.jl:296-318 (the reference
+ * runs it on the CPU after the solve; scripts/solve.jl:116-117 writes its
+ * result): rows scaled by min(1, a/rowsum), columns by min(1, b/colsum), then
+ * X += err_r err_c^T with err_r = (a - rowsum)/||a - rowsum||_1. In place, on
+ * device arrays and the given stream. */
+int pdot_rounding_f64(int64_t m, int64_t n, const double* source, const double* target, double* plan,
+                      void* stream);
+/* The same on host arrays (copied to `device` and back). */
+int pdot_rounding_host(int64_t m, int64_t n, const double* source, const double* target, double* plan,
+                       int32_t device);
+
+/* C_ij = ||x_i - y_j||^2 (divided by its maximum if `normalise`) into a device
+ * cost matrix (column-major, ld = m) from device FP64 coordinates (m x dim and
+ * n x dim, row-major): builds the problem where it is solved instead of
+ * copying m*n doubles to the device. */
+int pdot_sqeuclid_cost_f64(int64_t m, int64_t n, int32_t dim, const double* source_points,
+                           const double* target_points, int32_t normalise, double* cost, void* stream);
+
 /* The same fused primal pass for callers that cannot allocate device memory
  * (a host framework that hands out its whole memory budget from its own pool,
  * or a latency-critical loop that cannot afford cudaMalloc's implicit device

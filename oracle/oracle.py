@@ -51,6 +51,8 @@ def load():
         ct.POINTER(_abi.ProblemC), ct.POINTER(_abi.PdhgParametersC), ct.c_int, ct.c_int,
         ct.POINTER(ct.c_double),
     ]
+    lib.pdot_oracle_rounding.restype = None
+    lib.pdot_oracle_rounding.argtypes = [ct.c_int64, ct.c_int64, P, P, P]
     lib.pdot_oracle_version.restype = ct.c_int
     _lib = lib
     return lib
@@ -103,3 +105,13 @@ def time_steps(params, problem, steps: int, num_threads: int = 0) -> float:
     if rc != 0:
         raise _abi.PdotError(rc, f"oracle time_steps failed ({rc})")
     return sec.value
+
+
+def rounding(problem, X):
+    """Oracle restatement of the reference's rounding (in place on X)."""
+    lib = load()
+    assert X.flags.f_contiguous and X.dtype == np.float64
+    a = np.ascontiguousarray(problem.source_distribution, dtype=np.float64)
+    b = np.ascontiguousarray(problem.target_distribution, dtype=np.float64)
+    lib.pdot_oracle_rounding(X.shape[0], X.shape[1], _p(a), _p(b), _p(X))
+    return X

@@ -806,4 +806,47 @@ int pdot_oracle_time_steps(const pdot_problem* P, const pdot_pdhg_parameters* pr
   return PDOT_OK;
 }
 
+/* rounding, src/utils_gpu.jl:296-318, in place on a column-major plan. */
+void pdot_oracle_rounding(i64 m, i64 n, const double* a, const double* b, double* X) {
+  double* rs = (double*)zalloc(m);
+  double* cs = (double*)zalloc(n);
+  for (i64 j = 0; j < n; ++j)
+    for (i64 i = 0; i < m; ++i) rs[i] += X[i + j * m];
+  for (i64 i = 0; i < m; ++i) {
+    double t = a[i] / rs[i];
+    if (t != t) t = 0.0;
+    rs[i] = t < 1.0 ? t : 1.0; /* min.(tmp, 1.0) */
+  }
+  for (i64 j = 0; j < n; ++j)
+    for (i64 i = 0; i < m; ++i) X[i + j * m] = rs[i] * X[i + j * m]; /* Diagonal(d) * X */
+  for (i64 j = 0; j < n; ++j) {
+    double s = 0.0;
+    for (i64 i = 0; i < m; ++i) s += X[i + j * m];
+    double t = b[j] / s;
+    if (t != t) t = 0.0;
+    cs[j] = t < 1.0 ? t : 1.0;
+  }
+  for (i64 j = 0; j < n; ++j)
+    for (i64 i = 0; i < m; ++i) X[i + j * m] = X[i + j * m] * cs[j]; /* X * Diagonal(d) */
+  for (i64 i = 0; i < m; ++i) rs[i] = 0.0;
+  for (i64 j = 0; j < n; ++j)
+    for (i64 i = 0; i < m; ++i) rs[i] += X[i + j * m];
+  double n1 = 0.0;
+  for (i64 i = 0; i < m; ++i) {
+    rs[i] = a[i] - rs[i]; /* err_r */
+    n1 += fabs(rs[i]);
+  }
+  if (n1 != 0.0)
+    for (i64 i = 0; i < m; ++i) rs[i] /= n1;
+  for (i64 j = 0; j < n; ++j) {
+    double s = 0.0;
+    for (i64 i = 0; i < m; ++i) s += X[i + j * m];
+    cs[j] = b[j] - s; /* err_c */
+  }
+  for (i64 j = 0; j < n; ++j)
+    for (i64 i = 0; i < m; ++i) X[i + j * m] = X[i + j * m] + rs[i] * cs[j];
+  free(rs);
+  free(cs);
+}
+
 int pdot_oracle_version(void) { return PDOT_ABI_VERSION; }

@@ -178,6 +178,14 @@ cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& 
 cudaError_t launch_convert_cost(const double* src, void* dst, int cost_kind, size_t count, cudaStream_t s);
 cudaError_t launch_widen(const float* src, double* dst, size_t count, cudaStream_t s);
 
+// Passes around a solve (pdot_aux.cu).
+size_t rounding_workspace_doubles(int64_t m, int64_t n);
+cudaError_t launch_rounding(int64_t m, int64_t n, const double* a, const double* b, double* X, double* work,
+                            cudaStream_t s);
+size_t sqeuclid_workspace_doubles();
+cudaError_t launch_sqeuclid_cost(int64_t m, int64_t n, int dim, const double* xs, const double* ys, int normalise,
+                                 double* C, double* work, cudaStream_t s);
+
 // Sets the thread-local text pdot_last_error() returns (pdot_host.cu).
 void set_last_error(const char* msg);
 

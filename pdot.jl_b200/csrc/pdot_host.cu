@@ -805,4 +805,61 @@ int pdot_primal_pass_f64(int64_t m, int64_t n, const double* cost, double* prima
   });
 }
 
+int pdot_rounding_f64(int64_t m, int64_t n, const double* source, const double* target, double* plan,
+                      void* stream) {
+  return guarded([&] {
+    if (m < 1 || n < 1) fail(PDOT_ERR_INVALID_ARGUMENT, "empty matrix");
+    if (!source || !target || !plan) fail(PDOT_ERR_INVALID_ARGUMENT, "null pointer argument");
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double* work = nullptr;
+    CK(cudaMallocAsync(reinterpret_cast<void**>(&work), pdot::rounding_workspace_doubles(m, n) * sizeof(double), s));
+    const cudaError_t e = pdot::launch_rounding(m, n, source, target, plan, work, s);
+    const cudaError_t e2 = cudaFreeAsync(work, s);
+    CK(e);
+    CK(e2);
+  });
+}
+
+int pdot_rounding_host(int64_t m, int64_t n, const double* source, const double* target, double* plan,
+                       int32_t device) {
+  return guarded([&] {
+    if (m < 1 || n < 1) fail(PDOT_ERR_INVALID_ARGUMENT, "empty matrix");
+    if (!source || !target || !plan) fail(PDOT_ERR_INVALID_ARGUMENT, "null pointer argument");
+    require_sm100(device);
+    CK(cudaSetDevice(device));
+    const size_t N = (size_t)m * (size_t)n;
+    double *dX = nullptr, *da = nullptr, *db = nullptr, *work = nullptr;
+    const size_t wbytes = pdot::rounding_workspace_doubles(m, n) * sizeof(double);
+    cudaError_t e = cudaMalloc(&dX, N * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&da, m * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&db, n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&work, wbytes);
+    if (e == cudaSuccess) e = cudaMemcpy(dX, plan, N * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(da, source, m * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(db, target, n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = pdot::launch_rounding(m, n, da, db, dX, work, nullptr);
+    if (e == cudaSuccess) e = cudaMemcpy(plan, dX, N * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(dX);
+    cudaFree(da);
+    cudaFree(db);
+    cudaFree(work);
+    CK(e);
+  });
+}
+
+int pdot_sqeuclid_cost_f64(int64_t m, int64_t n, int32_t dim, const double* source_points,
+                           const double* target_points, int32_t normalise, double* cost, void* stream) {
+  return guarded([&] {
+    if (m < 1 || n < 1 || dim < 1) fail(PDOT_ERR_INVALID_ARGUMENT, "empty problem");
+    if (!source_points || !target_points || !cost) fail(PDOT_ERR_INVALID_ARGUMENT, "null pointer argument");
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double* work = nullptr;
+    CK(cudaMallocAsync(reinterpret_cast<void**>(&work), pdot::sqeuclid_workspace_doubles() * sizeof(double), s));
+    const cudaError_t e = pdot::launch_sqeuclid_cost(m, n, dim, source_points, target_points, normalise, cost, work, s);
+    const cudaError_t e2 = cudaFreeAsync(work, s);
+    CK(e);
+    CK(e2);
+  });
+}
+
 }  // extern "C"

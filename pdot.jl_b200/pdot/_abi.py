@@ -208,6 +208,9 @@ SIGNATURES = {
     "pdot_solver_finish": (ct.c_int, [_P, ct.POINTER(SaddlePointOutputC)]),
     "pdot_solver_stream": (_P, [_P]),
     "pdot_solver_destroy": (None, [_P]),
+    "pdot_rounding_f64": (ct.c_int, [_I64, _I64, _P, _P, _P, _P]),
+    "pdot_rounding_host": (ct.c_int, [_I64, _I64, _P, _P, _P, _I32]),
+    "pdot_sqeuclid_cost_f64": (ct.c_int, [_I64, _I64, _I32, _P, _P, _I32, _P, _P]),
     "pdot_primal_pass_workspace_bytes": (_I64, [_I64, _I64]),
     "pdot_primal_pass_f64_noalloc": (
         ct.c_int,

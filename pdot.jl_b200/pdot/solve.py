@@ -51,26 +51,23 @@ def write_vector_to_file(filename: str, vector) -> None:
             io.write(julia_float_str(x) + "\n")
 
 
-def rounding(problem: api.OptimalTransportProblem, primal_solution: np.ndarray) -> np.ndarray:
-    """src/utils_gpu.jl:296-318: make a plan feasible. Like the reference it
-    modifies `primal_solution` in place and returns it."""
+def rounding(problem: api.OptimalTransportProblem, primal_solution: np.ndarray, *, device: int = 0) -> np.ndarray:
+    """src/utils_gpu.jl:296-318, run on the GPU (pdot_rounding_host): scale the
+    rows, then the columns, onto the marginals and add the rank-one correction.
+    Like the reference it modifies `primal_solution` in place and returns it."""
+    import ctypes as ct
+
+    from . import _abi
+
     X = primal_solution
-    a = np.asarray(problem.source_distribution, dtype=np.float64)
-    b = np.asarray(problem.target_distribution, dtype=np.float64)
-    with np.errstate(divide="ignore", invalid="ignore"):
-        tmp = a / X.sum(axis=1)
-    tmp = np.where(np.isnan(tmp), 0.0, tmp)
-    X *= np.minimum(tmp, 1.0)[:, None]
-    with np.errstate(divide="ignore", invalid="ignore"):
-        tmp = b / X.sum(axis=0)
-    tmp = np.where(np.isnan(tmp), 0.0, tmp)
-    X *= np.minimum(tmp, 1.0)[None, :]
-    err_r = a - X.sum(axis=1)
-    n1 = np.abs(err_r).sum()
-    if n1 != 0.0:
-        err_r = err_r / n1
-    err_c = b - X.sum(axis=0)
-    X += np.outer(err_r, err_c)
+    if not (isinstance(X, np.ndarray) and X.dtype == np.float64 and X.flags.f_contiguous):
+        raise TypeError("primal_solution must be a Fortran-ordered float64 matrix (updated in place)")
+    a = np.ascontiguousarray(problem.source_distribution, dtype=np.float64)
+    b = np.ascontiguousarray(problem.target_distribution, dtype=np.float64)
+    m, n = X.shape
+    lib = _abi.load()
+    rc = lib.pdot_rounding_host(m, n, a.ctypes.data, b.ctypes.data, X.ctypes.data, device)
+    _abi.check(lib, rc, "pdot_rounding_host")
     return X
 
 

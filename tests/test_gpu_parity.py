@@ -323,3 +323,36 @@ def test_staged_and_direct_primal_pass_agree(cuda, precision, cost, m, n):
         ca, cb = a_.convergence_information[0], b_.convergence_information[0]
         assert ca.primal_objective == pytest.approx(cb.primal_objective, rel=1e-9, abs=1e-15)
         assert ca.l2_primal_residual == pytest.approx(cb.l2_primal_residual, rel=1e-9)
+
+
+@pytest.mark.parametrize("m,n", [(1, 5), (7, 5), (300, 129), (1000, 700)])
+def test_rounding_matches_oracle_and_is_feasible(cuda, m, n):
+    """pdot.rounding (the GPU pass of src/utils_gpu.jl:296-318) against the
+    oracle's restatement: same elementwise steps, sums in a different order, so
+    entries agree to 1e-12 relative; the result meets the marginals."""
+    prob = instances.uniform_sqeuclid(m, n, seed=m)
+    out = pdot.optimize(pdot.default_parameters(1e-3), prob)
+    Xg = out.primal_solution.copy(order="F")
+    Xr = out.primal_solution.copy(order="F")
+    pdot.rounding(prob, Xg)
+    oracle.rounding(prob, Xr)
+    np.testing.assert_allclose(Xg, Xr, rtol=1e-12, atol=1e-18)
+    np.testing.assert_allclose(Xg.sum(axis=1), prob.source_distribution, rtol=1e-10, atol=1e-15)
+    np.testing.assert_allclose(Xg.sum(axis=0), prob.target_distribution, rtol=1e-10, atol=1e-15)
+    # non-negative up to rounding: err_c = b - colsum can round a hair below zero
+    assert Xg.min() >= -1e-15
+
+
+def test_device_cost_builder_matches_host_generator(cuda):
+    import torch
+
+    rng = np.random.default_rng(4)
+    m, n, d = 333, 222, 3
+    xs, ys = rng.uniform(0, 1, (m, d)), rng.uniform(0, 1, (n, d))
+    lib = _abi.load()
+    dx, dy = torch.from_numpy(xs).to(cuda), torch.from_numpy(ys).to(cuda)
+    C = torch.empty((n, m), dtype=torch.float64, device=cuda)
+    rc = lib.pdot_sqeuclid_cost_f64(m, n, d, dx.data_ptr(), dy.data_ptr(), 1, C.data_ptr(), None)
+    _abi.check(lib, rc, "pdot_sqeuclid_cost_f64")
+    torch.cuda.synchronize()
+    assert np.array_equal(C.cpu().numpy().T, instances.sqeuclid_cost(xs, ys))

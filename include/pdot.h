@@ -132,8 +132,9 @@ enum {
   PDOT_COST_F64 = 0,              /* the problem's FP64 cost matrix, as given */
   PDOT_COST_F32 = 1,              /* stored in FP32 (converted on the device) */
   PDOT_COST_BF16 = 2,             /* stored in BF16 (converted on the device) */
-  PDOT_COST_SQEUCLID_POINTS = 3   /* C_ij = scale*||x_i - y_j||^2 computed on the fly
+  PDOT_COST_SQEUCLID_POINTS = 3,  /* C_ij = scale*||x_i - y_j||^2 computed on the fly
                                    * from FP32 coordinates; cost_matrix may be NULL */
+  PDOT_COST_L1_POINTS = 4         /* C_ij = scale*||x_i - y_j||_1, likewise */
 };
 /* How the fused primal pass reads its operands: with direct 16-byte vector
  * loads, or staged through shared memory by bulk copies with an mbarrier per
@@ -147,14 +148,15 @@ typedef struct pdot_solver_options {
   int32_t time_kernels;               /* 1: CUDA events around every launch (direct launches) */
   int32_t plan_precision;             /* PDOT_PRECISION_F64 (drop-in) or _F32 (mixed precision) */
   int32_t cost_storage;               /* PDOT_COST_*; anything but F64 needs plan_precision F32 */
-  int32_t point_dim;                  /* 1..4, for PDOT_COST_SQEUCLID_POINTS */
+  int32_t point_dim;                  /* 1..4, for the coordinate costs */
   const float* source_points;         /* m x point_dim, row-major (same memory kind as the problem) */
   const float* target_points;         /* n x point_dim, row-major */
-  double cost_scale;                  /* > 0: the scale; <= 0: 1 / max_ij ||x_i - y_j||^2 */
+  double cost_scale;                  /* > 0: the scale; <= 0: 1 / max_ij of the distance */
   const double* warm_dual_source;     /* m initial source duals, or NULL (zero start) */
   const double* warm_dual_target;     /* n initial target duals, or NULL */
   int32_t primal_pass;                /* PDOT_PASS_AUTO, _STAGED or _DIRECT */
-  int32_t reserved[7];                /* must be zero */
+  int32_t ctas_per_sm;                /* batched solver: CTAs per SM of its matrix passes (0 = most) */
+  int32_t reserved[6];                /* must be zero */
 } pdot_solver_options;
 
 /* ---- output -------------------------------------------------------------- */
@@ -304,6 +306,40 @@ int pdot_primal_pass_f64(int64_t m, int64_t n,
                          int32_t flags,
                          double* delta_row_sum, double* delta_col_sum, double* delta_sq_norm,
                          void* workspace, int64_t workspace_bytes, void* stream);
+
+/* ---- batched solver -------------------------------------------------------
+ * Many independent instances of uneven sizes in one solve: each runs
+ * optimize()'s loop with its own step size, primal weight, restarts and
+ * termination (the instances advance in lockstep, one loop body each per
+ * global iteration, and finished ones drop out). Plans are FP32 and the
+ * cost is stored FP32 (options->cost_storage = PDOT_COST_F32, converted from
+ * the FP64 matrices) or computed from FP32 coordinates (PDOT_COST_SQEUCLID_POINTS
+ * or PDOT_COST_L1_POINTS, point_dim 1..3, each instance normalised by its own
+ * maximum). options->plan_precision must be PDOT_PRECISION_F32. */
+typedef struct pdot_batch_problem {
+  int64_t num_instances;
+  const int64_t* num_rows;                  /* m of each instance */
+  const int64_t* num_cols;                  /* n of each instance */
+  const double* const* cost_matrices;       /* column-major host matrices, or NULL for coordinates */
+  const double* const* source_distributions;
+  const double* const* target_distributions;
+  const float* const* source_points;        /* m x point_dim, row-major, or NULL */
+  const float* const* target_points;        /* n x point_dim */
+} pdot_batch_problem;
+
+typedef struct pdot_batch_output {          /* one per instance; arrays may be NULL */
+  double* primal_solution;                  /* m*n column-major (the returned average, widened) */
+  double* dual_source_solution;             /* m */
+  double* dual_target_solution;             /* n */
+  int32_t termination_reason;
+  int32_t iteration_count;
+  pdot_iteration_stats final_stats;         /* the evaluation that ended this instance */
+} pdot_batch_output;
+
+/* `solve_seconds` (may be NULL) receives the device time of the solve. */
+int pdot_optimize_batched(const pdot_batch_problem* problem, const pdot_pdhg_parameters* params,
+                          const pdot_solver_options* options, pdot_batch_output* outputs,
+                          double* solve_seconds);
 
 /* ---- passes around a solve ------------------------------------------------ */
 

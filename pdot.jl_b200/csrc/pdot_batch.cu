@@ -1,0 +1,1075 @@
+// pdot_batch.cu — many independent OT instances of uneven sizes solved at once.
+//
+// Every instance runs the reference's full loop (src/solver_gpu.jl:413-720)
+// with its own step size, primal weight, averages, restart record and
+// termination; the instances advance in lockstep (one global iteration runs
+// one loop body of every active instance), so they share the evaluation
+// schedule. Plans are FP32 (the mixed-precision arithmetic of pdot_kernels.cu),
+// duals and control FP64; the cost is stored FP32 or computed from FP32
+// coordinates (squared-Euclidean or L1).
+//
+// Work decomposition: the units (one column of one 256-row panel) of all active
+// instances are concatenated into one line and cut into equal contiguous CTA
+// ranges, exactly as the single-instance pass cuts one instance's line. Row
+// partials live in slot (cta + global panel), column partials at the global
+// unit index, per-instance sums of squares and evaluation partials in slot
+// (cta + active index): along the line the owning CTA, the global panel and
+// the active index never decrease and one of them grows at every boundary, so
+// each slot is written by one (CTA, segment) pair. After every evaluation a
+// single CTA rebuilds the list of active instances and its prefix sums, so
+// finished instances cost nothing and the captured CUDA graph stays valid.
+//
+// Each instance's plan is stored column-major with its row count padded to a
+// multiple of 4 (16-byte FP32 vectors); padded rows hold zeros and are masked.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pdot_device.cuh"
+
+namespace pdot {
+namespace {
+
+constexpr int kBR = 4;                       // FP32 rows per lane load
+constexpr int kBRPL = kPanelRows / (32 * kBR);  // loads per lane per unit
+constexpr int kMaxBatch = 1 << 16;
+
+struct BatchInstance {
+  int64_t m, n, ld;  // rows, columns, padded leading dimension
+  int64_t x_off;     // offset of the plan / stored cost (elements)
+  int64_t row_off;   // offset of the row vectors (m entries)
+  int64_t col_off;   // offset of the column vectors (n entries)
+  int64_t pts_off;   // offset of the points (rows; times dim for elements)
+  int64_t tpts_off;  // offset of the target points (rows)
+  int64_t panels;    // ceil(m / 256)
+  int64_t rblocks, cblocks;  // vector blocks over rows and columns
+};
+
+struct BatchActive {
+  int count;
+  int pad_;
+  long long total_units;
+};
+
+struct BatchBuffers {
+  const BatchInstance* inst;
+  int num;                 // instances
+  int dim;                 // point dimension
+  const float* C;          // stored FP32 costs (per instance at x_off, ld)
+  const float* xs;         // source points (per instance at pts_off * dim)
+  const float* ys;         // target points
+  const double* a;         // marginals at row_off / col_off
+  const double* b;
+  float* X[2];
+  double* u[2];
+  double* v[2];
+  double* r[2];
+  double* c[2];
+  double* rowpart;         // (grid + total panels) * 256
+  double* colpart;         // total units
+  double* sqpart;          // grid + num
+  double* steppart;        // total vector blocks * kStepSums
+  double* evpart;          // (grid + num) * kEvalSums
+  double* vecpart;         // total vector blocks * kVecSums
+  DevState* st;            // per instance
+  pdot_iteration_stats* rec;  // per instance: the latest evaluation record
+  BatchActive* act;
+  int* ids;                // active instance ids
+  long long* unit_prefix;  // active prefix of units (count + 1)
+  long long* panel_prefix; // active prefix of panels
+  long long* vblock_prefix;// active prefix of vector blocks
+};
+
+__device__ __forceinline__ long long bunit_begin(long long units, int grid, long long cta) {
+  return cta * units / grid;
+}
+__device__ __forceinline__ long long bcta_of_unit(long long units, int grid, long long q) {
+  return ((q + 1) * (long long)grid - 1) / units;
+}
+// largest k in [0, count) with prefix[k] <= q
+__device__ __forceinline__ int find_segment(const long long* prefix, int count, long long q) {
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(prefix + mid) <= q)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ bool elect_last_of(unsigned int* ticket, unsigned int count) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(ticket, 1u) == count - 1);
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// Fixed-order sum of the non-empty CTA slots [lo, hi] (+ offset) of K values.
+template <int K>
+__device__ __forceinline__ void sum_cta_slots(const double* part, long long units, int grid, long long lo,
+                                              long long hi, long long slot_off, unsigned maxmask,
+                                              double (&out)[K]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const bool mx = (maxmask >> k) & 1u;
+    double acc = 0.0;
+    for (long long c = lo + lane; c <= hi; c += 32) {
+      if (bunit_begin(units, grid, c) == bunit_begin(units, grid, c + 1)) continue;  // empty CTA
+      const double v = __ldcg(part + (c + slot_off) * K + k);
+      acc = mx ? nanmax(acc, v) : acc + v;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double y = __shfl_xor_sync(0xffffffffu, acc, o);
+      acc = mx ? nanmax(acc, y) : acc + y;
+    }
+    out[k] = acc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Batched fused primal pass (FP32 plan): the per-entry step of pdot_kernels.cu.
+template <int CK>
+__global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
+  __shared__ double red[kWarps][kPanelRows];
+  __shared__ double sqw[kWarps];
+  const BatchActive act = *B.act;
+  if (act.count == 0) return;
+  const long long U = act.total_units;
+  const int G = gridDim.x;
+  const long long cta = blockIdx.x;
+  const long long q0 = bunit_begin(U, G, cta), q1 = bunit_begin(U, G, cta + 1);
+  if (q0 >= q1) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int kk = find_segment(B.unit_prefix, act.count, q0);
+  long long q = q0;
+  while (q < q1) {
+    const int k = B.ids[kk];
+    const BatchInstance I = B.inst[k];
+    const DevState* st = B.st + k;
+    const long long base_u = B.unit_prefix[kk];
+    const long long seg_end = min(q1, (long long)B.unit_prefix[kk + 1]);
+    const int buf = st->buf;
+    const double tau = st->step_size, omega = st->primal_weight, S = st->sum_weights;
+    const bool zero_g = st->g_is_zero != 0;
+    const bool first = !(S > 0.0);
+    const double s = __ddiv_rn(tau, omega);
+    const double nw = first ? 1.0 : __ddiv_rn(tau, S);
+    const double aw = first ? 1.0 : __ddiv_rn(S, __dadd_rn(S, tau));
+    float* __restrict__ X = B.X[buf] + I.x_off;
+    float* __restrict__ Xa = B.X[buf ^ 1] + I.x_off;
+    const double* __restrict__ u = B.u[buf] + I.row_off;
+    const double* __restrict__ v = B.v[buf] + I.col_off;
+    CostSource csrc;
+    csrc.C = B.C ? B.C + I.x_off : nullptr;
+    csrc.xs = B.xs ? B.xs + I.pts_off * B.dim : nullptr;
+    csrc.ys = B.ys ? B.ys + I.tpts_off * B.dim : nullptr;
+    csrc.dim = B.dim;
+    CostReader<CK, kBR, kBRPL> cost(csrc, (float)st->cost_scale);
+    double sq = 0.0;
+    const long long ql0 = q - base_u, ql1 = seg_end - base_u;  // local unit range
+    for (long long p = ql0 / I.n; p * I.n < ql1; ++p) {
+      const long long jb = (ql0 > p * I.n ? ql0 : p * I.n) - p * I.n;
+      const long long je = (ql1 < (p + 1) * I.n ? ql1 : (p + 1) * I.n) - p * I.n;
+      const long long row0 = p * kPanelRows;
+      double acc[kBRPL][kBR];
+      double ur[kBRPL][kBR];
+      bool ok[kBRPL];
+#pragma unroll
+      for (int kq = 0; kq < kBRPL; ++kq) {
+        const long long i = row0 + kq * 32 * kBR + lane * kBR;
+        ok[kq] = i < I.m;
+#pragma unroll
+        for (int e = 0; e < kBR; ++e) {
+          acc[kq][e] = 0.0;
+          ur[kq][e] = (ok[kq] && i + e < I.m && !zero_g) ? __ldg(u + i + e) : 0.0;
+        }
+      }
+      cost.panel(row0, lane, I.m, ok);
+      for (long long j = jb + warp; j < je; j += kWarps) {
+        const double vj = zero_g ? 0.0 : __ldg(v + j);
+        cost.column(j);
+        const long long col = j * I.ld + row0 + lane * kBR;
+        typename CostReader<CK, kBR, kBRPL>::value_t cv[kBRPL][kBR];
+        float xv[kBRPL][kBR], av[kBRPL][kBR];
+#pragma unroll
+        for (int kq = 0; kq < kBRPL; ++kq) {
+          if (ok[kq]) {
+            const long long idx = col + kq * 32 * kBR;
+            cost.get(idx, kq, cv[kq]);
+            vld<float, kBR>(X + idx, xv[kq]);
+            if (!first) vld<float, kBR>(Xa + idx, av[kq]);
+          }
+        }
+        double cs = 0.0;
+#pragma unroll
+        for (int kq = 0; kq < kBRPL; ++kq) {
+          if (ok[kq]) {
+            const long long i = row0 + kq * 32 * kBR + lane * kBR;
+#pragma unroll
+            for (int e = 0; e < kBR; ++e) {
+              if (i + e < I.m) {
+                double d;
+                primal_entry<float>(widen(cv[kq][e]), ur[kq][e], vj, s, nw, aw, zero_g, first, xv[kq][e],
+                                    av[kq][e], d);
+                acc[kq][e] += d;
+                cs += d;
+                sq += d * d;
+              } else {  // padded row
+                xv[kq][e] = 0.0f;
+                av[kq][e] = 0.0f;
+              }
+            }
+            const long long idx = col + kq * 32 * kBR;
+            vst<float, kBR>(X + idx, xv[kq]);
+            vst<float, kBR>(Xa + idx, av[kq]);
+          }
+        }
+        cs = warp_sum(cs);
+        if (lane == 0) B.colpart[base_u + p * I.n + j] = cs;
+      }
+#pragma unroll
+      for (int kq = 0; kq < kBRPL; ++kq)
+#pragma unroll
+        for (int e = 0; e < kBR; ++e) red[warp][kq * 32 * kBR + lane * kBR + e] = acc[kq][e];
+      __syncthreads();
+      const long long gp = B.panel_prefix[kk] + p;
+      for (int t = threadIdx.x; t < kPanelRows; t += kThreads) {
+        double s2 = red[0][t];
+#pragma unroll
+        for (int w = 1; w < kWarps; ++w) s2 += red[w][t];
+        B.rowpart[(cta + gp) * kPanelRows + t] = s2;
+      }
+      __syncthreads();
+    }
+    sq = warp_sum(sq);
+    if (lane == 0) sqw[warp] = sq;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s2 = sqw[0];
+#pragma unroll
+      for (int w = 1; w < kWarps; ++w) s2 += sqw[w];
+      B.sqpart[cta + kk] = s2;
+    }
+    __syncthreads();
+    q = seg_end;
+    ++kk;
+  }
+}
+
+// Batched dual step + per-instance step control (last CTA of each instance).
+__global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConfig cfg, int grid) {
+  const BatchActive act = *B.act;
+  if (act.count == 0) return;
+  const long long blk = blockIdx.x;
+  if (blk >= B.vblock_prefix[act.count]) return;
+  const int kk = find_segment(B.vblock_prefix, act.count, blk);
+  const int k = B.ids[kk];
+  const BatchInstance I = B.inst[k];
+  DevState* st = B.st + k;
+  const long long U = act.total_units;
+  const long long lb = blk - B.vblock_prefix[kk];  // block inside the instance
+  const int buf = st->buf;
+  const double tau = st->step_size, omega = st->primal_weight, S = st->sum_weights;
+  DualArgs A;
+  A.first = !(S > 0.0);
+  A.tw = __dmul_rn(tau, omega);
+  A.nw = A.first ? 1.0 : __ddiv_rn(tau, S);
+  A.aw = A.first ? 1.0 : __ddiv_rn(S, __dadd_rn(S, tau));
+  const long long ubase = B.unit_prefix[kk];
+  double vals[kStepSums] = {0.0, 0.0};
+  if (lb < I.rblocks) {
+    const long long i = lb * kVecThreads + threadIdx.x;
+    if (i < I.m) {
+      const long long p = i / kPanelRows, t = i - p * kPanelRows;
+      const long long gp = B.panel_prefix[kk] + p;
+      const long long lo = bcta_of_unit(U, grid, ubase + p * I.n), hi = bcta_of_unit(U, grid, ubase + (p + 1) * I.n - 1);
+      double sd = 0.0;
+      for (long long c = lo; c <= hi; ++c) {
+        if (bunit_begin(U, grid, c) == bunit_begin(U, grid, c + 1)) continue;
+        sd += B.rowpart[(c + gp) * kPanelRows + t];
+      }
+      const long long o = I.row_off + i;
+      dual_entry(sd, B.a[o], B.r[buf] + o, B.u[buf] + o, B.r[buf ^ 1] + o, B.u[buf ^ 1] + o, A, vals[0], vals[1]);
+    }
+  } else {
+    const long long j = (lb - I.rblocks) * kVecThreads + threadIdx.x;
+    if (j < I.n) {
+      double sd = 0.0;
+      for (long long p = 0; p < I.panels; ++p) sd += B.colpart[ubase + p * I.n + j];
+      const long long o = I.col_off + j;
+      dual_entry(sd, B.b[o], B.c[buf] + o, B.v[buf] + o, B.c[buf ^ 1] + o, B.v[buf ^ 1] + o, A, vals[0], vals[1]);
+    }
+  }
+  block_reduce<kStepSums>(vals, 0u, B.steppart + blk * kStepSums);
+  if (!elect_last_of(&st->ticket_step, (unsigned)(I.rblocks + I.cblocks))) return;
+  if (threadIdx.x < 32) {
+    double rs[kStepSums], cs[kStepSums], xs[1];
+    warp_reduce_partials<kStepSums>(B.steppart, B.vblock_prefix[kk], I.rblocks, 0u, rs);
+    warp_reduce_partials<kStepSums>(B.steppart, B.vblock_prefix[kk] + I.rblocks, I.cblocks, 0u, cs);
+    const long long lo = bcta_of_unit(U, grid, ubase), hi = bcta_of_unit(U, grid, B.unit_prefix[kk + 1] - 1);
+    sum_cta_slots<1>(B.sqpart, U, grid, lo, hi, kk, 0u, xs);
+    if (threadIdx.x == 0) {
+      step_control(st, cfg, rs[0], cs[0], xs[0], rs[1] + cs[1]);
+      st->ticket_step = 0;
+    }
+  }
+}
+
+// Batched evaluation, matrix part: per (CTA, instance) partials.
+template <int CK>
+__global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
+  const BatchActive act = *B.act;
+  if (act.count == 0) return;
+  const long long U = act.total_units;
+  const int G = gridDim.x;
+  const long long cta = blockIdx.x;
+  const long long q0 = bunit_begin(U, G, cta), q1 = bunit_begin(U, G, cta + 1);
+  if (q0 >= q1) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int kk = find_segment(B.unit_prefix, act.count, q0);
+  long long q = q0;
+  while (q < q1) {
+    const int k = B.ids[kk];
+    const BatchInstance I = B.inst[k];
+    DevState* st = B.st + k;
+    if (cta == bcta_of_unit(U, G, B.unit_prefix[kk]) && threadIdx.x == 0) st->eval_t0_ns = globaltimer_ns();
+    const long long base_u = B.unit_prefix[kk];
+    const long long seg_end = min(q1, (long long)B.unit_prefix[kk + 1]);
+    const int buf = st->buf;
+    const bool have_avg = st->avg_count > 0;
+    const bool zero_g = st->g_is_zero != 0;
+    const float* __restrict__ X = B.X[buf] + I.x_off;
+    const float* __restrict__ Xa = B.X[buf ^ 1] + I.x_off;
+    const double* __restrict__ u = B.u[buf] + I.row_off;
+    const double* __restrict__ v = B.v[buf] + I.col_off;
+    const double* __restrict__ ua = B.u[buf ^ 1] + I.row_off;
+    const double* __restrict__ va = B.v[buf ^ 1] + I.col_off;
+    CostSource csrc;
+    csrc.C = B.C ? B.C + I.x_off : nullptr;
+    csrc.xs = B.xs ? B.xs + I.pts_off * B.dim : nullptr;
+    csrc.ys = B.ys ? B.ys + I.tpts_off * B.dim : nullptr;
+    csrc.dim = B.dim;
+    CostReader<CK, kBR, kBRPL> cost(csrc, (float)st->cost_scale);
+    double accv[kEvalSums];
+#pragma unroll
+    for (int e = 0; e < kEvalSums; ++e) accv[e] = 0.0;
+    const long long ql0 = q - base_u, ql1 = seg_end - base_u;
+    for (long long p = ql0 / I.n; p * I.n < ql1; ++p) {
+      const long long jb = (ql0 > p * I.n ? ql0 : p * I.n) - p * I.n;
+      const long long je = (ql1 < (p + 1) * I.n ? ql1 : (p + 1) * I.n) - p * I.n;
+      const long long row0 = p * kPanelRows;
+      double ur[kBRPL][kBR], uar[kBRPL][kBR];
+      bool ok[kBRPL];
+#pragma unroll
+      for (int kq = 0; kq < kBRPL; ++kq) {
+        const long long i = row0 + kq * 32 * kBR + lane * kBR;
+        ok[kq] = i < I.m;
+#pragma unroll
+        for (int e = 0; e < kBR; ++e) {
+          const bool in = ok[kq] && i + e < I.m;
+          ur[kq][e] = in ? __ldg(u + i + e) : 0.0;
+          uar[kq][e] = (in && have_avg) ? __ldg(ua + i + e) : 0.0;
+        }
+      }
+      cost.panel(row0, lane, I.m, ok);
+      for (long long j = jb + warp; j < je; j += kWarps) {
+        const double vj = __ldg(v + j);
+        const double vaj = have_avg ? __ldg(va + j) : 0.0;
+        cost.column(j);
+        const long long col = j * I.ld + row0 + lane * kBR;
+#pragma unroll
+        for (int kq = 0; kq < kBRPL; ++kq) {
+          if (!ok[kq]) continue;
+          const long long idx = col + kq * 32 * kBR;
+          const long long i = row0 + kq * 32 * kBR + lane * kBR;
+          typename CostReader<CK, kBR, kBRPL>::value_t cv[kBR];
+          float xv[kBR], av[kBR];
+          cost.get(idx, kq, cv);
+          vldg<float, kBR>(X + idx, xv);
+          if (have_avg) vldg<float, kBR>(Xa + idx, av);
+#pragma unroll
+          for (int e = 0; e < kBR; ++e) {
+            if (i + e >= I.m) continue;
+            const double c = widen(cv[e]), x = widen(xv[e]);
+            const double gg = zero_g ? 0.0 : __dsub_rn(__dsub_rn(c, ur[kq][e]), vj);
+            const double mg = neg_part(gg);
+            accv[E_DOT] += c * x;
+            accv[E_SQX] += x * x;
+            accv[E_MAXX] = nanmax(accv[E_MAXX], fabs(x));
+            accv[E_SQG] += mg * mg;
+            accv[E_MAXG] = nanmax(accv[E_MAXG], mg);
+            if (have_avg) {
+              const double xa = widen(av[e]);
+              const double ga = __dsub_rn(__dsub_rn(c, uar[kq][e]), vaj);
+              const double mga = neg_part(ga);
+              accv[E_AVG + E_DOT] += c * xa;
+              accv[E_AVG + E_SQX] += xa * xa;
+              accv[E_AVG + E_MAXX] = nanmax(accv[E_AVG + E_MAXX], fabs(xa));
+              accv[E_AVG + E_SQG] += mga * mga;
+              accv[E_AVG + E_MAXG] = nanmax(accv[E_AVG + E_MAXG], mga);
+            }
+          }
+        }
+      }
+    }
+    block_reduce<kEvalSums>(accv, kEvalMaxMask, B.evpart + (cta + kk) * kEvalSums);
+    q = seg_end;
+    ++kk;
+  }
+}
+
+// Batched evaluation, vector part + per-instance evaluation control.
+__global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, SolveConfig cfg, int grid) {
+  const BatchActive act = *B.act;
+  if (act.count == 0) return;
+  const long long blk = blockIdx.x;
+  if (blk >= B.vblock_prefix[act.count]) return;
+  const int kk = find_segment(B.vblock_prefix, act.count, blk);
+  const int k = B.ids[kk];
+  const BatchInstance I = B.inst[k];
+  DevState* st = B.st + k;
+  const long long lb = blk - B.vblock_prefix[kk];
+  const int buf = st->buf;
+  const bool have_avg = st->avg_count > 0;
+  double acc[kVecSums];
+#pragma unroll
+  for (int e = 0; e < kVecSums; ++e) acc[e] = 0.0;
+  const bool is_row = lb < I.rblocks;
+  const long long idx = (is_row ? lb : lb - I.rblocks) * kVecThreads + threadIdx.x;
+  if (idx < (is_row ? I.m : I.n)) {
+    const long long o = (is_row ? I.row_off : I.col_off) + idx;
+    const double dist = is_row ? B.a[o] : B.b[o];
+    const double sc = (is_row ? B.r[buf] : B.c[buf])[o];
+    const double dc = (is_row ? B.u[buf] : B.v[buf])[o];
+    const double res = dist - sc;
+    acc[V_SQRES] = res * res;
+    acc[V_MAXRES] = fabs(res);
+    acc[V_DOT] = dist * dc;
+    acc[V_SQDUAL] = dc * dc;
+    acc[V_MAXDUAL] = fabs(dc);
+    if (have_avg) {
+      const double sa = (is_row ? B.r[buf ^ 1] : B.c[buf ^ 1])[o];
+      const double da = (is_row ? B.u[buf ^ 1] : B.v[buf ^ 1])[o];
+      const double ra = dist - sa;
+      acc[V_AVG + V_SQRES] = ra * ra;
+      acc[V_AVG + V_MAXRES] = fabs(ra);
+      acc[V_AVG + V_DOT] = dist * da;
+      acc[V_AVG + V_SQDUAL] = da * da;
+      acc[V_AVG + V_MAXDUAL] = fabs(da);
+    }
+  }
+  block_reduce<kVecSums>(acc, kVecMaxMask, B.vecpart + blk * kVecSums);
+  if (!elect_last_of(&st->ticket_eval, (unsigned)(I.rblocks + I.cblocks))) return;
+  if (threadIdx.x < 32) {
+    const long long U = act.total_units;
+    const long long lo = bcta_of_unit(U, grid, B.unit_prefix[kk]);
+    const long long hi = bcta_of_unit(U, grid, B.unit_prefix[kk + 1] - 1);
+    double E[kEvalSums], R[kVecSums], Cc[kVecSums];
+    sum_cta_slots<kEvalSums>(B.evpart, U, grid, lo, hi, kk, kEvalMaxMask, E);
+    warp_reduce_partials<kVecSums>(B.vecpart, B.vblock_prefix[kk], I.rblocks, kVecMaxMask, R);
+    warp_reduce_partials<kVecSums>(B.vecpart, B.vblock_prefix[kk] + I.rblocks, I.cblocks, kVecMaxMask, Cc);
+    if (threadIdx.x == 0) {
+      const PointSums cur = point_sums(E, R, Cc, 0);
+      const PointSums avg = point_sums(E, R, Cc, E_AVG);
+      eval_control(st, cfg, cur, avg, B.rec + k, 1);
+      st->ticket_eval = 0;
+    }
+  }
+}
+
+// Rebuild the active list and its prefix sums (one CTA, instances in order).
+__global__ void kb_compact(BatchBuffers B) {
+  __shared__ int flags[1024];
+  __shared__ int base;
+  if (threadIdx.x == 0) base = 0;
+  __syncthreads();
+  long long units = 0, panels = 0, vblocks = 0;
+  for (int off = 0; off < B.num; off += 1024) {
+    const int k = off + threadIdx.x;
+    flags[threadIdx.x] = (k < B.num && !B.st[k].done) ? 1 : 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int c = base;
+      for (int t = 0; t < 1024 && off + t < B.num; ++t) {
+        if (!flags[t]) continue;
+        const int kk = off + t;
+        const BatchInstance& I = B.inst[kk];
+        B.ids[c] = kk;
+        B.unit_prefix[c] = units;
+        B.panel_prefix[c] = panels;
+        B.vblock_prefix[c] = vblocks;
+        units += I.panels * I.n;
+        panels += I.panels;
+        vblocks += I.rblocks + I.cblocks;
+        ++c;
+      }
+      base = c;
+      B.unit_prefix[c] = units;
+      B.panel_prefix[c] = panels;
+      B.vblock_prefix[c] = vblocks;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    B.act->count = base;
+    B.act->total_units = units;
+  }
+}
+
+// Per-instance cost norms (stage one, over the full unit line).
+template <int CK>
+__global__ void __launch_bounds__(kThreads, 2) kb_norms(BatchBuffers B) {
+  const BatchActive act = *B.act;
+  const long long U = act.total_units;
+  const int G = gridDim.x;
+  const long long cta = blockIdx.x;
+  const long long q0 = bunit_begin(U, G, cta), q1 = bunit_begin(U, G, cta + 1);
+  if (q0 >= q1) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int kk = find_segment(B.unit_prefix, act.count, q0);
+  long long q = q0;
+  while (q < q1) {
+    const int k = B.ids[kk];
+    const BatchInstance I = B.inst[k];
+    const long long base_u = B.unit_prefix[kk];
+    const long long seg_end = min(q1, (long long)B.unit_prefix[kk + 1]);
+    CostSource csrc;
+    csrc.C = B.C ? B.C + I.x_off : nullptr;
+    csrc.xs = B.xs ? B.xs + I.pts_off * B.dim : nullptr;
+    csrc.ys = B.ys ? B.ys + I.tpts_off * B.dim : nullptr;
+    csrc.dim = B.dim;
+    CostReader<CK, kBR, kBRPL> cost(csrc, 1.0f);
+    double accv[kNormSums] = {0.0, 0.0};
+    const long long ql0 = q - base_u, ql1 = seg_end - base_u;
+    for (long long p = ql0 / I.n; p * I.n < ql1; ++p) {
+      const long long jb = (ql0 > p * I.n ? ql0 : p * I.n) - p * I.n;
+      const long long je = (ql1 < (p + 1) * I.n ? ql1 : (p + 1) * I.n) - p * I.n;
+      const long long row0 = p * kPanelRows;
+      bool ok[kBRPL];
+#pragma unroll
+      for (int kq = 0; kq < kBRPL; ++kq) ok[kq] = row0 + kq * 32 * kBR + lane * kBR < I.m;
+      cost.panel(row0, lane, I.m, ok);
+      for (long long j = jb + warp; j < je; j += kWarps) {
+        cost.column(j);
+        const long long col = j * I.ld + row0 + lane * kBR;
+#pragma unroll
+        for (int kq = 0; kq < kBRPL; ++kq) {
+          if (!ok[kq]) continue;
+          const long long i = row0 + kq * 32 * kBR + lane * kBR;
+          typename CostReader<CK, kBR, kBRPL>::value_t cv[kBR];
+          cost.get(col + kq * 32 * kBR, kq, cv);
+#pragma unroll
+          for (int e = 0; e < kBR; ++e) {
+            if (i + e >= I.m) continue;
+            const double c = widen(cv[e]);
+            accv[0] += c * c;
+            accv[1] = nanmax(accv[1], fabs(c));
+          }
+        }
+      }
+    }
+    block_reduce<kNormSums>(accv, 2u, B.evpart + (cta + kk) * kNormSums);
+    q = seg_end;
+    ++kk;
+  }
+}
+
+// Per-instance initial state (one warp per instance), cf. k0_init.
+__global__ void kb_init_state(BatchBuffers B, SolveConfig cfg, int grid) {
+  const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const BatchActive act = *B.act;
+  if (warp_global >= act.count) return;
+  const int kk = warp_global;
+  const int k = B.ids[kk];
+  const BatchInstance I = B.inst[k];
+  const long long U = act.total_units;
+  const long long lo = bcta_of_unit(U, grid, B.unit_prefix[kk]), hi = bcta_of_unit(U, grid, B.unit_prefix[kk + 1] - 1);
+  double nc[kNormSums];
+  sum_cta_slots<kNormSums>(B.evpart, U, grid, lo, hi, kk, 2u, nc);
+  double sqab = 0.0, mxab = 0.0;
+  for (long long i = lane; i < I.m + I.n; i += 32) {
+    const double x = i < I.m ? B.a[I.row_off + i] : B.b[I.col_off + i - I.m];
+    sqab += x * x;
+    mxab = nanmax(mxab, fabs(x));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sqab += __shfl_xor_sync(0xffffffffu, sqab, o);
+    mxab = nanmax(mxab, __shfl_xor_sync(0xffffffffu, mxab, o));
+  }
+  if (lane != 0) return;
+  DevState* st = B.st + k;
+  double scale = 1.0;
+  if (B.xs) {
+    scale = cfg.cost_scale > 0.0 ? cfg.cost_scale : (nc[1] > 0.0 ? 1.0 / nc[1] : 1.0);
+    nc[0] *= scale * scale;
+    nc[1] *= scale;
+  }
+  memset(st, 0, sizeof(*st));
+  st->cost_scale = scale;
+  st->linf_obj = nc[1];
+  st->l2_obj = sqrt(nc[0]);
+  st->linf_rhs = mxab;
+  st->l2_rhs = sqrt(sqab);
+  st->step_size = cfg.adaptive ? 1.0 : (1.0 - 0.2) / sqrt((double)(I.m + I.n));
+  if (cfg.scale_invariant_initial_primal_weight) {
+    const double rhs = st->l2_rhs, obj = st->l2_obj;
+    st->primal_weight = (obj > 0.0 && rhs > 0.0) ? cfg.primal_importance * (obj / rhs) : cfg.primal_importance;
+  } else {
+    st->primal_weight = cfg.primal_importance;
+  }
+  st->iteration = 1;
+  st->last_rp = st->l2_rhs;
+  st->ratio_last_trial = 1.0;
+  st->last_restart_length = 1;
+  st->g_is_zero = 1;
+  st->out_current = 1;
+  if (!(isfinite(st->l2_obj) && isfinite(st->l2_rhs) && isfinite(st->linf_obj))) {
+    st->done = 1;
+    st->termination_reason = PDOT_TERMINATION_REASON_INVALID_PROBLEM;
+  }
+  st->t_start_ns = globaltimer_ns();
+}
+
+// Widen a padded FP32 plan of one instance into a dense FP64 column-major one.
+__global__ void kb_widen(const float* __restrict__ X, int64_t m, int64_t n, int64_t ld, double* __restrict__ out) {
+  const int64_t N = m * n;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < N; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = e / m, i = e - j * m;
+    out[e] = (double)X[i + j * ld];
+  }
+}
+
+__global__ void kb_convert_cost(const double* __restrict__ src, int64_t m, int64_t n, int64_t ld,
+                                float* __restrict__ dst) {
+  const int64_t N = ld * n;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < N; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = e / ld, i = e - j * ld;
+    dst[e] = i < m ? __double2float_rn(src[i + j * m]) : 0.0f;
+  }
+}
+
+#define PDOT_BATCH_VARIANT(kind, KERNEL, LAUNCH)                                      \
+  do {                                                                                \
+    switch (kind) {                                                                   \
+      case PDOT_COST_F32: { auto kfn = KERNEL<PDOT_COST_F32>; LAUNCH; } break;        \
+      case pdot::kCostSqBase + 1: { auto kfn = KERNEL<pdot::kCostSqBase + 1>; LAUNCH; } break;    \
+      case pdot::kCostSqBase + 2: { auto kfn = KERNEL<pdot::kCostSqBase + 2>; LAUNCH; } break;    \
+      case pdot::kCostSqBase + 3: { auto kfn = KERNEL<pdot::kCostSqBase + 3>; LAUNCH; } break;    \
+      case pdot::kCostL1Base + 1: { auto kfn = KERNEL<pdot::kCostL1Base + 1>; LAUNCH; } break;    \
+      case pdot::kCostL1Base + 2: { auto kfn = KERNEL<pdot::kCostL1Base + 2>; LAUNCH; } break;    \
+      default: { auto kfn = KERNEL<pdot::kCostL1Base + 3>; LAUNCH; } break;                 \
+    }                                                                                 \
+  } while (0)
+
+}  // namespace
+}  // namespace pdot
+
+// ============================================================================
+// Host side
+namespace {
+
+struct BatchFailure {
+  int code;
+  std::string msg;
+};
+
+[[noreturn]] void bfail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  throw BatchFailure{code, buf};
+}
+
+void bck(cudaError_t e, const char* what, int line) {
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    bfail(e == cudaErrorMemoryAllocation ? PDOT_ERR_OUT_OF_MEMORY : PDOT_ERR_CUDA, "%s failed: %s (pdot_batch.cu:%d)",
+          what, cudaGetErrorString(e), line);
+  }
+}
+#define BCK(x) bck((x), #x, __LINE__)
+
+class BatchSolver {
+ public:
+  BatchSolver(const pdot_batch_problem& P, const pdot_pdhg_parameters& prm, const pdot_solver_options* opt) {
+    device_ = opt ? opt->device : 0;
+    const int pub_kind = opt ? opt->cost_storage : PDOT_COST_F32;
+    dim_ = (pub_kind == PDOT_COST_SQEUCLID_POINTS || pub_kind == PDOT_COST_L1_POINTS) ? opt->point_dim : 0;
+    kind_ = pdot::internal_cost_kind(pub_kind, dim_);
+    use_graph_ = opt ? opt->use_cuda_graph != 0 : true;
+    const int B = (int)P.num_instances;
+    num_ = B;
+    BCK(cudaSetDevice(device_));
+    BCK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    // instance layout
+    inst_.resize(B);
+    int64_t xo = 0, ro = 0, co = 0, po = 0, to = 0, units = 0, panels = 0, vblocks = 0;
+    for (int k = 0; k < B; ++k) {
+      pdot::BatchInstance& I = inst_[k];
+      I.m = P.num_rows[k];
+      I.n = P.num_cols[k];
+      I.ld = (I.m + 3) / 4 * 4;
+      I.x_off = xo;
+      I.row_off = ro;
+      I.col_off = co;
+      I.pts_off = po;
+      I.tpts_off = to;
+      I.panels = (I.m + pdot::kPanelRows - 1) / pdot::kPanelRows;
+      I.rblocks = (I.m + pdot::kVecThreads - 1) / pdot::kVecThreads;
+      I.cblocks = (I.n + pdot::kVecThreads - 1) / pdot::kVecThreads;
+      xo += I.ld * I.n;
+      ro += I.m;
+      co += I.n;
+      po += I.m;
+      to += I.n;
+      units += I.panels * I.n;
+      panels += I.panels;
+      vblocks += I.rblocks + I.cblocks;
+    }
+    total_x_ = xo;
+    total_units_ = units;
+    total_panels_ = panels;
+    total_vblocks_ = vblocks;
+    int sms = 148;
+    BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+    int occ = 1;
+    PDOT_BATCH_VARIANT(kind_, pdot::kb_primal,
+                       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, pdot::kThreads, 0) != cudaSuccess ||
+                           occ < 1) occ = 1);
+    cudaGetLastError();
+    grid_ = (int)std::min<int64_t>((int64_t)sms * occ, std::max<int64_t>(units, 1));
+    if (opt && opt->ctas_per_sm > 0)
+      grid_ = (int)std::min<int64_t>((int64_t)std::min(opt->ctas_per_sm, occ) * sms, std::max<int64_t>(units, 1));
+
+    // device buffers
+    D_.inst = upload(inst_.data(), B);
+    D_.num = B;
+    D_.dim = dim_;
+    if (dim_ == 0) {
+      float* C = alloc<float>(total_x_);
+      double* tmp = nullptr;
+      size_t tmp_cap = 0;
+      for (int k = 0; k < B; ++k) {
+        const size_t mn = (size_t)inst_[k].m * inst_[k].n;
+        if (mn > tmp_cap) {
+          if (tmp) BCK(cudaFree(tmp));
+          BCK(cudaMalloc(&tmp, mn * sizeof(double)));
+          tmp_cap = mn;
+        }
+        BCK(cudaMemcpyAsync(tmp, P.cost_matrices[k], mn * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        pdot::kb_convert_cost<<<256, 256, 0, stream_>>>(tmp, inst_[k].m, inst_[k].n, inst_[k].ld, C + inst_[k].x_off);
+        BCK(cudaGetLastError());
+        BCK(cudaStreamSynchronize(stream_));
+      }
+      if (tmp) BCK(cudaFree(tmp));
+      D_.C = C;
+      D_.xs = D_.ys = nullptr;
+    } else {
+      float* xs = alloc<float>((size_t)po * dim_);
+      float* ys = alloc<float>((size_t)to * dim_);
+      for (int k = 0; k < B; ++k) {
+        BCK(cudaMemcpyAsync(xs + inst_[k].pts_off * dim_, P.source_points[k], (size_t)inst_[k].m * dim_ * sizeof(float),
+                            cudaMemcpyHostToDevice, stream_));
+        BCK(cudaMemcpyAsync(ys + inst_[k].tpts_off * dim_, P.target_points[k], (size_t)inst_[k].n * dim_ * sizeof(float),
+                            cudaMemcpyHostToDevice, stream_));
+      }
+      D_.C = nullptr;
+      D_.xs = xs;
+      D_.ys = ys;
+    }
+    double* a = alloc<double>(ro);
+    double* b = alloc<double>(co);
+    for (int k = 0; k < B; ++k) {
+      BCK(cudaMemcpyAsync(a + inst_[k].row_off, P.source_distributions[k], inst_[k].m * sizeof(double),
+                          cudaMemcpyHostToDevice, stream_));
+      BCK(cudaMemcpyAsync(b + inst_[k].col_off, P.target_distributions[k], inst_[k].n * sizeof(double),
+                          cudaMemcpyHostToDevice, stream_));
+    }
+    D_.a = a;
+    D_.b = b;
+    for (int h = 0; h < 2; ++h) {
+      D_.X[h] = alloc<float>(total_x_);
+      D_.u[h] = alloc<double>(ro);
+      D_.r[h] = alloc<double>(ro);
+      D_.v[h] = alloc<double>(co);
+      D_.c[h] = alloc<double>(co);
+    }
+    rows_ = ro;
+    cols_ = co;
+    D_.rowpart = alloc<double>(((size_t)grid_ + total_panels_) * pdot::kPanelRows);
+    D_.colpart = alloc<double>(total_units_);
+    D_.sqpart = alloc<double>((size_t)grid_ + B);
+    D_.steppart = alloc<double>((size_t)total_vblocks_ * pdot::kStepSums);
+    D_.evpart = alloc<double>(((size_t)grid_ + B) * pdot::kEvalSums);
+    D_.vecpart = alloc<double>((size_t)total_vblocks_ * pdot::kVecSums);
+    D_.st = alloc<pdot::DevState>(B);
+    D_.rec = alloc<pdot_iteration_stats>(B);
+    D_.act = alloc<pdot::BatchActive>(1);
+    D_.ids = alloc<int>(B);
+    D_.unit_prefix = alloc<long long>(B + 1);
+    D_.panel_prefix = alloc<long long>(B + 1);
+    D_.vblock_prefix = alloc<long long>(B + 1);
+    cfg_ = pdot::SolveConfig{};
+    fill_config(prm);
+    freq_ = prm.termination_evaluation_frequency;
+    limit_ = prm.termination_criteria.iteration_limit;
+    void* hp = nullptr;
+    BCK(cudaMallocHost(&hp, sizeof(pdot::BatchActive) * 2));
+    host_act_ = static_cast<pdot::BatchActive*>(hp);
+    for (int k = 0; k < 2; ++k) BCK(cudaEventCreateWithFlags(&ev_[k], cudaEventDisableTiming));
+    if (use_graph_) capture();
+  }
+
+  ~BatchSolver() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    if (graph_) cudaGraphExecDestroy(graph_);
+    for (int k = 0; k < 2; ++k)
+      if (ev_[k]) cudaEventDestroy(ev_[k]);
+    if (host_act_) cudaFreeHost(host_act_);
+    for (void* p : allocs_) cudaFree(p);
+    if (stream_) cudaStreamDestroy(stream_);
+  }
+
+  void run(pdot_batch_output* outs, double* seconds) {
+    cudaEvent_t t0, t1;
+    BCK(cudaEventCreate(&t0));
+    BCK(cudaEventCreate(&t1));
+    BCK(cudaEventRecord(t0, stream_));
+    init();
+    long long it = 1;
+    int issued = 0, completed = 0;
+    for (;;) {
+      while (issued - completed < 2) {
+        enqueue_chunk(it);
+        BCK(cudaMemcpyAsync(&host_act_[issued % 2], D_.act, sizeof(pdot::BatchActive), cudaMemcpyDeviceToHost, stream_));
+        BCK(cudaEventRecord(ev_[issued % 2], stream_));
+        ++issued;
+      }
+      BCK(cudaEventSynchronize(ev_[completed % 2]));
+      const pdot::BatchActive a = host_act_[completed % 2];
+      ++completed;
+      if (a.count == 0) break;
+      if (it > (long long)limit_ + 2 * freq_ + 16)
+        bfail(PDOT_ERR_CUDA, "batched solve did not finish by the iteration limit");
+    }
+    BCK(cudaEventRecord(t1, stream_));
+    BCK(cudaStreamSynchronize(stream_));
+    float ms = 0.0f;
+    BCK(cudaEventElapsedTime(&ms, t0, t1));
+    if (seconds) *seconds = ms / 1000.0;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    collect(outs);
+  }
+
+ private:
+  template <typename T>
+  T* alloc(size_t count) {
+    void* p = nullptr;
+    BCK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    allocs_.push_back(p);
+    return static_cast<T*>(p);
+  }
+  template <typename T>
+  const T* upload(const T* src, size_t count) {
+    T* d = alloc<T>(count);
+    BCK(cudaMemcpy(d, src, count * sizeof(T), cudaMemcpyHostToDevice));
+    return d;
+  }
+
+  void fill_config(const pdot_pdhg_parameters& p) {
+    pdot::SolveConfig& c = cfg_;
+    c.adaptive = p.step_size_policy == PDOT_STEP_SIZE_ADAPTIVE;
+    c.reduction_exponent = p.reduction_exponent;
+    c.growth_exponent = p.growth_exponent;
+    c.restart_scheme = p.restart_params.restart_scheme;
+    c.restart_to_current_metric = p.restart_params.restart_to_current_metric;
+    c.restart_frequency_if_fixed = p.restart_params.restart_frequency_if_fixed;
+    c.artificial_restart_threshold = p.restart_params.artificial_restart_threshold;
+    c.sufficient_reduction_for_restart = p.restart_params.sufficient_reduction_for_restart;
+    c.necessary_reduction_for_restart = p.restart_params.necessary_reduction_for_restart;
+    c.primal_weight_update_smoothing = p.restart_params.primal_weight_update_smoothing;
+    c.optimality_norm = p.termination_criteria.optimality_norm;
+    c.eps_abs = p.termination_criteria.eps_optimal_absolute;
+    c.eps_rel = p.termination_criteria.eps_optimal_relative;
+    c.time_sec_limit = p.termination_criteria.time_sec_limit;
+    c.iteration_limit = p.termination_criteria.iteration_limit;
+    c.kkt_matrix_pass_limit = p.termination_criteria.kkt_matrix_pass_limit;
+    c.record_iteration_stats = 0;
+    c.scale_invariant_initial_primal_weight = p.scale_invariant_initial_primal_weight != 0;
+    c.primal_importance = p.primal_importance;
+    c.cost_scale = 0.0;
+    c.warm_start = 0;
+  }
+
+  // zero starts, cost norms, initial states, the first active list
+  void init() {
+    BCK(cudaMemsetAsync(D_.X[0], 0, total_x_ * sizeof(float), stream_));
+    BCK(cudaMemsetAsync(D_.X[1], 0, total_x_ * sizeof(float), stream_));
+    BCK(cudaMemsetAsync(D_.u[0], 0, rows_ * sizeof(double), stream_));
+    BCK(cudaMemsetAsync(D_.r[0], 0, rows_ * sizeof(double), stream_));
+    BCK(cudaMemsetAsync(D_.v[0], 0, cols_ * sizeof(double), stream_));
+    BCK(cudaMemsetAsync(D_.c[0], 0, cols_ * sizeof(double), stream_));
+    BCK(cudaMemsetAsync(D_.st, 0, num_ * sizeof(pdot::DevState), stream_));
+    pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_);
+    BCK(cudaGetLastError());
+    PDOT_BATCH_VARIANT(kind_, pdot::kb_norms, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
+    BCK(cudaGetLastError());
+    pdot::kb_init_state<<<(num_ * 32 + 255) / 256, 256, 0, stream_>>>(D_, cfg_, grid_);
+    BCK(cudaGetLastError());
+    pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_);  // drops invalid problems
+    BCK(cudaGetLastError());
+  }
+
+  bool is_eval(long long it) const { return (it - 1) % freq_ == 0 || it == limit_ + 1 || it <= 10; }
+
+  void launch_eval() {
+    PDOT_BATCH_VARIANT(kind_, pdot::kb_eval, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
+    pdot::kb_eval_vec<<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_);
+    pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_);
+    BCK(cudaGetLastError());
+  }
+  void launch_step() {
+    PDOT_BATCH_VARIANT(kind_, pdot::kb_primal, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
+    pdot::kb_dual<<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_);
+    BCK(cudaGetLastError());
+  }
+
+  bool regular_start(long long it) const {
+    if (!graph_ || it <= 10 || (it - 1) % freq_ != 0) return false;
+    for (long long k = it + 1; k < it + freq_; ++k)
+      if (is_eval(k)) return false;
+    return true;
+  }
+
+  void enqueue_chunk(long long& it) {
+    if (regular_start(it)) {
+      BCK(cudaGraphLaunch(graph_, stream_));
+      it += freq_;
+      return;
+    }
+    long long k = 0;
+    do {
+      if (is_eval(it)) launch_eval();
+      launch_step();
+      ++it;
+      ++k;
+    } while (k < freq_ && !regular_start(it));
+  }
+
+  void capture() {
+    cudaGraph_t g = nullptr;
+    BCK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    launch_eval();
+    for (long long k = 0; k < freq_; ++k) launch_step();
+    BCK(cudaStreamEndCapture(stream_, &g));
+    const cudaError_t e = cudaGraphInstantiate(&graph_, g, 0);
+    cudaGraphDestroy(g);
+    BCK(e);
+  }
+
+  void collect(pdot_batch_output* outs) {
+    std::vector<pdot::DevState> st(num_);
+    std::vector<pdot_iteration_stats> rec(num_);
+    BCK(cudaMemcpy(st.data(), D_.st, num_ * sizeof(pdot::DevState), cudaMemcpyDeviceToHost));
+    BCK(cudaMemcpy(rec.data(), D_.rec, num_ * sizeof(pdot_iteration_stats), cudaMemcpyDeviceToHost));
+    double* tmp = nullptr;
+    size_t cap = 0;
+    for (int k = 0; k < num_; ++k) {
+      const pdot::BatchInstance& I = inst_[k];
+      pdot_batch_output& o = outs[k];
+      o.termination_reason = st[k].termination_reason;
+      o.iteration_count = (int32_t)(st[k].iteration - 1);
+      o.final_stats = rec[k];
+      const int xb = st[k].out_current ? st[k].buf : (st[k].buf ^ 1);
+      const size_t mn = (size_t)I.m * I.n;
+      if (o.primal_solution) {
+        if (mn > cap) {
+          if (tmp) BCK(cudaFree(tmp));
+          BCK(cudaMalloc(&tmp, mn * sizeof(double)));
+          cap = mn;
+        }
+        pdot::kb_widen<<<256, 256, 0, stream_>>>(D_.X[xb] + I.x_off, I.m, I.n, I.ld, tmp);
+        BCK(cudaGetLastError());
+        BCK(cudaMemcpyAsync(o.primal_solution, tmp, mn * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        BCK(cudaStreamSynchronize(stream_));
+      }
+      if (o.dual_source_solution)
+        BCK(cudaMemcpy(o.dual_source_solution, D_.u[xb] + I.row_off, I.m * sizeof(double), cudaMemcpyDeviceToHost));
+      if (o.dual_target_solution)
+        BCK(cudaMemcpy(o.dual_target_solution, D_.v[xb] + I.col_off, I.n * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    if (tmp) BCK(cudaFree(tmp));
+  }
+
+  int device_ = 0, num_ = 0, dim_ = 0, kind_ = 0, grid_ = 1;
+  bool use_graph_ = true;
+  int64_t total_x_ = 0, total_units_ = 0, total_panels_ = 0, total_vblocks_ = 0, rows_ = 0, cols_ = 0;
+  long long freq_ = 128, limit_ = 0;
+  std::vector<pdot::BatchInstance> inst_;
+  std::vector<void*> allocs_;
+  pdot::BatchBuffers D_{};
+  pdot::SolveConfig cfg_{};
+  cudaStream_t stream_ = nullptr;
+  cudaGraphExec_t graph_ = nullptr;
+  cudaEvent_t ev_[2] = {};
+  pdot::BatchActive* host_act_ = nullptr;
+};
+
+}  // namespace
+
+extern "C" int pdot_optimize_batched(const pdot_batch_problem* problem, const pdot_pdhg_parameters* params,
+                                     const pdot_solver_options* options, pdot_batch_output* outputs,
+                                     double* solve_seconds) {
+  pdot::set_last_error("");
+  try {
+    if (!problem || !params || !outputs) bfail(PDOT_ERR_INVALID_ARGUMENT, "null argument");
+    if (problem->num_instances < 1 || problem->num_instances > pdot::kMaxBatch)
+      bfail(PDOT_ERR_INVALID_ARGUMENT, "num_instances must be 1..%d", pdot::kMaxBatch);
+    if (!problem->num_rows || !problem->num_cols || !problem->source_distributions || !problem->target_distributions)
+      bfail(PDOT_ERR_INVALID_ARGUMENT, "null instance arrays");
+    const int kind = options ? options->cost_storage : PDOT_COST_F32;
+    const bool points = kind == PDOT_COST_SQEUCLID_POINTS || kind == PDOT_COST_L1_POINTS;
+    if (!(kind == PDOT_COST_F32 || points))
+      bfail(PDOT_ERR_INVALID_ARGUMENT, "the batched solver takes an FP32-stored or a coordinate cost");
+    if (options && options->plan_precision != PDOT_PRECISION_F32)
+      bfail(PDOT_ERR_INVALID_ARGUMENT, "the batched solver keeps FP32 plans (plan_precision must be F32)");
+    if (points && (options->point_dim < 1 || options->point_dim > 3))
+      bfail(PDOT_ERR_INVALID_ARGUMENT, "point_dim must be 1..3 for the batched solver");
+    if (points && (!problem->source_points || !problem->target_points))
+      bfail(PDOT_ERR_INVALID_ARGUMENT, "null point arrays");
+    if (!points && !problem->cost_matrices) bfail(PDOT_ERR_INVALID_ARGUMENT, "null cost matrices");
+    if (params->termination_evaluation_frequency < 1 || !(params->primal_importance > 0))
+      bfail(PDOT_ERR_INVALID_ARGUMENT, "invalid parameters");
+    for (int64_t k = 0; k < problem->num_instances; ++k)
+      if (problem->num_rows[k] < 1 || problem->num_cols[k] < 1) bfail(PDOT_ERR_INVALID_ARGUMENT, "empty instance %lld", (long long)k);
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count < 1) {
+      cudaGetLastError();
+      bfail(PDOT_ERR_NO_DEVICE, "no CUDA device is visible");
+    }
+    BatchSolver solver(*problem, *params, options);
+    solver.run(outputs, solve_seconds);
+    return PDOT_OK;
+  } catch (const BatchFailure& f) {
+    pdot::set_last_error(f.msg.c_str());
+    return f.code;
+  } catch (...) {
+    pdot::set_last_error("unexpected C++ exception");
+    return PDOT_ERR_CUDA;
+  }
+}

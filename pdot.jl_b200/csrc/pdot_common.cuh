@@ -46,7 +46,7 @@ struct Geometry {
   int32_t row_blocks;  // CTAs of the vector passes covering m
   int32_t col_blocks;  // CTAs of the vector passes covering n
   int32_t plan_f32;    // 1: FP32 plan and average, 0: FP64
-  int32_t cost_kind;   // PDOT_COST_F64 / _F32 / _BF16, or kCostSqBase + point dim
+  int32_t cost_kind;   // PDOT_COST_F64 / _F32 / _BF16, or a coordinate kind (internal_cost_kind)
   int32_t tma;         // 1: the fused pass stages its operands with bulk copies
   int32_t tma_smem;    // dynamic shared memory of the staged pass (bytes)
 };
@@ -59,10 +59,22 @@ struct CostSource {
   int dim;             // 1..kMaxPointDim
 };
 constexpr int kMaxPointDim = 4;
-// Internal cost kinds: the PDOT_COST_* values, and kCostSqBase + dim for the
-// coordinate cost (the point dimension is a compile-time constant of the kernels).
+// Internal cost kinds: the stored PDOT_COST_* values, kCostSqBase + dim for the
+// squared-Euclidean coordinate cost and kCostL1Base + dim for the L1 one (the
+// point dimension is a compile-time constant of the kernels).
 constexpr int kCostSqBase = 10;
-__host__ __device__ constexpr bool is_sq_cost(int kind) { return kind > kCostSqBase; }
+constexpr int kCostL1Base = 20;
+__host__ __device__ constexpr bool is_sq_cost(int kind) {
+  return kind > kCostSqBase && kind <= kCostSqBase + kMaxPointDim;
+}
+__host__ __device__ constexpr bool is_l1_cost(int kind) {
+  return kind > kCostL1Base && kind <= kCostL1Base + kMaxPointDim;
+}
+__host__ __device__ constexpr bool is_point_cost(int kind) { return is_sq_cost(kind) || is_l1_cost(kind); }
+// The internal kind of a public PDOT_COST_* with points of dimension `dim`.
+__host__ __device__ constexpr int internal_cost_kind(int pub, int dim) {
+  return pub == PDOT_COST_SQEUCLID_POINTS ? kCostSqBase + dim : (pub == PDOT_COST_L1_POINTS ? kCostL1Base + dim : pub);
+}
 
 __host__ __device__ __forceinline__ int64_t unit_begin(const Geometry& g, int64_t cta) {
   return cta * g.units / g.grid;

@@ -141,12 +141,12 @@ Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
     fail(PDOT_ERR_INVALID_ARGUMENT, "unknown plan_precision %d", o->plan_precision);
   v.plan_f32 = o->plan_precision == PDOT_PRECISION_F32;
   v.cost_kind = o->cost_storage;
-  if (v.cost_kind < PDOT_COST_F64 || v.cost_kind > PDOT_COST_SQEUCLID_POINTS)
+  if (v.cost_kind < PDOT_COST_F64 || v.cost_kind > PDOT_COST_L1_POINTS)
     fail(PDOT_ERR_INVALID_ARGUMENT, "unknown cost_storage %d", v.cost_kind);
   if (v.plan_f32 == (v.cost_kind == PDOT_COST_F64))
     fail(PDOT_ERR_INVALID_ARGUMENT,
          "the FP64 plan runs with the FP64 cost; an FP32 plan runs with FP32, BF16 or coordinate costs");
-  if (v.cost_kind == PDOT_COST_SQEUCLID_POINTS) {
+  if (v.cost_kind == PDOT_COST_SQEUCLID_POINTS || v.cost_kind == PDOT_COST_L1_POINTS) {
     if (o->point_dim < 1 || o->point_dim > pdot::kMaxPointDim)
       fail(PDOT_ERR_INVALID_ARGUMENT, "point_dim must be 1..%d", pdot::kMaxPointDim);
     if (!o->source_points || !o->target_points) fail(PDOT_ERR_INVALID_ARGUMENT, "null point coordinates");
@@ -164,7 +164,7 @@ Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
   if (o->primal_pass != PDOT_PASS_AUTO && o->primal_pass != PDOT_PASS_STAGED && o->primal_pass != PDOT_PASS_DIRECT)
     fail(PDOT_ERR_INVALID_ARGUMENT, "unknown primal_pass %d", o->primal_pass);
   v.staged = o->primal_pass == PDOT_PASS_STAGED ? 1 : (o->primal_pass == PDOT_PASS_DIRECT ? 0 : 2);
-  for (int k = 0; k < 7; ++k)
+  for (int k = 0; k < 6; ++k)
     if (o->reserved[k] != 0) fail(PDOT_ERR_INVALID_ARGUMENT, "reserved option fields must be zero");
   return v;
 }
@@ -230,7 +230,7 @@ class Solver {
     // the cost: as given (FP64), converted to FP32 / BF16 on the device, or
     // coordinates for the on-the-fly squared-Euclidean cost
     bool cost_aligned = true;
-    if (var.cost_kind == PDOT_COST_SQEUCLID_POINTS) {
+    if (var.cost_kind == PDOT_COST_SQEUCLID_POINTS || var.cost_kind == PDOT_COST_L1_POINTS) {
       const size_t d = (size_t)var.point_dim;
       if (device_inputs) {
         cost_.xs = var.xs;
@@ -273,7 +273,7 @@ class Solver {
       if (tmp) CK(cudaFree(tmp));
       cost_.C = Cs;
     }
-    const int kind = var.cost_kind == PDOT_COST_SQEUCLID_POINTS ? pdot::kCostSqBase + var.point_dim : var.cost_kind;
+    const int kind = pdot::internal_cost_kind(var.cost_kind, var.point_dim);
     g_ = pdot::make_geometry(m, n, cost_aligned ? 1 : 0, device_, var.plan_f32, kind, var.staged);
     if (device_inputs) {
       a_ = P.source_distribution;

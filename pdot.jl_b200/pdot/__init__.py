@@ -32,6 +32,7 @@ from .api import (  # noqa: F401
     construct_restart_parameters,
     construct_termination_criteria,
     optimize,
+    optimize_batched,
     termination_reason_to_string,
 )
 from .solve import default_parameters, rounding, solve_instance_and_output, warm_up, write_vector_to_file  # noqa: F401

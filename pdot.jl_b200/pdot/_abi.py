@@ -76,6 +76,7 @@ COST_F64 = 0
 COST_F32 = 1
 COST_BF16 = 2
 COST_SQEUCLID_POINTS = 3
+COST_L1_POINTS = 4
 PASS_AUTO = 0
 PASS_STAGED = 1
 PASS_DIRECT = 2
@@ -95,7 +96,8 @@ class SolverOptionsC(ct.Structure):
         ("warm_dual_source", ct.POINTER(ct.c_double)),
         ("warm_dual_target", ct.POINTER(ct.c_double)),
         ("primal_pass", ct.c_int32),
-        ("reserved", ct.c_int32 * 7),
+        ("ctas_per_sm", ct.c_int32),
+        ("reserved", ct.c_int32 * 6),
     ]
 
 
@@ -115,6 +117,19 @@ class SolverStatusC(ct.Structure):
         ("primal_pass_ms", ct.c_double),
         ("dual_step_ms", ct.c_double),
         ("evaluation_ms", ct.c_double),
+    ]
+
+
+class BatchProblemC(ct.Structure):
+    _fields_ = [
+        ("num_instances", ct.c_int64),
+        ("num_rows", ct.POINTER(ct.c_int64)),
+        ("num_cols", ct.POINTER(ct.c_int64)),
+        ("cost_matrices", ct.POINTER(ct.c_void_p)),
+        ("source_distributions", ct.POINTER(ct.c_void_p)),
+        ("target_distributions", ct.POINTER(ct.c_void_p)),
+        ("source_points", ct.POINTER(ct.c_void_p)),
+        ("target_points", ct.POINTER(ct.c_void_p)),
     ]
 
 
@@ -181,6 +196,17 @@ class SaddlePointOutputC(ct.Structure):
     ]
 
 
+class BatchOutputC(ct.Structure):
+    _fields_ = [
+        ("primal_solution", ct.POINTER(ct.c_double)),
+        ("dual_source_solution", ct.POINTER(ct.c_double)),
+        ("dual_target_solution", ct.POINTER(ct.c_double)),
+        ("termination_reason", ct.c_int32),
+        ("iteration_count", ct.c_int32),
+        ("final_stats", IterationStatsC),
+    ]
+
+
 # Every symbol include/pdot.h declares, with its ctypes signature.
 _P = ct.c_void_p
 _D = ct.c_double
@@ -208,6 +234,11 @@ SIGNATURES = {
     "pdot_solver_finish": (ct.c_int, [_P, ct.POINTER(SaddlePointOutputC)]),
     "pdot_solver_stream": (_P, [_P]),
     "pdot_solver_destroy": (None, [_P]),
+    "pdot_optimize_batched": (
+        ct.c_int,
+        [ct.POINTER(BatchProblemC), ct.POINTER(PdhgParametersC), ct.POINTER(SolverOptionsC),
+         ct.POINTER(BatchOutputC), ct.POINTER(ct.c_double)],
+    ),
     "pdot_rounding_f64": (ct.c_int, [_I64, _I64, _P, _P, _P, _P]),
     "pdot_rounding_host": (ct.c_int, [_I64, _I64, _P, _P, _P, _I32]),
     "pdot_sqeuclid_cost_f64": (ct.c_int, [_I64, _I64, _I32, _P, _P, _I32, _P, _P]),

@@ -365,7 +365,7 @@ def validate(params: PdhgParameters) -> None:
 # ---------------------------------------------------------------- optimize
 _PRECISIONS = {"f64": _abi.PRECISION_F64, "f32": _abi.PRECISION_F32}
 _COSTS = {"f64": _abi.COST_F64, "f32": _abi.COST_F32, "bf16": _abi.COST_BF16,
-          "sqeuclid": _abi.COST_SQEUCLID_POINTS}
+          "sqeuclid": _abi.COST_SQEUCLID_POINTS, "l1": _abi.COST_L1_POINTS}
 
 
 def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, precision: str = "f64",
@@ -374,7 +374,7 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
     """Build pdot_solver_options. Returns (options, objects to keep alive).
 
     precision  "f64" (the drop-in) or "f32" (mixed precision: FP32 plan)
-    cost       "f64", "f32", "bf16" or "sqeuclid" (from `points`); defaults to
+    cost       "f64", "f32", "bf16", "sqeuclid" or "l1" (from `points`); defaults to
                "f64" for an FP64 plan and "f32" for an FP32 plan
     points     (xs, ys) coordinate arrays (m x d, n x d) for "sqeuclid"; with
                device_pointers, (xs_ptr, ys_ptr, d)
@@ -389,10 +389,10 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
     if cost is None:
         cost = "f64" if precision == "f64" else "f32"
     opts.cost_storage = _COSTS[cost]
+    if points is None and cost in ("sqeuclid", "l1"):
+        return opts, keep  # coordinates supplied per instance by the batched entry
     opts.primal_pass = {"auto": _abi.PASS_AUTO, "staged": _abi.PASS_STAGED, "direct": _abi.PASS_DIRECT}[primal_pass]
-    if cost == "sqeuclid":
-        if points is None:
-            raise ValueError("the sqeuclid cost needs point coordinates")
+    if cost in ("sqeuclid", "l1"):
         if device_pointers:
             xs_ptr, ys_ptr, dim = points
             opts.source_points = ct.cast(ct.c_void_p(xs_ptr), ct.POINTER(ct.c_float))
@@ -509,3 +509,83 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+
+def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", points=None, device: int = 0,
+                     use_cuda_graph: bool = True, ctas_per_sm: int = 0):
+    """Solve many independent instances at once (pdot_optimize_batched).
+
+    problems  a list of OptimalTransportProblem (cost_matrix may be None for
+              coordinate costs)
+    cost      "f32" (each FP64 matrix stored in FP32), "sqeuclid" or "l1"
+              (from `points`, a list of (xs, ys) per instance)
+    Returns (outputs, seconds): a SaddlePointOutput per instance (its
+    iteration_stats holds the final evaluation record) and the device time.
+    """
+    validate(params)
+    lib = _abi.load()
+    B = len(problems)
+    keep = []
+    rows = (ct.c_int64 * B)()
+    cols = (ct.c_int64 * B)()
+    costs = (ct.c_void_p * B)()
+    srcs = (ct.c_void_p * B)()
+    tgts = (ct.c_void_p * B)()
+    xs_p = (ct.c_void_p * B)()
+    ys_p = (ct.c_void_p * B)()
+    outs = (_abi.BatchOutputC * B)()
+    results = []
+    dim = 0
+    for k, prob in enumerate(problems):
+        a = np.ascontiguousarray(prob.source_distribution, dtype=np.float64)
+        b = np.ascontiguousarray(prob.target_distribution, dtype=np.float64)
+        m, n = a.shape[0], b.shape[0]
+        rows[k], cols[k] = m, n
+        srcs[k], tgts[k] = a.ctypes.data, b.ctypes.data
+        keep += [a, b]
+        if cost == "f32":
+            C = np.asfortranarray(prob.cost_matrix, dtype=np.float64)
+            if C.shape != (m, n):
+                raise ValueError(f"instance {k}: cost matrix shape {C.shape} != {(m, n)}")
+            costs[k] = C.ctypes.data
+            keep.append(C)
+        else:
+            xs = np.ascontiguousarray(points[k][0], dtype=np.float32)
+            ys = np.ascontiguousarray(points[k][1], dtype=np.float32)
+            if xs.ndim == 1:
+                xs, ys = xs[:, None], ys[:, None]
+            dim = xs.shape[1]
+            xs_p[k], ys_p[k] = xs.ctypes.data, ys.ctypes.data
+            keep += [xs, ys]
+        X = np.zeros((m, n), order="F")
+        u = np.zeros(m)
+        v = np.zeros(n)
+        outs[k].primal_solution = _dptr(X)
+        outs[k].dual_source_solution = _dptr(u)
+        outs[k].dual_target_solution = _dptr(v)
+        results.append((X, u, v))
+    bp = _abi.BatchProblemC()
+    bp.num_instances = B
+    bp.num_rows = rows
+    bp.num_cols = cols
+    bp.source_distributions = srcs
+    bp.target_distributions = tgts
+    if cost == "f32":
+        bp.cost_matrices = costs
+    else:
+        bp.source_points = xs_p
+        bp.target_points = ys_p
+    opts, _k = _options(device, use_cuda_graph, precision="f32", cost=cost)
+    if cost != "f32":
+        opts.point_dim = dim
+    opts.ctas_per_sm = int(ctas_per_sm)
+    cp = marshal_params(params)
+    sec = ct.c_double(0.0)
+    rc = lib.pdot_optimize_batched(ct.byref(bp), ct.byref(cp), ct.byref(opts), outs, ct.byref(sec))
+    _abi.check(lib, rc, "pdot_optimize_batched")
+    out = []
+    for k, (X, u, v) in enumerate(results):
+        reason = TerminationReason(outs[k].termination_reason)
+        out.append(SaddlePointOutput(X, u, v, reason, termination_reason_to_string(reason),
+                                     int(outs[k].iteration_count), [stats_from_c(outs[k].final_stats)]))
+    return out, sec.value

@@ -85,3 +85,30 @@ def grid_cost(side: int = 32) -> np.ndarray:
 def grid_histograms(seed: int = 0, side: int = 32) -> OptimalTransportProblem:
     rng = np.random.default_rng(seed)
     return OptimalTransportProblem(grid_cost(side), grid_histogram(rng, side), grid_histogram(rng, side))
+
+
+def batched_l1(count: int = 512, lo: int = 64, hi: int = 2048, seed: int = 0):
+    """`count` instances with m, n each log-uniform in [lo, hi], points U[0,1]^2,
+    marginals Dirichlet(1). Returns (problems without cost matrices, points):
+    the L1 cost |x - y|_1 / max is computed from the points."""
+    rng = np.random.default_rng(seed)
+    probs, pts = [], []
+    for _ in range(count):
+        m = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
+        n = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
+        xs = rng.uniform(0.0, 1.0, size=(m, 2))
+        ys = rng.uniform(0.0, 1.0, size=(n, 2))
+        probs.append(OptimalTransportProblem(None, rng.dirichlet(np.ones(m)), rng.dirichlet(np.ones(n))))
+        pts.append((xs, ys))
+    return probs, pts
+
+
+def l1_cost(xs: np.ndarray, ys: np.ndarray) -> np.ndarray:
+    """C_ij = ||x_i - y_j||_1 / max(C), Fortran-ordered float64."""
+    C = np.zeros((xs.shape[0], ys.shape[0]), order="F")
+    for k in range(xs.shape[1]):
+        C += np.abs(xs[:, k : k + 1] - ys[None, :, k])
+    mx = C.max()
+    if mx > 0:
+        C /= mx
+    return C

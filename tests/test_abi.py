@@ -52,6 +52,8 @@ STRUCTS = {
     "pdot_convergence_information": _abi.ConvergenceInformationC,
     "pdot_iteration_stats": _abi.IterationStatsC,
     "pdot_saddle_point_output": _abi.SaddlePointOutputC,
+    "pdot_batch_problem": _abi.BatchProblemC,
+    "pdot_batch_output": _abi.BatchOutputC,
 }
 
 

@@ -1,0 +1,98 @@
+"""The batched solver (pdot_optimize_batched): many instances of uneven sizes,
+each with its own step size, restarts and termination, in one lockstep solve.
+
+Each instance is checked against the FP64 problem built from the same
+coordinates: OPTIMAL, FP64 relative KKT of its returned solution within 2x the
+tolerance (FP32 plans), objective within the tolerance band of the FP64
+single-instance solve. Sizes cover a single row/column, rows that are not a
+multiple of 4 (padded plan storage) and more than one row panel.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import pdot
+from pdot import instances
+
+pytestmark = pytest.mark.gpu
+
+OPTIMAL = pdot.TerminationReason.TERMINATION_REASON_OPTIMAL
+
+
+def fp64_kkt(C, a, b, X, u, v):
+    pres = math.sqrt(np.sum((a - X.sum(axis=1)) ** 2) + np.sum((b - X.sum(axis=0)) ** 2))
+    dres = float(np.linalg.norm(np.minimum(C - u[:, None] - v[None, :], 0.0)))
+    pobj, dobj = float(np.vdot(C, X)), float(a @ u + b @ v)
+    return pobj, max(pres / (1 + np.linalg.norm(np.concatenate([a, b]))), dres / (1 + np.linalg.norm(C)),
+                     abs(pobj - dobj) / (1 + abs(pobj) + abs(dobj)))
+
+
+SIZES = [(1, 1), (1, 17), (13, 1), (7, 5), (64, 64), (130, 77), (257, 300), (511, 129), (600, 601)]
+
+
+@pytest.mark.parametrize("cost", ["l1", "sqeuclid", "f32"])
+def test_batched_instances_solve_their_fp64_problems(cuda, cost):
+    tol = 1e-4
+    rng = np.random.default_rng(7)
+    probs, pts, fp64 = [], [], []
+    for m, n in SIZES:
+        xs, ys = rng.uniform(0, 1, (m, 2)).astype(np.float32), rng.uniform(0, 1, (n, 2)).astype(np.float32)
+        a, b = rng.dirichlet(np.ones(m)), rng.dirichlet(np.ones(n))
+        C = (instances.l1_cost if cost == "l1" else instances.sqeuclid_cost)(xs.astype(np.float64),
+                                                                             ys.astype(np.float64))
+        fp64.append(pdot.OptimalTransportProblem(C, a, b))
+        probs.append(pdot.OptimalTransportProblem(C if cost == "f32" else None, a, b))
+        pts.append((xs, ys))
+    params = pdot.default_parameters(tol)
+    outs, seconds = pdot.optimize_batched(params, probs, cost=cost, points=None if cost == "f32" else pts)
+    assert seconds > 0
+    for (m, n), o, p64 in zip(SIZES, outs, fp64):
+        assert o.termination_reason == OPTIMAL, (m, n, o.termination_string)
+        pobj, kkt = fp64_kkt(p64.cost_matrix, p64.source_distribution, p64.target_distribution,
+                             o.primal_solution, o.dual_source_solution, o.dual_target_solution)
+        assert kkt <= 2 * tol, (m, n, kkt)
+        ref = pdot.optimize(params, p64)
+        ref_obj = ref.iteration_stats[-1].convergence_information[0].primal_objective
+        assert abs(pobj - ref_obj) <= 2 * tol * (1 + abs(ref_obj)), (m, n)
+
+
+def test_batched_matches_single_instance_mixed_precision_early(cuda):
+    """Same arithmetic per entry as the single-instance FP32 solve of one
+    instance: the first evaluations agree to rounding of the sums."""
+    rng = np.random.default_rng(3)
+    m, n = 300, 200
+    xs, ys = rng.uniform(0, 1, (m, 2)).astype(np.float32), rng.uniform(0, 1, (n, 2)).astype(np.float32)
+    a, b = rng.dirichlet(np.ones(m)), rng.dirichlet(np.ones(n))
+    prob = pdot.OptimalTransportProblem(None, a, b)
+    params = pdot.default_parameters(1e-4, iteration_limit=9)
+    single = pdot.optimize(params, prob, precision="f32", cost="l1", points=(xs, ys))
+    outs, _ = pdot.optimize_batched(params, [prob], cost="l1", points=[(xs, ys)])
+    assert outs[0].iteration_count == single.iteration_count
+    cs = single.iteration_stats[-1].convergence_information[0]
+    cb = outs[0].iteration_stats[-1].convergence_information[0]
+    assert cb.primal_objective == pytest.approx(cs.primal_objective, rel=1e-7, abs=1e-12)
+    assert cb.l2_primal_residual == pytest.approx(cs.l2_primal_residual, rel=1e-7)
+    np.testing.assert_allclose(outs[0].dual_source_solution, single.dual_source_solution, rtol=1e-7, atol=1e-12)
+
+
+def test_batched_invalid_instance_does_not_stop_the_others(cuda):
+    rng = np.random.default_rng(1)
+    probs = []
+    for m, n in [(40, 30), (20, 25), (33, 33)]:
+        C = np.asfortranarray(rng.uniform(0, 1, (m, n)))
+        probs.append(pdot.OptimalTransportProblem(C, rng.dirichlet(np.ones(m)), rng.dirichlet(np.ones(n))))
+    probs[1].cost_matrix[3, 4] = math.nan
+    outs, _ = pdot.optimize_batched(pdot.default_parameters(1e-4), probs, cost="f32")
+    assert outs[1].termination_reason == pdot.TerminationReason.TERMINATION_REASON_INVALID_PROBLEM
+    assert outs[0].termination_reason == OPTIMAL and outs[2].termination_reason == OPTIMAL
+
+
+def test_batched_is_deterministic(cuda):
+    probs, pts = instances.batched_l1(count=24, lo=16, hi=300, seed=5)
+    params = pdot.default_parameters(1e-4)
+    o1, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts)
+    o2, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts)
+    for x, y in zip(o1, o2):
+        assert x.iteration_count == y.iteration_count
+        assert np.array_equal(x.primal_solution, y.primal_solution)

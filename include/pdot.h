@@ -156,7 +156,8 @@ typedef struct pdot_solver_options {
   const double* warm_dual_target;     /* n initial target duals, or NULL */
   int32_t primal_pass;                /* PDOT_PASS_AUTO, _STAGED or _DIRECT */
   int32_t ctas_per_sm;                /* batched solver: CTAs per SM of its matrix passes (0 = most) */
-  int32_t reserved[6];                /* must be zero */
+  const double* warm_primal;          /* m x n column-major initial plan (needs the warm duals), or NULL */
+  int32_t reserved[4];                /* must be zero */
 } pdot_solver_options;
 
 /* ---- output -------------------------------------------------------------- */
@@ -325,6 +326,11 @@ typedef struct pdot_batch_problem {
   const double* const* target_distributions;
   const float* const* source_points;        /* m x point_dim, row-major, or NULL */
   const float* const* target_points;        /* n x point_dim */
+  /* Warm starts (NULL arrays, or NULL entries, start that instance at zero):
+   * initial duals and, optionally, an initial plan (column-major, m x n). */
+  const double* const* warm_dual_sources;
+  const double* const* warm_dual_targets;
+  const double* const* warm_primals;
 } pdot_batch_problem;
 
 typedef struct pdot_batch_output {          /* one per instance; arrays may be NULL */

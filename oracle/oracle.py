@@ -42,6 +42,11 @@ def load():
     ]
     P = ct.c_void_p
     D = ct.c_double
+    lib.pdot_oracle_optimize_warm.restype = ct.c_int
+    lib.pdot_oracle_optimize_warm.argtypes = [
+        ct.POINTER(_abi.ProblemC), ct.POINTER(_abi.PdhgParametersC), ct.c_void_p, ct.c_void_p, ct.c_void_p,
+        ct.c_double, ct.POINTER(_abi.SaddlePointOutputC), ct.c_int,
+    ]
     lib.pdot_oracle_primal_pass.restype = None
     lib.pdot_oracle_primal_pass.argtypes = [
         ct.c_int64, ct.c_int64, P, P, P, P, P, D, D, D, ct.c_int32, P, P, P,
@@ -68,6 +73,29 @@ def optimize(params, problem, num_threads: int = 0):
     cp = api.marshal_params(params)
     ob = api.OutputBuffers(mp.m, mp.n, api.stats_capacity_for(params))
     rc = lib.pdot_oracle_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(ob.c), int(num_threads))
+    if rc != 0:
+        raise _abi.PdotError(rc, f"oracle optimize failed ({rc})")
+    return ob.to_output()
+
+
+def optimize_warm(params, problem, u0, v0, X0=None, omega0=0.0, num_threads: int = 0):
+    """The oracle's solve from a warm start (initial duals, optional plan and
+    primal weight)."""
+    from pdot import api, _abi
+
+    api.validate(params)
+    lib = load()
+    mp = api.MarshalledProblem(problem)
+    cp = api.marshal_params(params)
+    ob = api.OutputBuffers(mp.m, mp.n, api.stats_capacity_for(params))
+    u0 = np.ascontiguousarray(u0, dtype=np.float64)
+    v0 = np.ascontiguousarray(v0, dtype=np.float64)
+    X0p = None
+    if X0 is not None:
+        X0 = np.asfortranarray(X0, dtype=np.float64)
+        X0p = X0.ctypes.data
+    rc = lib.pdot_oracle_optimize_warm(ct.byref(mp.c), ct.byref(cp), u0.ctypes.data, v0.ctypes.data, X0p,
+                                       float(omega0), ct.byref(ob.c), int(num_threads))
     if rc != 0:
         raise _abi.PdotError(rc, f"oracle optimize failed ({rc})")
     return ob.to_output()

@@ -613,8 +613,23 @@ static int ostate_init(ostate* S, const pdot_problem* P) {
 }
 
 /* ---- src/solver_gpu.jl:413-720  optimize ----------------------------- */
+int pdot_oracle_optimize_warm(const pdot_problem* P, const pdot_pdhg_parameters* prm, const double* u0,
+                              const double* v0, const double* X0, double omega0,
+                              pdot_saddle_point_output* out, int num_threads);
+
 int pdot_oracle_optimize(const pdot_problem* P, const pdot_pdhg_parameters* prm,
                          pdot_saddle_point_output* out, int num_threads) {
+  return pdot_oracle_optimize_warm(P, prm, NULL, NULL, NULL, 0.0, out, num_threads);
+}
+
+/* Warm start (an addition; the reference always starts at zero,
+ * src/solver_gpu.jl:428-441): initial duals u0, v0, optional initial plan X0
+ * (its row and column sums become r and c) and optional initial primal weight
+ * (omega0 > 0). The stored gradient is C - u0 - v0 from the start. The last
+ * restart point stays the zero point, as in the CUDA solver. */
+int pdot_oracle_optimize_warm(const pdot_problem* P, const pdot_pdhg_parameters* prm, const double* u0,
+                              const double* v0, const double* X0, double omega0,
+                              pdot_saddle_point_output* out, int num_threads) {
   int rc = pdot_oracle_validate(P, prm);
   if (rc != PDOT_OK) return rc;
 #ifdef _OPENMP
@@ -642,6 +657,29 @@ int pdot_oracle_optimize(const pdot_problem* P, const pdot_pdhg_parameters* prm,
                                                 : prm->primal_importance;
   } else {
     S->primal_weight = prm->primal_importance;
+  }
+  if (omega0 > 0.0) S->primal_weight = omega0;
+  if (u0 && v0) {
+    memcpy(S->u, u0, sizeof(double) * m);
+    memcpy(S->v, v0, sizeof(double) * n);
+    if (X0) {
+      memcpy(S->X, X0, sizeof(double) * N);
+      for (i64 j = 0; j < n; ++j)
+        for (i64 i = 0; i < m; ++i) {
+          S->r[i] += X0[i + j * m];
+          S->c[j] += X0[i + j * m];
+        }
+    }
+    for (i64 j = 0; j < n; ++j)
+      for (i64 i = 0; i < m; ++i) S->G[i + j * m] = (S->C[i + j * m] - S->u[i]) - S->v[j];
+    if (getenv("PDOT_WARM_RESTART_POINT")) {
+      memcpy(S->Xl, S->X, sizeof(double) * N);
+      memcpy(S->ul, S->u, sizeof(double) * m);
+      memcpy(S->vl, S->v, sizeof(double) * n);
+      memcpy(S->rl, S->r, sizeof(double) * m);
+      memcpy(S->cl, S->c, sizeof(double) * n);
+      memcpy(S->Gl, S->G, sizeof(double) * N);
+    }
   }
   const double smoothing = prm->restart_params.primal_weight_update_smoothing;
   const double start_time = now_sec();

@@ -150,6 +150,40 @@ __global__ void k_divide_by_max(int64_t N, double* __restrict__ C, const double*
     C[e] = __ddiv_rn(C[e], mx);
 }
 
+// Row and column sums of a plan in storage type TX (the sums of a warm-start
+// plan): row partials over column chunks, then their fixed-order total; one CTA
+// per column for the column sums.
+template <typename TX>
+__global__ void k_plan_row_partials(int64_t m, int64_t n, const TX* __restrict__ X, double* __restrict__ part) {
+  const int64_t i = (int64_t)blockIdx.x * kAuxThreads + threadIdx.x;
+  const int64_t j0 = (int64_t)blockIdx.y * kColChunk;
+  const int64_t j1 = (j0 + kColChunk < n) ? j0 + kColChunk : n;
+  if (i >= m) return;
+  double s = 0.0;
+  for (int64_t j = j0; j < j1; ++j) s += (double)X[i + j * m];
+  part[(int64_t)blockIdx.y * m + i] = s;
+}
+
+template <typename TX>
+__global__ void k_plan_col_sums(int64_t m, const TX* __restrict__ X, double* __restrict__ out) {
+  __shared__ double sh[kAuxThreads];
+  const int64_t j = blockIdx.x;
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < m; i += kAuxThreads) s += (double)X[i + j * m];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = kAuxThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[j] = sh[0];
+}
+
+__global__ void k_plan_row_totals(int64_t m, int chunks, const double* __restrict__ part, double* __restrict__ r) {
+  const int64_t i = (int64_t)blockIdx.x * kAuxThreads + threadIdx.x;
+  if (i < m) r[i] = row_sum(part, m, chunks, i);
+}
+
 int grid_for(int64_t count) {
   int64_t g = (count + kAuxThreads - 1) / kAuxThreads;
   return (int)(g < 1 ? 1 : (g > 148 * 16 ? 148 * 16 : g));
@@ -184,6 +218,26 @@ cudaError_t launch_rounding(int64_t m, int64_t n, const double* a, const double*
   k_norm1<<<1, kAuxThreads, 0, s>>>(m, rscale, norm1);
   k_col_sums<<<(unsigned)n, kAuxThreads, 0, s>>>(m, X, colsum);
   k_rank_one<<<eg, kAuxThreads, 0, s>>>(m, n, X, rscale, norm1, colsum, b);
+  return cudaGetLastError();
+}
+
+size_t plan_sums_workspace_doubles(int64_t m, int64_t n) {
+  return (size_t)((n + kColChunk - 1) / kColChunk) * (size_t)m;
+}
+
+cudaError_t launch_plan_sums(int64_t m, int64_t n, const void* X, int plan_f32, double* r, double* c, double* work,
+                             cudaStream_t s) {
+  const int chunks = (int)((n + kColChunk - 1) / kColChunk);
+  const dim3 rgrid((unsigned)((m + kAuxThreads - 1) / kAuxThreads), (unsigned)chunks);
+  const int rb = (int)((m + kAuxThreads - 1) / kAuxThreads);
+  if (plan_f32) {
+    k_plan_row_partials<float><<<rgrid, kAuxThreads, 0, s>>>(m, n, static_cast<const float*>(X), work);
+    k_plan_col_sums<float><<<(unsigned)n, kAuxThreads, 0, s>>>(m, static_cast<const float*>(X), c);
+  } else {
+    k_plan_row_partials<double><<<rgrid, kAuxThreads, 0, s>>>(m, n, static_cast<const double*>(X), work);
+    k_plan_col_sums<double><<<(unsigned)n, kAuxThreads, 0, s>>>(m, static_cast<const double*>(X), c);
+  }
+  k_plan_row_totals<<<rb, kAuxThreads, 0, s>>>(m, chunks, work, r);
   return cudaGetLastError();
 }
 

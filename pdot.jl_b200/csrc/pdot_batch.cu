@@ -74,6 +74,7 @@ struct BatchBuffers {
   double* steppart;        // total vector blocks * kStepSums
   double* evpart;          // (grid + num) * kEvalSums
   double* vecpart;         // total vector blocks * kVecSums
+  const int* warm;         // per instance: 1 when it starts from a warm start
   DevState* st;            // per instance
   pdot_iteration_stats* rec;  // per instance: the latest evaluation record
   BatchActive* act;
@@ -633,7 +634,7 @@ __global__ void kb_init_state(BatchBuffers B, SolveConfig cfg, int grid) {
   st->last_rp = st->l2_rhs;
   st->ratio_last_trial = 1.0;
   st->last_restart_length = 1;
-  st->g_is_zero = 1;
+  st->g_is_zero = B.warm[k] ? 0 : 1;
   st->out_current = 1;
   if (!(isfinite(st->l2_obj) && isfinite(st->l2_rhs) && isfinite(st->linf_obj))) {
     st->done = 1;
@@ -810,6 +811,50 @@ class BatchSolver {
     }
     rows_ = ro;
     cols_ = co;
+    // warm starts: duals, the plan narrowed to FP32 (padded columns) and its sums
+    std::vector<int> warm(B, 0);
+    for (int k = 0; k < B; ++k)
+      if (P.warm_dual_sources && P.warm_dual_targets && P.warm_dual_sources[k] && P.warm_dual_targets[k])
+        warm[k] = 1;
+      else if (P.warm_primals && P.warm_primals[k])
+        bfail(PDOT_ERR_INVALID_ARGUMENT, "instance %d: a warm-start plan needs the warm-start dual vectors", k);
+    any_warm_ = false;
+    for (int k = 0; k < B; ++k) any_warm_ = any_warm_ || warm[k];
+    D_.warm = upload(warm.data(), B);
+    if (any_warm_) {
+      std::vector<double> hu(ro, 0.0), hv(co, 0.0), hr(ro, 0.0), hc(co, 0.0);
+      std::vector<float> hx;
+      warm_x_ = alloc<float>(total_x_);
+      BCK(cudaMemsetAsync(warm_x_, 0, total_x_ * sizeof(float), stream_));
+      for (int k = 0; k < B; ++k) {
+        if (!warm[k]) continue;
+        const pdot::BatchInstance& I = inst_[k];
+        memcpy(hu.data() + I.row_off, P.warm_dual_sources[k], I.m * sizeof(double));
+        memcpy(hv.data() + I.col_off, P.warm_dual_targets[k], I.n * sizeof(double));
+        if (!P.warm_primals || !P.warm_primals[k]) continue;
+        const double* X0 = P.warm_primals[k];
+        hx.assign((size_t)I.ld * I.n, 0.0f);
+        for (int64_t j = 0; j < I.n; ++j) {
+          double cs = 0.0;
+          for (int64_t i = 0; i < I.m; ++i) {
+            const float x = (float)X0[i + j * I.m];
+            hx[i + j * I.ld] = x;
+            cs += (double)x;
+            hr[I.row_off + i] += (double)x;
+          }
+          hc[I.col_off + j] = cs;
+        }
+        BCK(cudaMemcpy(warm_x_ + I.x_off, hx.data(), hx.size() * sizeof(float), cudaMemcpyHostToDevice));
+      }
+      warm_u_ = alloc<double>(ro);
+      warm_v_ = alloc<double>(co);
+      warm_r_ = alloc<double>(ro);
+      warm_c_ = alloc<double>(co);
+      BCK(cudaMemcpy(warm_u_, hu.data(), ro * sizeof(double), cudaMemcpyHostToDevice));
+      BCK(cudaMemcpy(warm_v_, hv.data(), co * sizeof(double), cudaMemcpyHostToDevice));
+      BCK(cudaMemcpy(warm_r_, hr.data(), ro * sizeof(double), cudaMemcpyHostToDevice));
+      BCK(cudaMemcpy(warm_c_, hc.data(), co * sizeof(double), cudaMemcpyHostToDevice));
+    }
     D_.rowpart = alloc<double>(((size_t)grid_ + total_panels_) * pdot::kPanelRows);
     D_.colpart = alloc<double>(total_units_);
     D_.sqpart = alloc<double>((size_t)grid_ + B);
@@ -916,14 +961,22 @@ class BatchSolver {
     c.warm_start = 0;
   }
 
-  // zero starts, cost norms, initial states, the first active list
+  // zero (or warm) starts, cost norms, initial states, the first active list
   void init() {
-    BCK(cudaMemsetAsync(D_.X[0], 0, total_x_ * sizeof(float), stream_));
     BCK(cudaMemsetAsync(D_.X[1], 0, total_x_ * sizeof(float), stream_));
-    BCK(cudaMemsetAsync(D_.u[0], 0, rows_ * sizeof(double), stream_));
-    BCK(cudaMemsetAsync(D_.r[0], 0, rows_ * sizeof(double), stream_));
-    BCK(cudaMemsetAsync(D_.v[0], 0, cols_ * sizeof(double), stream_));
-    BCK(cudaMemsetAsync(D_.c[0], 0, cols_ * sizeof(double), stream_));
+    if (any_warm_) {
+      BCK(cudaMemcpyAsync(D_.X[0], warm_x_, total_x_ * sizeof(float), cudaMemcpyDeviceToDevice, stream_));
+      BCK(cudaMemcpyAsync(D_.u[0], warm_u_, rows_ * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+      BCK(cudaMemcpyAsync(D_.r[0], warm_r_, rows_ * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+      BCK(cudaMemcpyAsync(D_.v[0], warm_v_, cols_ * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+      BCK(cudaMemcpyAsync(D_.c[0], warm_c_, cols_ * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    } else {
+      BCK(cudaMemsetAsync(D_.X[0], 0, total_x_ * sizeof(float), stream_));
+      BCK(cudaMemsetAsync(D_.u[0], 0, rows_ * sizeof(double), stream_));
+      BCK(cudaMemsetAsync(D_.r[0], 0, rows_ * sizeof(double), stream_));
+      BCK(cudaMemsetAsync(D_.v[0], 0, cols_ * sizeof(double), stream_));
+      BCK(cudaMemsetAsync(D_.c[0], 0, cols_ * sizeof(double), stream_));
+    }
     BCK(cudaMemsetAsync(D_.st, 0, num_ * sizeof(pdot::DevState), stream_));
     pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_);
     BCK(cudaGetLastError());
@@ -1017,7 +1070,9 @@ class BatchSolver {
   }
 
   int device_ = 0, num_ = 0, dim_ = 0, kind_ = 0, grid_ = 1;
-  bool use_graph_ = true;
+  bool use_graph_ = true, any_warm_ = false;
+  float* warm_x_ = nullptr;
+  double *warm_u_ = nullptr, *warm_v_ = nullptr, *warm_r_ = nullptr, *warm_c_ = nullptr;
   int64_t total_x_ = 0, total_units_ = 0, total_panels_ = 0, total_vblocks_ = 0, rows_ = 0, cols_ = 0;
   long long freq_ = 128, limit_ = 0;
   std::vector<pdot::BatchInstance> inst_;

@@ -191,6 +191,10 @@ cudaError_t launch_convert_cost(const double* src, void* dst, int cost_kind, siz
 cudaError_t launch_widen(const float* src, double* dst, size_t count, cudaStream_t s);
 
 // Passes around a solve (pdot_aux.cu).
+size_t plan_sums_workspace_doubles(int64_t m, int64_t n);
+// r = X 1 and c = X^T 1 of an m x n column-major plan (FP32 when plan_f32)
+cudaError_t launch_plan_sums(int64_t m, int64_t n, const void* X, int plan_f32, double* r, double* c, double* work,
+                             cudaStream_t s);
 size_t rounding_workspace_doubles(int64_t m, int64_t n);
 cudaError_t launch_rounding(int64_t m, int64_t n, const double* a, const double* b, double* X, double* work,
                             cudaStream_t s);

@@ -125,6 +125,7 @@ struct Variant {
   double cost_scale = 0.0;
   const double* warm_u = nullptr;
   const double* warm_v = nullptr;
+  const double* warm_x = nullptr;
   int staged = 2;  // 0 direct, 1 staged, 2 automatic
 };
 
@@ -161,10 +162,13 @@ Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
     fail(PDOT_ERR_INVALID_ARGUMENT, "give both warm-start dual vectors or neither");
   v.warm_u = o->warm_dual_source;
   v.warm_v = o->warm_dual_target;
+  if (o->warm_primal && !o->warm_dual_source)
+    fail(PDOT_ERR_INVALID_ARGUMENT, "a warm-start plan needs the warm-start dual vectors");
+  v.warm_x = o->warm_primal;
   if (o->primal_pass != PDOT_PASS_AUTO && o->primal_pass != PDOT_PASS_STAGED && o->primal_pass != PDOT_PASS_DIRECT)
     fail(PDOT_ERR_INVALID_ARGUMENT, "unknown primal_pass %d", o->primal_pass);
   v.staged = o->primal_pass == PDOT_PASS_STAGED ? 1 : (o->primal_pass == PDOT_PASS_DIRECT ? 0 : 2);
-  for (int k = 0; k < 6; ++k)
+  for (int k = 0; k < 4; ++k)
     if (o->reserved[k] != 0) fail(PDOT_ERR_INVALID_ARGUMENT, "reserved option fields must be zero");
   return v;
 }
@@ -294,6 +298,34 @@ class Solver {
       CK(cudaMemcpyAsync(warm_u_, var.warm_u, m * sizeof(double), kind, stream_));
       CK(cudaMemcpyAsync(warm_v_, var.warm_v, n * sizeof(double), kind, stream_));
     }
+    if (var.warm_x) {
+      // the warm plan in plan precision, and its row and column sums
+      void* wx = nullptr;
+      CK(cudaMalloc(&wx, std::max<size_t>(N, 1) * xbytes));
+      allocs_.push_back(wx);
+      warm_x_ = wx;
+      alloc(&warm_r_, m);
+      alloc(&warm_c_, n);
+      const double* src = var.warm_x;
+      double* tmp = nullptr;
+      if (!device_inputs || var.plan_f32) {
+        if (!device_inputs) {
+          CK(cudaMalloc(&tmp, std::max<size_t>(N, 1) * sizeof(double)));
+          CK(cudaMemcpyAsync(tmp, var.warm_x, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
+          src = tmp;
+        }
+      }
+      if (var.plan_f32)
+        CK(pdot::launch_convert_cost(src, wx, PDOT_COST_F32, N, stream_));
+      else
+        CK(cudaMemcpyAsync(wx, src, N * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+      double* work = nullptr;
+      CK(cudaMalloc(&work, std::max<size_t>(pdot::plan_sums_workspace_doubles(m, n), 1) * sizeof(double)));
+      CK(pdot::launch_plan_sums(m, n, wx, var.plan_f32, warm_r_, warm_c_, work, stream_));
+      CK(cudaStreamSynchronize(stream_));
+      CK(cudaFree(work));
+      if (tmp) CK(cudaFree(tmp));
+    }
     void* xp = nullptr;
     for (int k = 0; k < 2; ++k) {
       CK(cudaMalloc(&xp, std::max<size_t>(N, 1) * xbytes));
@@ -377,13 +409,17 @@ class Solver {
 
   cudaStream_t stream() const { return stream_; }
 
-  // CuPdhgSolverState starts at zero (src/solver_gpu.jl:428-441); the average
+  // CuPdhgSolverState starts at zero (src/solver_gpu.jl:428-441), or at the
+  // warm start (duals, and the plan with its row and column sums); the average
   // halves need no clearing: the first accepted step overwrites them.
   void reset() {
     CK(cudaSetDevice(device_));
     CK(cudaStreamSynchronize(stream_));
     const size_t N = (size_t)g_.m * (size_t)g_.n;
-    CK(cudaMemsetAsync(X_[0], 0, N * xbytes_, stream_));
+    if (warm_x_)
+      CK(cudaMemcpyAsync(X_[0], warm_x_, N * xbytes_, cudaMemcpyDeviceToDevice, stream_));
+    else
+      CK(cudaMemsetAsync(X_[0], 0, N * xbytes_, stream_));
     if (warm_u_) {
       CK(cudaMemcpyAsync(u_[0], warm_u_, g_.m * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
       CK(cudaMemcpyAsync(v_[0], warm_v_, g_.n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
@@ -391,8 +427,13 @@ class Solver {
       CK(cudaMemsetAsync(u_[0], 0, g_.m * sizeof(double), stream_));
       CK(cudaMemsetAsync(v_[0], 0, g_.n * sizeof(double), stream_));
     }
-    CK(cudaMemsetAsync(r_[0], 0, g_.m * sizeof(double), stream_));
-    CK(cudaMemsetAsync(c_[0], 0, g_.n * sizeof(double), stream_));
+    if (warm_x_) {
+      CK(cudaMemcpyAsync(r_[0], warm_r_, g_.m * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+      CK(cudaMemcpyAsync(c_[0], warm_c_, g_.n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    } else {
+      CK(cudaMemsetAsync(r_[0], 0, g_.m * sizeof(double), stream_));
+      CK(cudaMemsetAsync(c_[0], 0, g_.n * sizeof(double), stream_));
+    }
     CK(cudaMemsetAsync(st_, 0, sizeof(pdot::DevState), stream_));
     CK(pdot::launch_init(B_, g_, cfg_, stream_));
     CK(cudaStreamSynchronize(stream_));
@@ -647,6 +688,9 @@ class Solver {
   const double* b_ = nullptr;
   double* warm_u_ = nullptr;
   double* warm_v_ = nullptr;
+  void* warm_x_ = nullptr;
+  double* warm_r_ = nullptr;
+  double* warm_c_ = nullptr;
   void* X_[2] = {};
   size_t xbytes_ = sizeof(double);
   double* u_[2] = {};

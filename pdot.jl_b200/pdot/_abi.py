@@ -97,7 +97,8 @@ class SolverOptionsC(ct.Structure):
         ("warm_dual_target", ct.POINTER(ct.c_double)),
         ("primal_pass", ct.c_int32),
         ("ctas_per_sm", ct.c_int32),
-        ("reserved", ct.c_int32 * 6),
+        ("warm_primal", ct.POINTER(ct.c_double)),
+        ("reserved", ct.c_int32 * 4),
     ]
 
 
@@ -130,6 +131,9 @@ class BatchProblemC(ct.Structure):
         ("target_distributions", ct.POINTER(ct.c_void_p)),
         ("source_points", ct.POINTER(ct.c_void_p)),
         ("target_points", ct.POINTER(ct.c_void_p)),
+        ("warm_dual_sources", ct.POINTER(ct.c_void_p)),
+        ("warm_dual_targets", ct.POINTER(ct.c_void_p)),
+        ("warm_primals", ct.POINTER(ct.c_void_p)),
     ]
 
 

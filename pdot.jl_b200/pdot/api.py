@@ -378,7 +378,8 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
                "f64" for an FP64 plan and "f32" for an FP32 plan
     points     (xs, ys) coordinate arrays (m x d, n x d) for "sqeuclid"; with
                device_pointers, (xs_ptr, ys_ptr, d)
-    warm_start (u0, v0) initial duals; with device_pointers, (u_ptr, v_ptr)
+    warm_start (u0, v0) initial duals, or (u0, v0, X0) with an initial plan
+               (m x n); with device_pointers, (u_ptr, v_ptr[, X_ptr])
     """
     keep = []
     opts = _abi.SolverOptionsC()
@@ -412,12 +413,20 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
         if device_pointers:
             opts.warm_dual_source = ct.cast(ct.c_void_p(warm_start[0]), ct.POINTER(ct.c_double))
             opts.warm_dual_target = ct.cast(ct.c_void_p(warm_start[1]), ct.POINTER(ct.c_double))
+            if len(warm_start) > 2 and warm_start[2]:
+                opts.warm_primal = ct.cast(ct.c_void_p(warm_start[2]), ct.POINTER(ct.c_double))
         else:
             u0 = np.ascontiguousarray(warm_start[0], dtype=np.float64)
             v0 = np.ascontiguousarray(warm_start[1], dtype=np.float64)
             keep += [u0, v0]
             opts.warm_dual_source = _dptr(u0)
             opts.warm_dual_target = _dptr(v0)
+            if len(warm_start) > 2 and warm_start[2] is not None:
+                X0 = np.asfortranarray(warm_start[2], dtype=np.float64)
+                if X0.shape != (u0.shape[0], v0.shape[0]):
+                    raise ValueError(f"warm-start plan shape {X0.shape} != {(u0.shape[0], v0.shape[0])}")
+                keep.append(X0)
+                opts.warm_primal = _dptr(X0)
     return opts, keep
 
 
@@ -428,7 +437,7 @@ def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device
 
     The keyword options beyond `device` select this implementation's mixed
     precision (FP32 plan; FP32/BF16/coordinate cost) and a warm start from
-    given duals; the defaults are the FP64 drop-in."""
+    given duals (and plan); the defaults are the FP64 drop-in."""
     validate(params)
     lib = _abi.load()
     mp = MarshalledProblem(problem)
@@ -512,13 +521,16 @@ class Solver:
 
 
 def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", points=None, device: int = 0,
-                     use_cuda_graph: bool = True, ctas_per_sm: int = 0):
+                     use_cuda_graph: bool = True, ctas_per_sm: int = 0, warm_starts=None,
+                     return_primal: bool = True):
     """Solve many independent instances at once (pdot_optimize_batched).
 
-    problems  a list of OptimalTransportProblem (cost_matrix may be None for
-              coordinate costs)
-    cost      "f32" (each FP64 matrix stored in FP32), "sqeuclid" or "l1"
-              (from `points`, a list of (xs, ys) per instance)
+    problems     a list of OptimalTransportProblem (cost_matrix may be None for
+                 coordinate costs)
+    cost         "f32" (each FP64 matrix stored in FP32), "sqeuclid" or "l1"
+                 (from `points`, a list of (xs, ys) per instance)
+    warm_starts  None, or per instance None / (u0, v0) / (u0, v0, X0)
+    return_primal  False leaves every primal_solution None (no m x n copies)
     Returns (outputs, seconds): a SaddlePointOutput per instance (its
     iteration_stats holds the final evaluation record) and the device time.
     """
@@ -534,6 +546,9 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
     xs_p = (ct.c_void_p * B)()
     ys_p = (ct.c_void_p * B)()
     outs = (_abi.BatchOutputC * B)()
+    wu = (ct.c_void_p * B)()
+    wv = (ct.c_void_p * B)()
+    wx = (ct.c_void_p * B)()
     results = []
     dim = 0
     for k, prob in enumerate(problems):
@@ -557,10 +572,25 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
             dim = xs.shape[1]
             xs_p[k], ys_p[k] = xs.ctypes.data, ys.ctypes.data
             keep += [xs, ys]
-        X = np.zeros((m, n), order="F")
+        if warm_starts is not None and warm_starts[k] is not None:
+            w = warm_starts[k]
+            u0 = np.ascontiguousarray(w[0], dtype=np.float64)
+            v0 = np.ascontiguousarray(w[1], dtype=np.float64)
+            if u0.shape != (m,) or v0.shape != (n,):
+                raise ValueError(f"instance {k}: warm-start dual shapes {u0.shape}, {v0.shape}")
+            wu[k], wv[k] = u0.ctypes.data, v0.ctypes.data
+            keep += [u0, v0]
+            if len(w) > 2 and w[2] is not None:
+                X0 = np.asfortranarray(w[2], dtype=np.float64)
+                if X0.shape != (m, n):
+                    raise ValueError(f"instance {k}: warm-start plan shape {X0.shape} != {(m, n)}")
+                wx[k] = X0.ctypes.data
+                keep.append(X0)
+        X = np.zeros((m, n), order="F") if return_primal else None
         u = np.zeros(m)
         v = np.zeros(n)
-        outs[k].primal_solution = _dptr(X)
+        if X is not None:
+            outs[k].primal_solution = _dptr(X)
         outs[k].dual_source_solution = _dptr(u)
         outs[k].dual_target_solution = _dptr(v)
         results.append((X, u, v))
@@ -575,6 +605,10 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
     else:
         bp.source_points = xs_p
         bp.target_points = ys_p
+    if warm_starts is not None:
+        bp.warm_dual_sources = wu
+        bp.warm_dual_targets = wv
+        bp.warm_primals = wx
     opts, _k = _options(device, use_cuda_graph, precision="f32", cost=cost)
     if cost != "f32":
         opts.point_dim = dim

@@ -672,14 +672,6 @@ int pdot_oracle_optimize_warm(const pdot_problem* P, const pdot_pdhg_parameters*
     }
     for (i64 j = 0; j < n; ++j)
       for (i64 i = 0; i < m; ++i) S->G[i + j * m] = (S->C[i + j * m] - S->u[i]) - S->v[j];
-    if (getenv("PDOT_WARM_RESTART_POINT")) {
-      memcpy(S->Xl, S->X, sizeof(double) * N);
-      memcpy(S->ul, S->u, sizeof(double) * m);
-      memcpy(S->vl, S->v, sizeof(double) * n);
-      memcpy(S->rl, S->r, sizeof(double) * m);
-      memcpy(S->cl, S->c, sizeof(double) * n);
-      memcpy(S->Gl, S->G, sizeof(double) * N);
-    }
   }
   const double smoothing = prm->restart_params.primal_weight_update_smoothing;
   const double start_time = now_sec();

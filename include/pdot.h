@@ -157,7 +157,12 @@ typedef struct pdot_solver_options {
   int32_t primal_pass;                /* PDOT_PASS_AUTO, _STAGED or _DIRECT */
   int32_t ctas_per_sm;                /* batched solver: CTAs per SM of its matrix passes (0 = most) */
   const double* warm_primal;          /* m x n column-major initial plan (needs the warm duals), or NULL */
-  int32_t reserved[4];                /* must be zero */
+  /* > 0 with warm duals and no warm plan: the plan is recovered from the duals
+   * by warm_plan_iterations rounds of log-domain row/column balancing of
+   * exp((u_i + v_j - C_ij) / eps) (0 rounds: that kernel as it is) */
+  double warm_plan_epsilon;
+  int32_t warm_plan_iterations;
+  int32_t reserved[1];                /* must be zero */
 } pdot_solver_options;
 
 /* ---- output -------------------------------------------------------------- */
@@ -384,6 +389,37 @@ int pdot_primal_pass_f64_noalloc(int64_t m, int64_t n,
                                  int32_t flags,
                                  double* delta_row_sum, double* delta_col_sum, double* delta_sq_norm,
                                  void* stream);
+
+/* ---- the learned warm start ---------------------------------------------
+ * A small MLP predicts optimal dual potentials from the marginals; its warm
+ * start is finished by plain PDHG (pdot_solver_options.warm_dual_*). It has no
+ * counterpart in the reference. Layers input -> hidden -> hidden -> output
+ * with GELU; BF16 weights and activations, FP32 master weights, AdamW moments
+ * and accumulation; every product on the tensor cores (tcgen05). Widths are
+ * multiples of 128. Parameters are laid out W1 [hidden x input] (row-major),
+ * b1, W2 [hidden x hidden], b2, W3 [output x hidden], b3. Device pointers are
+ * on the network's device; calls are ordered on pdot_mlp_stream. */
+typedef struct pdot_mlp pdot_mlp;
+int pdot_mlp_create(int32_t device, int64_t input_dim, int64_t hidden_dim, int64_t output_dim,
+                    int64_t max_batch, uint64_t seed, pdot_mlp** out);
+int pdot_mlp_destroy(pdot_mlp* net);
+int64_t pdot_mlp_num_parameters(const pdot_mlp* net);
+void* pdot_mlp_stream(pdot_mlp* net);
+int pdot_mlp_get_parameters(pdot_mlp* net, float* host, int64_t count);
+int pdot_mlp_set_parameters(pdot_mlp* net, const float* host, int64_t count);  /* resets AdamW */
+int pdot_mlp_get_gradients(pdot_mlp* net, float* host, int64_t count);
+/* The input rows: x = bf16((log(max(h, 1e-30)) + shift) * scale) of the
+ * device array histograms [batch x input_dim] (row-major, FP64). */
+int pdot_mlp_set_input(pdot_mlp* net, int64_t batch, const double* histograms, double shift, double scale);
+/* Y = the network's output for the input rows; copied to `out` (device,
+ * batch x output_dim) when not NULL. */
+int pdot_mlp_forward(pdot_mlp* net, float* out);
+/* After pdot_mlp_forward: the gradients of the mean squared error against the
+ * device array target [batch x output_dim]; the loss to *loss when not NULL. */
+int pdot_mlp_backward(pdot_mlp* net, const float* target, double* loss);
+int pdot_mlp_adamw(pdot_mlp* net, float lr, float beta1, float beta2, float eps, float weight_decay);
+/* forward + backward + AdamW(beta1 0.9, beta2 0.999, eps 1e-8) */
+int pdot_mlp_train_step(pdot_mlp* net, const float* target, float lr, float weight_decay, double* loss);
 
 #ifdef __cplusplus
 }

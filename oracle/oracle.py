@@ -143,3 +143,20 @@ def rounding(problem, X):
     b = np.ascontiguousarray(problem.target_distribution, dtype=np.float64)
     lib.pdot_oracle_rounding(X.shape[0], X.shape[1], _p(a), _p(b), _p(X))
     return X
+
+
+def warm_plan(C, a, b, u0, v0, eps: float, rounds: int):
+    """The plan recovered from warm duals (csrc/pdot_warmplan.cu), in FP64:
+    `rounds` of log-domain balancing from (f, g) = (u0, v0), then
+    X = exp((f_i + g_j - C_ij) / eps). Returns (X, f, g)."""
+    from scipy.special import logsumexp
+
+    C = np.asarray(C, dtype=np.float64)
+    f = np.asarray(u0, dtype=np.float64).copy()
+    g = np.asarray(v0, dtype=np.float64).copy()
+    la, lb = np.log(a), np.log(b)
+    for _ in range(rounds):
+        f = eps * (la - logsumexp((g[None, :] - C) / eps, axis=1))
+        g = eps * (lb - logsumexp((f[:, None] - C) / eps, axis=0))
+    X = np.exp((f[:, None] + g[None, :] - C) / eps)
+    return X, f, g

@@ -22,6 +22,7 @@
 // Each instance's plan is stored column-major with its row count padded to a
 // multiple of 4 (16-byte FP32 vectors); padded rows hold zeros and are masked.
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -855,6 +856,46 @@ class BatchSolver {
       BCK(cudaMemcpy(warm_r_, hr.data(), ro * sizeof(double), cudaMemcpyHostToDevice));
       BCK(cudaMemcpy(warm_c_, hc.data(), co * sizeof(double), cudaMemcpyHostToDevice));
     }
+    // plans recovered from the warm duals of the instances given no warm plan
+    const double peps = opt ? opt->warm_plan_epsilon : 0.0;
+    if (opt && (!(peps >= 0.0) || !std::isfinite(peps) || opt->warm_plan_iterations < 0 ||
+                opt->warm_plan_iterations > 100000))
+      bfail(PDOT_ERR_INVALID_ARGUMENT, "warm_plan_epsilon must be finite and >= 0, warm_plan_iterations 0..100000");
+    if (peps > 0.0 && any_warm_) {
+      std::vector<pdot::PlanInstance> pi(B);
+      std::vector<long long> rp(B + 1, 0), cp(B + 1, 0);
+      for (int k = 0; k < B; ++k) {
+        const pdot::BatchInstance& I = inst_[k];
+        pi[k] = pdot::PlanInstance{I.m, I.n, I.ld, I.x_off, I.row_off, I.col_off,
+                                   (warm[k] && !(P.warm_primals && P.warm_primals[k])) ? 1 : 0, 0};
+        rp[k + 1] = rp[k] + I.m;
+        cp[k + 1] = cp[k] + I.n;
+      }
+      plan_iters_ = opt->warm_plan_iterations;
+      wp_.inst = upload(pi.data(), B);
+      wp_.num = B;
+      wp_.row_prefix = upload(rp.data(), B + 1);
+      wp_.col_prefix = upload(cp.data(), B + 1);
+      wp_.total_rows = ro;
+      wp_.total_cols = co;
+      wp_.kind = kind_;
+      wp_.dim = dim_;
+      wp_.C = D_.C;
+      wp_.xs = D_.xs;
+      wp_.ys = D_.ys;
+      wp_.a = D_.a;
+      wp_.b = D_.b;
+      wp_.u0 = warm_u_;
+      wp_.v0 = warm_v_;
+      wp_.f = alloc<double>(ro);
+      wp_.g = alloc<double>(co);
+      wp_.X = D_.X[0];
+      wp_.plan_f32 = 1;
+      wp_.r = D_.r[0];
+      wp_.c = D_.c[0];
+      wp_.eps = peps;
+      recover_plans_ = true;
+    }
     D_.rowpart = alloc<double>(((size_t)grid_ + total_panels_) * pdot::kPanelRows);
     D_.colpart = alloc<double>(total_units_);
     D_.sqpart = alloc<double>((size_t)grid_ + B);
@@ -984,6 +1025,10 @@ class BatchSolver {
     BCK(cudaGetLastError());
     pdot::kb_init_state<<<(num_ * 32 + 255) / 256, 256, 0, stream_>>>(D_, cfg_, grid_);
     BCK(cudaGetLastError());
+    if (recover_plans_) {
+      wp_.st = D_.st;  // allocated after the recovery arguments were set up
+      BCK(pdot::launch_warm_plan(wp_, plan_iters_, stream_));
+    }
     pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_);  // drops invalid problems
     BCK(cudaGetLastError());
   }
@@ -1070,7 +1115,9 @@ class BatchSolver {
   }
 
   int device_ = 0, num_ = 0, dim_ = 0, kind_ = 0, grid_ = 1;
-  bool use_graph_ = true, any_warm_ = false;
+  bool use_graph_ = true, any_warm_ = false, recover_plans_ = false;
+  int plan_iters_ = 0;
+  pdot::WarmPlanArgs wp_{};
   float* warm_x_ = nullptr;
   double *warm_u_ = nullptr, *warm_v_ = nullptr, *warm_r_ = nullptr, *warm_c_ = nullptr;
   int64_t total_x_ = 0, total_units_ = 0, total_panels_ = 0, total_vblocks_ = 0, rows_ = 0, cols_ = 0;

@@ -202,6 +202,37 @@ size_t sqeuclid_workspace_doubles();
 cudaError_t launch_sqeuclid_cost(int64_t m, int64_t n, int dim, const double* xs, const double* ys, int normalise,
                                  double* C, double* work, cudaStream_t s);
 
+// A warm-start plan recovered from warm duals (pdot_warmplan.cu), for one
+// instance or the concatenated instances of the batched solver.
+struct PlanInstance {
+  int64_t m, n, ld;  // rows, columns, leading dimension of the plan (and stored cost)
+  int64_t x_off;     // offset of the plan and of the stored cost (elements)
+  int64_t row_off;   // offset of the row vectors and source points (rows)
+  int64_t col_off;   // offset of the column vectors and target points (columns)
+  int active;        // 1: recover this instance's plan
+  int pad_;
+};
+struct WarmPlanArgs {
+  const PlanInstance* inst;     // num (device)
+  int num;
+  const long long* row_prefix;  // num + 1: instance k owns global rows [row_prefix[k], row_prefix[k+1])
+  const long long* col_prefix;  // num + 1
+  long long total_rows, total_cols;
+  int kind;                     // internal cost kind
+  int dim;                      // point dimension of the coordinate costs
+  const void* C;
+  const float* xs;
+  const float* ys;
+  const DevState* st;           // per instance: cost_scale
+  const double *a, *b, *u0, *v0;
+  double *f, *g;                // balanced potentials (work, total rows / columns)
+  void* X;                      // the plans (FP32 when plan_f32)
+  int plan_f32;
+  double *r, *c;                // their row and column sums
+  double eps;
+};
+cudaError_t launch_warm_plan(const WarmPlanArgs& A, int iterations, cudaStream_t s);
+
 // Sets the thread-local text pdot_last_error() returns (pdot_host.cu).
 void set_last_error(const char* msg);
 

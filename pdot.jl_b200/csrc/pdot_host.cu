@@ -126,6 +126,8 @@ struct Variant {
   const double* warm_u = nullptr;
   const double* warm_v = nullptr;
   const double* warm_x = nullptr;
+  double plan_eps = 0.0;  // > 0: recover the warm plan from the warm duals
+  int plan_iters = 0;
   int staged = 2;  // 0 direct, 1 staged, 2 automatic
 };
 
@@ -165,11 +167,20 @@ Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
   if (o->warm_primal && !o->warm_dual_source)
     fail(PDOT_ERR_INVALID_ARGUMENT, "a warm-start plan needs the warm-start dual vectors");
   v.warm_x = o->warm_primal;
+  if (!(o->warm_plan_epsilon >= 0.0) || !std::isfinite(o->warm_plan_epsilon))
+    fail(PDOT_ERR_INVALID_ARGUMENT, "warm_plan_epsilon must be finite and >= 0");
+  if (o->warm_plan_iterations < 0 || o->warm_plan_iterations > 100000)
+    fail(PDOT_ERR_INVALID_ARGUMENT, "warm_plan_iterations must be 0..100000");
+  if (o->warm_plan_epsilon > 0.0) {
+    if (!o->warm_dual_source) fail(PDOT_ERR_INVALID_ARGUMENT, "a recovered warm plan needs the warm-start duals");
+    if (o->warm_primal) fail(PDOT_ERR_INVALID_ARGUMENT, "give a warm plan or warm_plan_epsilon, not both");
+    v.plan_eps = o->warm_plan_epsilon;
+    v.plan_iters = o->warm_plan_iterations;
+  }
   if (o->primal_pass != PDOT_PASS_AUTO && o->primal_pass != PDOT_PASS_STAGED && o->primal_pass != PDOT_PASS_DIRECT)
     fail(PDOT_ERR_INVALID_ARGUMENT, "unknown primal_pass %d", o->primal_pass);
   v.staged = o->primal_pass == PDOT_PASS_STAGED ? 1 : (o->primal_pass == PDOT_PASS_DIRECT ? 0 : 2);
-  for (int k = 0; k < 4; ++k)
-    if (o->reserved[k] != 0) fail(PDOT_ERR_INVALID_ARGUMENT, "reserved option fields must be zero");
+  if (o->reserved[0] != 0) fail(PDOT_ERR_INVALID_ARGUMENT, "reserved option fields must be zero");
   return v;
 }
 
@@ -298,6 +309,35 @@ class Solver {
       CK(cudaMemcpyAsync(warm_u_, var.warm_u, m * sizeof(double), kind, stream_));
       CK(cudaMemcpyAsync(warm_v_, var.warm_v, n * sizeof(double), kind, stream_));
     }
+    if (var.plan_eps > 0.0) {
+      // recovery of the warm plan from the warm duals (run by reset())
+      plan_eps_ = var.plan_eps;
+      plan_iters_ = var.plan_iters;
+      pdot::PlanInstance pi{};
+      pi.m = m;
+      pi.n = n;
+      pi.ld = m;
+      pi.active = 1;
+      const long long pre[4] = {0, (long long)m, 0, (long long)n};
+      void* p = nullptr;
+      CK(cudaMalloc(&p, sizeof(pi) + sizeof(pre)));
+      allocs_.push_back(p);
+      CK(cudaMemcpy(p, &pi, sizeof(pi), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(static_cast<char*>(p) + sizeof(pi), pre, sizeof(pre), cudaMemcpyHostToDevice));
+      double *f = nullptr, *gg = nullptr;
+      alloc(&f, m);
+      alloc(&gg, n);
+      wp_.inst = static_cast<const pdot::PlanInstance*>(p);
+      wp_.num = 1;
+      wp_.row_prefix = reinterpret_cast<const long long*>(static_cast<char*>(p) + sizeof(pi));
+      wp_.col_prefix = wp_.row_prefix + 2;
+      wp_.total_rows = m;
+      wp_.total_cols = n;
+      wp_.f = f;
+      wp_.g = gg;
+      wp_.eps = plan_eps_;
+      wp_.plan_f32 = var.plan_f32;
+    }
     if (var.warm_x) {
       // the warm plan in plan precision, and its row and column sums
       void* wx = nullptr;
@@ -378,6 +418,18 @@ class Solver {
     B_.ring = ring_;
     B_.ring_cap = kRingCap;
     B_.st = st_;
+    if (plan_eps_ > 0.0) {
+      wp_.kind = pdot::internal_cost_kind(var.cost_kind, var.point_dim);
+      wp_.dim = cost_.dim;
+      wp_.C = cost_.C;
+      wp_.xs = cost_.xs;
+      wp_.ys = cost_.ys;
+      wp_.st = st_;
+      wp_.a = a_;
+      wp_.b = b_;
+      wp_.u0 = warm_u_;
+      wp_.v0 = warm_v_;
+    }
 
     cfg_ = make_config(prm);
     cfg_.cost_scale = var.cost_scale;
@@ -436,6 +488,12 @@ class Solver {
     }
     CK(cudaMemsetAsync(st_, 0, sizeof(pdot::DevState), stream_));
     CK(pdot::launch_init(B_, g_, cfg_, stream_));
+    if (plan_eps_ > 0.0) {
+      wp_.X = X_[0];
+      wp_.r = r_[0];
+      wp_.c = c_[0];
+      CK(pdot::launch_warm_plan(wp_, plan_iters_, stream_));
+    }
     CK(cudaStreamSynchronize(stream_));
     CK(cudaMemcpy(&status_, st_, sizeof(status_), cudaMemcpyDeviceToHost));
     host_it_ = 1;
@@ -691,6 +749,9 @@ class Solver {
   void* warm_x_ = nullptr;
   double* warm_r_ = nullptr;
   double* warm_c_ = nullptr;
+  double plan_eps_ = 0.0;
+  int plan_iters_ = 0;
+  pdot::WarmPlanArgs wp_{};
   void* X_[2] = {};
   size_t xbytes_ = sizeof(double);
   double* u_[2] = {};

@@ -98,7 +98,9 @@ class SolverOptionsC(ct.Structure):
         ("primal_pass", ct.c_int32),
         ("ctas_per_sm", ct.c_int32),
         ("warm_primal", ct.POINTER(ct.c_double)),
-        ("reserved", ct.c_int32 * 4),
+        ("warm_plan_epsilon", ct.c_double),
+        ("warm_plan_iterations", ct.c_int32),
+        ("reserved", ct.c_int32 * 1),
     ]
 
 
@@ -255,6 +257,18 @@ SIGNATURES = {
         ct.c_int,
         [_I64, _I64, _P, _P, _P, _P, _P, _D, _D, _D, _I32, _P, _P, _P, _P, _I64, _P],
     ),
+    "pdot_mlp_create": (ct.c_int, [_I32, _I64, _I64, _I64, _I64, ct.c_uint64, ct.POINTER(_P)]),
+    "pdot_mlp_destroy": (ct.c_int, [_P]),
+    "pdot_mlp_num_parameters": (_I64, [_P]),
+    "pdot_mlp_stream": (_P, [_P]),
+    "pdot_mlp_get_parameters": (ct.c_int, [_P, _P, _I64]),
+    "pdot_mlp_set_parameters": (ct.c_int, [_P, _P, _I64]),
+    "pdot_mlp_get_gradients": (ct.c_int, [_P, _P, _I64]),
+    "pdot_mlp_set_input": (ct.c_int, [_P, _I64, _P, _D, _D]),
+    "pdot_mlp_forward": (ct.c_int, [_P, _P]),
+    "pdot_mlp_backward": (ct.c_int, [_P, _P, ct.POINTER(_D)]),
+    "pdot_mlp_adamw": (ct.c_int, [_P, ct.c_float, ct.c_float, ct.c_float, ct.c_float, ct.c_float]),
+    "pdot_mlp_train_step": (ct.c_int, [_P, _P, ct.c_float, ct.c_float, ct.POINTER(_D)]),
 }
 
 _lib = None

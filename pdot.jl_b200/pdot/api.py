@@ -370,7 +370,7 @@ _COSTS = {"f64": _abi.COST_F64, "f32": _abi.COST_F32, "bf16": _abi.COST_BF16,
 
 def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, precision: str = "f64",
              cost: Optional[str] = None, points=None, cost_scale: Optional[float] = None, warm_start=None,
-             device_pointers: bool = False, primal_pass: str = "auto"):
+             device_pointers: bool = False, primal_pass: str = "auto", recover_plan=None):
     """Build pdot_solver_options. Returns (options, objects to keep alive).
 
     precision  "f64" (the drop-in) or "f32" (mixed precision: FP32 plan)
@@ -380,6 +380,9 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
                device_pointers, (xs_ptr, ys_ptr, d)
     warm_start (u0, v0) initial duals, or (u0, v0, X0) with an initial plan
                (m x n); with device_pointers, (u_ptr, v_ptr[, X_ptr])
+    recover_plan  (eps, rounds): with warm duals and no plan, the plan is
+               recovered from the duals by `rounds` of log-domain balancing
+               of exp((u_i + v_j - C_ij) / eps)
     """
     keep = []
     opts = _abi.SolverOptionsC()
@@ -390,6 +393,9 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
     if cost is None:
         cost = "f64" if precision == "f64" else "f32"
     opts.cost_storage = _COSTS[cost]
+    if recover_plan is not None:
+        opts.warm_plan_epsilon = float(recover_plan[0])
+        opts.warm_plan_iterations = int(recover_plan[1])
     if points is None and cost in ("sqeuclid", "l1"):
         return opts, keep  # coordinates supplied per instance by the batched entry
     opts.primal_pass = {"auto": _abi.PASS_AUTO, "staged": _abi.PASS_STAGED, "direct": _abi.PASS_DIRECT}[primal_pass]
@@ -432,7 +438,8 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
 
 def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device: int = 0,
              use_cuda_graph: bool = True, precision: str = "f64", cost: Optional[str] = None, points=None,
-             cost_scale: Optional[float] = None, warm_start=None, primal_pass: str = "auto") -> SaddlePointOutput:
+             cost_scale: Optional[float] = None, warm_start=None, primal_pass: str = "auto",
+             recover_plan=None) -> SaddlePointOutput:
     """PDOT.optimize, src/solver_gpu.jl:413-720, run by libpdot.so on the GPU.
 
     The keyword options beyond `device` select this implementation's mixed
@@ -443,7 +450,8 @@ def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device
     mp = MarshalledProblem(problem)
     cp = marshal_params(params)
     opts, _keep = _options(device, use_cuda_graph, precision=precision, cost=cost, points=points,
-                           cost_scale=cost_scale, warm_start=warm_start, primal_pass=primal_pass)
+                           cost_scale=cost_scale, warm_start=warm_start, primal_pass=primal_pass,
+                           recover_plan=recover_plan)
     ob = OutputBuffers(mp.m, mp.n, stats_capacity_for(params))
     rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
     _abi.check(lib, rc, "pdot_optimize")
@@ -459,14 +467,16 @@ class Solver:
     def __init__(self, params: PdhgParameters, problem: Optional[OptimalTransportProblem] = None, *,
                  device_problem=None, device: int = 0, use_cuda_graph: bool = True,
                  time_kernels: bool = False, precision: str = "f64", cost: Optional[str] = None,
-                 points=None, cost_scale: Optional[float] = None, warm_start=None, primal_pass: str = "auto"):
+                 points=None, cost_scale: Optional[float] = None, warm_start=None, primal_pass: str = "auto",
+                 recover_plan=None):
         validate(params)
         self._lib = _abi.load()
         self._params = params
         self._cp = marshal_params(params)
         opts, self._keep = _options(device, use_cuda_graph, time_kernels, precision=precision, cost=cost,
                                     points=points, cost_scale=cost_scale, warm_start=warm_start,
-                                    device_pointers=device_problem is not None, primal_pass=primal_pass)
+                                    device_pointers=device_problem is not None, primal_pass=primal_pass,
+                                    recover_plan=recover_plan)
         handle = ct.c_void_p()
         if device_problem is not None:
             m, n, cptr, aptr, bptr = device_problem
@@ -522,7 +532,7 @@ class Solver:
 
 def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", points=None, device: int = 0,
                      use_cuda_graph: bool = True, ctas_per_sm: int = 0, warm_starts=None,
-                     return_primal: bool = True):
+                     return_primal: bool = True, recover_plan=None):
     """Solve many independent instances at once (pdot_optimize_batched).
 
     problems     a list of OptimalTransportProblem (cost_matrix may be None for
@@ -530,6 +540,8 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
     cost         "f32" (each FP64 matrix stored in FP32), "sqeuclid" or "l1"
                  (from `points`, a list of (xs, ys) per instance)
     warm_starts  None, or per instance None / (u0, v0) / (u0, v0, X0)
+    recover_plan (eps, rounds): plans recovered from the warm duals of the
+                 instances given no plan (see _options)
     return_primal  False leaves every primal_solution None (no m x n copies)
     Returns (outputs, seconds): a SaddlePointOutput per instance (its
     iteration_stats holds the final evaluation record) and the device time.
@@ -609,7 +621,7 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
         bp.warm_dual_sources = wu
         bp.warm_dual_targets = wv
         bp.warm_primals = wx
-    opts, _k = _options(device, use_cuda_graph, precision="f32", cost=cost)
+    opts, _k = _options(device, use_cuda_graph, precision="f32", cost=cost, recover_plan=recover_plan)
     if cost != "f32":
         opts.point_dim = dim
     opts.ctas_per_sm = int(ctas_per_sm)

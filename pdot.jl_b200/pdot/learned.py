@@ -1,0 +1,461 @@
+"""The learned warm start (an addition beside the drop-in; the reference has
+none).
+
+A small MLP maps the two marginals of an OT instance on the 32 x 32 grid to
+its optimal dual potentials; the predicted duals, with a plan recovered from
+them by a few rounds of log-domain balancing on the GPU, start plain PDHG,
+which finishes the solve and is the judge of its error. Without a network (or
+when it is not trusted) the solve starts cold.
+
+    instances   a, b = 32 x 32 histograms (mixtures of 1-5 isotropic Gaussians
+                with sigma in [1, 6] px plus a 1e-4 floor, normalised), C the
+                squared grid distance / max, computed on the fly from the grid
+                coordinates (the solver's "sqeuclid" cost)
+    network     2048 -> 1024 -> 1024 -> 2048, GELU, BF16 weights and
+                activations, FP32 accumulation on the tensor cores
+                (pdot_mlp_* in include/pdot.h, csrc/pdot_mlp.cu)
+    features    log(1024 h) / 2 of the concatenated histograms
+    targets     the solver's duals (u, v), shifted so that mean(u) = mean(v),
+                then standardised with one mean and one scale
+    data        solver-generated: batched PDHG solves to relative KKT 1e-4;
+                every solved instance also gives the exact solutions of its
+                15 images under the symmetries of the grid cost (the 8
+                isometries of the square, each with or without exchanging
+                source and target), which carry the duals along
+
+Device memory for the network's inputs and targets is held by torch (the
+plumbing); every network computation is a pdot_mlp_* kernel.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import math
+import time
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _abi, api, instances
+
+SIDE = 32
+BINS = SIDE * SIDE
+FEATURE_SHIFT = math.log(BINS)
+FEATURE_SCALE = 0.5
+RECOVER_PLAN = (3e-4, 100)  # (eps, rounds) of the plan recovered from predicted duals
+
+
+def grid_points(side: int = SIDE) -> np.ndarray:
+    yy, xx = np.mgrid[0:side, 0:side]
+    return np.stack([xx.ravel(), yy.ravel()], axis=1).astype(np.float32)
+
+
+def grid_pair(seed: int, side: int = SIDE):
+    """The marginals of instance `seed` (source, target)."""
+    rng = np.random.default_rng(seed)
+    return instances.grid_histogram(rng, side), instances.grid_histogram(rng, side)
+
+
+def canonical_duals(u: np.ndarray, v: np.ndarray):
+    """Shift (u + t, v - t) so that mean(u) = mean(v); the shift keeps u_i + v_j."""
+    t = 0.5 * (np.mean(v) - np.mean(u))
+    return u + t, v - t
+
+
+def grid_symmetries(side: int = SIDE):
+    """Index maps p of the 8 isometries of the square grid: (h o p) is the
+    image of histogram h. The squared grid distance is invariant under each."""
+    idx = np.arange(side * side).reshape(side, side)
+    maps = []
+    for k in range(4):
+        r = np.rot90(idx, k)
+        maps.append(r.ravel().copy())
+        maps.append(r.T.ravel().copy())
+    return maps
+
+
+def augment(a, b, u, v, side: int = SIDE):
+    """The 16 images of a solved instance: (a[p], b[p]) has duals (u[p], v[p])
+    for every isometry p, and (b, a) has duals (v, u) since C is symmetric."""
+    out = []
+    for p in grid_symmetries(side):
+        out.append((a[p], b[p], u[p], v[p]))
+        out.append((b[p], a[p], v[p], u[p]))
+    return out
+
+
+def solve_grid_batch(seeds, params: api.PdhgParameters, *, device: int = 0, warm_starts=None,
+                     recover_plan=None):
+    """Solve the grid instances of `seeds` in one batched launch with the
+    on-the-fly squared-Euclidean cost. Returns (outputs, device seconds)."""
+    pts = grid_points()
+    probs = []
+    for s in seeds:
+        a, b = grid_pair(int(s))
+        probs.append(api.OptimalTransportProblem(None, a, b))
+    return api.optimize_batched(params, probs, cost="sqeuclid", points=[(pts, pts)] * len(probs), device=device,
+                                warm_starts=warm_starts, return_primal=False, recover_plan=recover_plan)
+
+
+def generate(seeds, params: api.PdhgParameters, *, batch: int = 256, device: int = 0, log=print):
+    """Solver-generated training pairs: for each seed its canonical duals,
+    iteration count and termination reason."""
+    seeds = list(seeds)
+    U = np.zeros((len(seeds), BINS))
+    V = np.zeros((len(seeds), BINS))
+    its = np.zeros(len(seeds), dtype=np.int64)
+    reasons = np.zeros(len(seeds), dtype=np.int64)
+    total = 0.0
+    for k0 in range(0, len(seeds), batch):
+        chunk = seeds[k0 : k0 + batch]
+        outs, sec = solve_grid_batch(chunk, params, device=device)
+        total += sec
+        for k, o in enumerate(outs):
+            U[k0 + k], V[k0 + k] = canonical_duals(o.dual_source_solution, o.dual_target_solution)
+            its[k0 + k] = o.iteration_count
+            reasons[k0 + k] = int(o.termination_reason)
+        if log:
+            log(f"generate: {k0 + len(chunk)}/{len(seeds)} solved, {sec:.1f} s device, "
+                f"mean iterations {its[k0:k0 + len(chunk)].mean():.0f}")
+    return {"seeds": np.asarray(seeds), "u": U, "v": V, "iterations": its, "reasons": reasons,
+            "seconds": total}
+
+
+class MLP:
+    """pdot_mlp: the network on one GPU (weights, moments, activations)."""
+
+    def __init__(self, input_dim: int = 2 * BINS, hidden_dim: int = 1024, output_dim: int = 2 * BINS,
+                 max_batch: int = 256, seed: int = 0, device: int = 0):
+        self._lib = _abi.load()
+        h = ct.c_void_p()
+        rc = self._lib.pdot_mlp_create(device, input_dim, hidden_dim, output_dim, max_batch, seed, ct.byref(h))
+        _abi.check(self._lib, rc, "pdot_mlp_create")
+        self._h = h
+        self.dims = (input_dim, hidden_dim, output_dim)
+        self.max_batch = max_batch
+        self.device = device
+        self.num_parameters = int(self._lib.pdot_mlp_num_parameters(h))
+
+    def close(self):
+        if self._h:
+            self._lib.pdot_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream_handle(self) -> int:
+        return int(self._lib.pdot_mlp_stream(self._h) or 0)
+
+    def get_parameters(self) -> np.ndarray:
+        p = np.zeros(self.num_parameters, dtype=np.float32)
+        _abi.check(self._lib, self._lib.pdot_mlp_get_parameters(self._h, p.ctypes.data, p.size), "get_parameters")
+        return p
+
+    def set_parameters(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != self.num_parameters:
+            raise ValueError(f"{p.size} parameters given, {self.num_parameters} expected")
+        _abi.check(self._lib, self._lib.pdot_mlp_set_parameters(self._h, p.ctypes.data, p.size), "set_parameters")
+
+    def gradients(self) -> np.ndarray:
+        g = np.zeros(self.num_parameters, dtype=np.float32)
+        _abi.check(self._lib, self._lib.pdot_mlp_get_gradients(self._h, g.ctypes.data, g.size), "get_gradients")
+        return g
+
+    def set_input(self, hist_ptr: int, batch: int, shift: float = FEATURE_SHIFT, scale: float = FEATURE_SCALE):
+        """hist_ptr: device FP64 [batch x input_dim] (row-major)."""
+        _abi.check(self._lib, self._lib.pdot_mlp_set_input(self._h, batch, hist_ptr, shift, scale), "set_input")
+
+    def forward(self, out_ptr: Optional[int] = None):
+        _abi.check(self._lib, self._lib.pdot_mlp_forward(self._h, out_ptr), "forward")
+
+    def backward(self, target_ptr: int) -> float:
+        loss = ct.c_double(0.0)
+        _abi.check(self._lib, self._lib.pdot_mlp_backward(self._h, target_ptr, ct.byref(loss)), "backward")
+        return loss.value
+
+    def adamw(self, lr: float, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8,
+              weight_decay: float = 0.0):
+        _abi.check(self._lib, self._lib.pdot_mlp_adamw(self._h, lr, beta1, beta2, eps, weight_decay), "adamw")
+
+    def train_step(self, target_ptr: int, lr: float, weight_decay: float, want_loss: bool) -> float:
+        loss = ct.c_double(float("nan"))
+        rc = self._lib.pdot_mlp_train_step(self._h, target_ptr, lr, weight_decay,
+                                           ct.byref(loss) if want_loss else None)
+        _abi.check(self._lib, rc, "train_step")
+        return loss.value
+
+
+@dataclass
+class WarmStartModel:
+    """A trained network with the target standardisation."""
+
+    parameters: np.ndarray  # FP32 (the BF16 weights and FP32 biases widened)
+    target_mean: float
+    target_scale: float
+    hidden_dim: int = 1024
+
+    def save(self, path: str):
+        I, H, O = 2 * BINS, self.hidden_dim, 2 * BINS
+        p = self.parameters
+        sizes = [H * I, H, H * H, H, O * H, O]
+        parts, off = [], 0
+        for s in sizes:
+            parts.append(p[off : off + s])
+            off += s
+        w = [parts[0], parts[2], parts[4]]
+        wbits = [np.ascontiguousarray(x, dtype=np.float32).view(np.uint32) for x in w]
+        # the weights are stored as their BF16 bits (what the kernels use)
+        np.savez(path, W1=_bf16_bits(wbits[0]), W2=_bf16_bits(wbits[1]), W3=_bf16_bits(wbits[2]), b1=parts[1],
+                 b2=parts[3], b3=parts[5], target_mean=self.target_mean, target_scale=self.target_scale,
+                 hidden_dim=self.hidden_dim)
+
+    @staticmethod
+    def load(path: str) -> "WarmStartModel":
+        z = np.load(path)
+        f = [_bf16_to_f32(z["W1"]), z["b1"], _bf16_to_f32(z["W2"]), z["b2"], _bf16_to_f32(z["W3"]), z["b3"]]
+        return WarmStartModel(np.concatenate([np.asarray(x, dtype=np.float32).ravel() for x in f]),
+                              float(z["target_mean"]), float(z["target_scale"]), int(z["hidden_dim"]))
+
+
+def _bf16_bits(u32: np.ndarray) -> np.ndarray:
+    u = u32.astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
+    return u.astype(np.uint16)
+
+
+def _bf16_to_f32(b: np.ndarray) -> np.ndarray:
+    return (np.asarray(b, dtype=np.uint32) << 16).view(np.float32)
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def train(mlp: MLP, hist: np.ndarray, targets: np.ndarray, *, epochs: int = 60, batch: int = 256,
+          lr: float = 1e-3, weight_decay: float = 1e-4, seed: int = 0, log=print):
+    """Train on (hist [N x 2048] FP64, targets [N x 2048] standardised) with
+    AdamW and a cosine learning-rate schedule; batches are drawn without
+    replacement each epoch (the last partial batch is dropped). Returns the
+    mean loss of every epoch."""
+    torch = _torch()
+    dev = torch.device("cuda", mlp.device)
+    H = torch.from_numpy(np.ascontiguousarray(hist, dtype=np.float64)).to(dev)
+    T = torch.from_numpy(np.ascontiguousarray(targets, dtype=np.float32)).to(dev)
+    n = H.shape[0]
+    steps_per_epoch = n // batch
+    total = epochs * steps_per_epoch
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    losses = []
+    step = 0
+    for ep in range(epochs):
+        perm = torch.randperm(n, generator=g).to(dev)
+        Hs = H.index_select(0, perm).contiguous()
+        Ts = T.index_select(0, perm).contiguous()
+        torch.cuda.synchronize(dev)
+        acc = 0.0
+        for k in range(steps_per_epoch):
+            lr_k = lr * 0.5 * (1.0 + math.cos(math.pi * step / max(total, 1)))
+            mlp.set_input(Hs[k * batch:(k + 1) * batch].data_ptr(), batch)
+            want = (k == steps_per_epoch - 1) or (k % 16 == 0)
+            loss = mlp.train_step(Ts[k * batch:(k + 1) * batch].data_ptr(), lr_k, weight_decay, want)
+            if want:
+                acc = loss if k == 0 else acc
+                losses.append((ep, k, loss))
+            step += 1
+        if log:
+            log(f"train: epoch {ep + 1}/{epochs} loss {losses[-1][2]:.5f}")
+    return losses
+
+
+def predict(mlp: MLP, model: WarmStartModel, a_rows: np.ndarray, b_rows: np.ndarray):
+    """Predicted canonical duals (u, v) for instances given row-wise."""
+    torch = _torch()
+    dev = torch.device("cuda", mlp.device)
+    hist = np.concatenate([a_rows, b_rows], axis=1)
+    n = hist.shape[0]
+    out = np.zeros((n, 2 * BINS), dtype=np.float32)
+    Y = torch.zeros((mlp.max_batch, 2 * BINS), dtype=torch.float32, device=dev)
+    for k0 in range(0, n, mlp.max_batch):
+        h = torch.from_numpy(np.ascontiguousarray(hist[k0 : k0 + mlp.max_batch])).to(dev)
+        torch.cuda.synchronize(dev)
+        mlp.set_input(h.data_ptr(), h.shape[0])
+        mlp.forward(Y.data_ptr())
+        out[k0 : k0 + h.shape[0]] = Y[: h.shape[0]].cpu().numpy()
+    duals = out.astype(np.float64) * model.target_scale + model.target_mean
+    return duals[:, :BINS], duals[:, BINS:]
+
+
+def dataset(data: dict, augment_symmetries: bool = True):
+    """(hist [N x 2048], duals [N x 2048]) of generated data, with the 16
+    images of every instance when `augment_symmetries`."""
+    A, D = [], []
+    for k, s in enumerate(data["seeds"]):
+        if data["reasons"][k] != int(api.TerminationReason.TERMINATION_REASON_OPTIMAL):
+            continue
+        a, b = grid_pair(int(s))
+        u, v = data["u"][k], data["v"][k]
+        imgs = augment(a, b, u, v) if augment_symmetries else [(a, b, u, v)]
+        for (aa, bb, uu, vv) in imgs:
+            A.append(np.concatenate([aa, bb]))
+            D.append(np.concatenate([uu, vv]))
+    return np.asarray(A), np.asarray(D)
+
+
+def evaluate(mlp: MLP, model: WarmStartModel, seeds, params: api.PdhgParameters, *, batch: int = 256,
+             device: int = 0, cold: Optional[dict] = None, log=print):
+    """Cold and learned-warm batched solves of the held-out `seeds`:
+    iterations, device seconds, and the network's time (inference)."""
+    seeds = list(seeds)
+    res = {"cold_iterations": [], "warm_iterations": [], "cold_seconds": 0.0, "warm_seconds": 0.0,
+           "predict_seconds": 0.0, "cold_reasons": [], "warm_reasons": [], "dual_rel_error": []}
+    for k0 in range(0, len(seeds), batch):
+        chunk = seeds[k0 : k0 + batch]
+        ab = [grid_pair(int(s)) for s in chunk]
+        t0 = time.perf_counter()
+        u, v = predict(mlp, model, np.asarray([x[0] for x in ab]), np.asarray([x[1] for x in ab]))
+        res["predict_seconds"] += time.perf_counter() - t0
+        warm = [(u[k], v[k]) for k in range(len(chunk))]
+        outs_w, sec_w = solve_grid_batch(chunk, params, device=device, warm_starts=warm, recover_plan=RECOVER_PLAN)
+        res["warm_seconds"] += sec_w
+        res["warm_iterations"] += [o.iteration_count for o in outs_w]
+        res["warm_reasons"] += [int(o.termination_reason) for o in outs_w]
+        if cold is None:
+            outs_c, sec_c = solve_grid_batch(chunk, params, device=device)
+            res["cold_seconds"] += sec_c
+            res["cold_iterations"] += [o.iteration_count for o in outs_c]
+            res["cold_reasons"] += [int(o.termination_reason) for o in outs_c]
+            for k, o in enumerate(outs_c):
+                uc, vc = canonical_duals(o.dual_source_solution, o.dual_target_solution)
+                ref = np.concatenate([uc, vc])
+                res["dual_rel_error"].append(float(np.linalg.norm(np.concatenate([u[k], v[k]]) - ref)
+                                                   / np.linalg.norm(ref - ref.mean())))
+        if log:
+            log(f"evaluate: {k0 + len(chunk)}/{len(seeds)}: warm {np.mean(res['warm_iterations']):.0f} it, "
+                f"cold {np.mean(res['cold_iterations']) if res['cold_iterations'] else float('nan'):.0f} it")
+    return res
+
+
+# ------------------------------------------------------------------ command line
+# python -m pdot.learned generate --first SEED --count N --out data.npz
+# python -m pdot.learned train --data a.npz [b.npz ...] --model model.npz
+# python -m pdot.learned evaluate --model model.npz --first SEED --count N --out eval.json
+TRAIN_SEED0 = 1_000_000   # training instances: seeds TRAIN_SEED0 + k
+HELDOUT_SEED0 = 9_000_000  # held-out instances: seeds HELDOUT_SEED0 + k
+
+
+def _params(tol: float = 1e-4, iteration_limit: int = 400_000):
+    from .solve import default_parameters
+
+    return default_parameters(tol, iteration_limit=iteration_limit)
+
+
+def _cmd_generate(args):
+    seeds = list(range(args.first, args.first + args.count))
+    data = generate(seeds, _params(iteration_limit=args.iteration_limit), batch=args.batch)
+    np.savez(args.out, seeds=data["seeds"], u=data["u"].astype(np.float32), v=data["v"].astype(np.float32),
+             iterations=data["iterations"], reasons=data["reasons"], seconds=data["seconds"])
+    print(f"generate: {len(seeds)} instances in {data['seconds']:.1f} s device; "
+          f"optimal {int(np.sum(data['reasons'] == 1))}; mean iterations {data['iterations'].mean():.0f}")
+
+
+def _load_data(paths):
+    parts = [np.load(p) for p in paths]
+    return {k: np.concatenate([z[k] for z in parts]) if np.ndim(parts[0][k]) else float(sum(z[k] for z in parts))
+            for k in ("seeds", "u", "v", "iterations", "reasons", "seconds")}
+
+
+def _cmd_train(args):
+    data = _load_data(args.data)
+    data["u"] = data["u"].astype(np.float64)
+    data["v"] = data["v"].astype(np.float64)
+    hist, duals = dataset(data, augment_symmetries=not args.no_augment)
+    mean, scale = float(duals.mean()), float(duals.std())
+    targets = ((duals - mean) / scale).astype(np.float32)
+    print(f"train: {hist.shape[0]} pairs from {len(data['seeds'])} solved instances; target mean {mean:.4f} "
+          f"scale {scale:.4f}")
+    mlp = MLP(max_batch=args.batch, seed=args.seed)
+    t0 = time.perf_counter()
+    losses = train(mlp, hist, targets, epochs=args.epochs, batch=args.batch, lr=args.lr,
+                   weight_decay=args.weight_decay, seed=args.seed)
+    secs = time.perf_counter() - t0
+    model = WarmStartModel(mlp.get_parameters(), mean, scale, hidden_dim=mlp.dims[1])
+    model.save(args.model)
+    print(f"train: {args.epochs} epochs in {secs:.1f} s; final loss {losses[-1][2]:.5f}")
+    if args.log:
+        import json
+
+        with open(args.log, "w") as f:
+            json.dump({"pairs": int(hist.shape[0]), "instances": int(len(data["seeds"])), "epochs": args.epochs,
+                       "batch": args.batch, "lr": args.lr, "seconds": secs, "target_mean": mean,
+                       "target_scale": scale, "losses": losses}, f)
+
+
+def _cmd_evaluate(args):
+    import json
+
+    model = WarmStartModel.load(args.model)
+    mlp = MLP(hidden_dim=model.hidden_dim, max_batch=args.batch)
+    mlp.set_parameters(model.parameters)
+    seeds = list(range(args.first, args.first + args.count))
+    res = evaluate(mlp, model, seeds, _params(iteration_limit=args.iteration_limit), batch=args.batch)
+    cold = np.asarray(res["cold_iterations"], dtype=float)
+    warm = np.asarray(res["warm_iterations"], dtype=float)
+    summary = {
+        "instances": len(seeds),
+        "cold_mean_iterations": float(cold.mean()), "warm_mean_iterations": float(warm.mean()),
+        "cold_median_iterations": float(np.median(cold)), "warm_median_iterations": float(np.median(warm)),
+        "warm_better_fraction": float(np.mean(warm < cold)),
+        "cold_seconds": res["cold_seconds"], "warm_seconds": res["warm_seconds"],
+        "predict_seconds": res["predict_seconds"],
+        "cold_optimal": int(sum(1 for r in res["cold_reasons"] if r == 1)),
+        "warm_optimal": int(sum(1 for r in res["warm_reasons"] if r == 1)),
+        "dual_rel_error_median": float(np.median(res["dual_rel_error"])),
+    }
+    print(json.dumps(summary, indent=1))
+    if args.out:
+        with open(args.out, "w") as f:
+            json.dump({"summary": summary, "per_instance": {k: v for k, v in res.items()}}, f)
+
+
+def main(argv=None):
+    import argparse
+
+    ap = argparse.ArgumentParser(prog="python -m pdot.learned")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    g = sub.add_parser("generate")
+    g.add_argument("--first", type=int, default=TRAIN_SEED0)
+    g.add_argument("--count", type=int, default=256)
+    g.add_argument("--batch", type=int, default=512)
+    g.add_argument("--iteration-limit", type=int, default=400_000)
+    g.add_argument("--out", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--data", nargs="+", required=True)
+    t.add_argument("--model", required=True)
+    t.add_argument("--epochs", type=int, default=60)
+    t.add_argument("--batch", type=int, default=256)
+    t.add_argument("--lr", type=float, default=1e-3)
+    t.add_argument("--weight-decay", type=float, default=1e-4)
+    t.add_argument("--seed", type=int, default=0)
+    t.add_argument("--no-augment", action="store_true")
+    t.add_argument("--log")
+    e = sub.add_parser("evaluate")
+    e.add_argument("--model", required=True)
+    e.add_argument("--first", type=int, default=HELDOUT_SEED0)
+    e.add_argument("--count", type=int, default=1024)
+    e.add_argument("--batch", type=int, default=256)
+    e.add_argument("--iteration-limit", type=int, default=400_000)
+    e.add_argument("--out")
+    args = ap.parse_args(argv)
+    {"generate": _cmd_generate, "train": _cmd_train, "evaluate": _cmd_evaluate}[args.cmd](args)
+
+
+if __name__ == "__main__":
+    main()

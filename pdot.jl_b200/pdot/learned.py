@@ -15,8 +15,10 @@ when it is not trusted) the solve starts cold.
                 activations, FP32 accumulation on the tensor cores
                 (pdot_mlp_* in include/pdot.h, csrc/pdot_mlp.cu)
     features    log(1024 h) / 2 of the concatenated histograms
-    targets     the solver's duals (u, v), shifted so that mean(u) = mean(v),
-                then standardised with one mean and one scale
+    targets     the solver's duals (u, v) made tight by a double c-transform
+                (rows and columns of tiny mass leave PDHG's duals loose),
+                shifted so that mean(u) = mean(v), then standardised with one
+                mean and one scale
     data        solver-generated: batched PDHG solves to relative KKT 1e-4;
                 every solved instance also gives the exact solutions of its
                 15 images under the symmetries of the grid cost (the 8
@@ -60,6 +62,25 @@ def canonical_duals(u: np.ndarray, v: np.ndarray):
     """Shift (u + t, v - t) so that mean(u) = mean(v); the shift keeps u_i + v_j."""
     t = 0.5 * (np.mean(v) - np.mean(u))
     return u + t, v - t
+
+
+_GRID_COST = {}
+
+
+def grid_cost(side: int = SIDE) -> np.ndarray:
+    if side not in _GRID_COST:
+        _GRID_COST[side] = instances.grid_cost(side)
+    return _GRID_COST[side]
+
+
+def tight_duals(u: np.ndarray, v: np.ndarray, C: np.ndarray):
+    """The double c-transform u' = min_j (C_ij - v_j), v' = min_i (C_ij - u'_i):
+    a feasible dual pair, each the c-transform of the other, in which the
+    values PDHG leaves loose (rows and columns of tiny mass, whose constraints
+    never bind) are made tight; then the canonical shift."""
+    u1 = np.min(C - np.asarray(v, dtype=np.float64)[None, :], axis=1)
+    v1 = np.min(C - u1[:, None], axis=0)
+    return canonical_duals(u1, v1)
 
 
 def grid_symmetries(side: int = SIDE):
@@ -239,12 +260,29 @@ def _torch():
     return torch
 
 
+def forward_rows(mlp: MLP, hist: np.ndarray) -> np.ndarray:
+    """The network's outputs for the rows of hist [N x input_dim] (FP64)."""
+    torch = _torch()
+    dev = torch.device("cuda", mlp.device)
+    n = hist.shape[0]
+    out = np.zeros((n, mlp.dims[2]), dtype=np.float32)
+    Y = torch.zeros((mlp.max_batch, mlp.dims[2]), dtype=torch.float32, device=dev)
+    for k0 in range(0, n, mlp.max_batch):
+        h = torch.from_numpy(np.ascontiguousarray(hist[k0 : k0 + mlp.max_batch], dtype=np.float64)).to(dev)
+        torch.cuda.synchronize(dev)
+        mlp.set_input(h.data_ptr(), h.shape[0])
+        mlp.forward(Y.data_ptr())
+        out[k0 : k0 + h.shape[0]] = Y[: h.shape[0]].cpu().numpy()
+    return out
+
+
 def train(mlp: MLP, hist: np.ndarray, targets: np.ndarray, *, epochs: int = 60, batch: int = 256,
-          lr: float = 1e-3, weight_decay: float = 1e-4, seed: int = 0, log=print):
+          lr: float = 1e-3, weight_decay: float = 1e-4, seed: int = 0, validation=None, log=print):
     """Train on (hist [N x 2048] FP64, targets [N x 2048] standardised) with
     AdamW and a cosine learning-rate schedule; batches are drawn without
-    replacement each epoch (the last partial batch is dropped). Returns the
-    mean loss of every epoch."""
+    replacement each epoch (the last partial batch is dropped). `validation`
+    = (hist, targets) of instances kept out of training, scored after every
+    epoch. Returns (training losses (epoch, step, loss), validation losses)."""
     torch = _torch()
     dev = torch.device("cuda", mlp.device)
     H = torch.from_numpy(np.ascontiguousarray(hist, dtype=np.float64)).to(dev)
@@ -253,7 +291,7 @@ def train(mlp: MLP, hist: np.ndarray, targets: np.ndarray, *, epochs: int = 60, 
     steps_per_epoch = n // batch
     total = epochs * steps_per_epoch
     g = torch.Generator(device="cpu").manual_seed(seed)
-    losses = []
+    losses, val = [], []
     step = 0
     for ep in range(epochs):
         perm = torch.randperm(n, generator=g).to(dev)
@@ -270,25 +308,18 @@ def train(mlp: MLP, hist: np.ndarray, targets: np.ndarray, *, epochs: int = 60, 
                 acc = loss if k == 0 else acc
                 losses.append((ep, k, loss))
             step += 1
+        if validation is not None:
+            pred = forward_rows(mlp, validation[0])
+            val.append(float(np.mean((pred.astype(np.float64) - validation[1]) ** 2)))
         if log:
-            log(f"train: epoch {ep + 1}/{epochs} loss {losses[-1][2]:.5f}")
-    return losses
+            log(f"train: epoch {ep + 1}/{epochs} loss {losses[-1][2]:.5f}"
+                + (f" validation {val[-1]:.5f}" if val else ""))
+    return losses, val
 
 
 def predict(mlp: MLP, model: WarmStartModel, a_rows: np.ndarray, b_rows: np.ndarray):
     """Predicted canonical duals (u, v) for instances given row-wise."""
-    torch = _torch()
-    dev = torch.device("cuda", mlp.device)
-    hist = np.concatenate([a_rows, b_rows], axis=1)
-    n = hist.shape[0]
-    out = np.zeros((n, 2 * BINS), dtype=np.float32)
-    Y = torch.zeros((mlp.max_batch, 2 * BINS), dtype=torch.float32, device=dev)
-    for k0 in range(0, n, mlp.max_batch):
-        h = torch.from_numpy(np.ascontiguousarray(hist[k0 : k0 + mlp.max_batch])).to(dev)
-        torch.cuda.synchronize(dev)
-        mlp.set_input(h.data_ptr(), h.shape[0])
-        mlp.forward(Y.data_ptr())
-        out[k0 : k0 + h.shape[0]] = Y[: h.shape[0]].cpu().numpy()
+    out = forward_rows(mlp, np.concatenate([a_rows, b_rows], axis=1))
     duals = out.astype(np.float64) * model.target_scale + model.target_mean
     return duals[:, :BINS], duals[:, BINS:]
 
@@ -297,11 +328,12 @@ def dataset(data: dict, augment_symmetries: bool = True):
     """(hist [N x 2048], duals [N x 2048]) of generated data, with the 16
     images of every instance when `augment_symmetries`."""
     A, D = [], []
+    C = grid_cost()
     for k, s in enumerate(data["seeds"]):
         if data["reasons"][k] != int(api.TerminationReason.TERMINATION_REASON_OPTIMAL):
             continue
         a, b = grid_pair(int(s))
-        u, v = data["u"][k], data["v"][k]
+        u, v = tight_duals(data["u"][k], data["v"][k], C)
         imgs = augment(a, b, u, v) if augment_symmetries else [(a, b, u, v)]
         for (aa, bb, uu, vv) in imgs:
             A.append(np.concatenate([aa, bb]))
@@ -310,10 +342,16 @@ def dataset(data: dict, augment_symmetries: bool = True):
 
 
 def evaluate(mlp: MLP, model: WarmStartModel, seeds, params: api.PdhgParameters, *, batch: int = 256,
-             device: int = 0, cold: Optional[dict] = None, log=print):
+             device: int = 0, cold: Optional[dict] = None, recover_plan=RECOVER_PLAN, tighten: bool = False,
+             log=print):
     """Cold and learned-warm batched solves of the held-out `seeds`:
-    iterations, device seconds, and the network's time (inference)."""
+    iterations, device seconds, and the network's time (inference). `cold`,
+    when given, holds the cold solves already made (generate()'s output for
+    the same seeds, solved in chunks of the same `batch`). `tighten` replaces
+    the predicted duals by their double c-transform (on the host) before the
+    warm start."""
     seeds = list(seeds)
+    C = grid_cost()
     res = {"cold_iterations": [], "warm_iterations": [], "cold_seconds": 0.0, "warm_seconds": 0.0,
            "predict_seconds": 0.0, "cold_reasons": [], "warm_reasons": [], "dual_rel_error": []}
     for k0 in range(0, len(seeds), batch):
@@ -322,8 +360,11 @@ def evaluate(mlp: MLP, model: WarmStartModel, seeds, params: api.PdhgParameters,
         t0 = time.perf_counter()
         u, v = predict(mlp, model, np.asarray([x[0] for x in ab]), np.asarray([x[1] for x in ab]))
         res["predict_seconds"] += time.perf_counter() - t0
+        if tighten:
+            for k in range(len(chunk)):
+                u[k], v[k] = tight_duals(u[k], v[k], C)
         warm = [(u[k], v[k]) for k in range(len(chunk))]
-        outs_w, sec_w = solve_grid_batch(chunk, params, device=device, warm_starts=warm, recover_plan=RECOVER_PLAN)
+        outs_w, sec_w = solve_grid_batch(chunk, params, device=device, warm_starts=warm, recover_plan=recover_plan)
         res["warm_seconds"] += sec_w
         res["warm_iterations"] += [o.iteration_count for o in outs_w]
         res["warm_reasons"] += [int(o.termination_reason) for o in outs_w]
@@ -332,15 +373,38 @@ def evaluate(mlp: MLP, model: WarmStartModel, seeds, params: api.PdhgParameters,
             res["cold_seconds"] += sec_c
             res["cold_iterations"] += [o.iteration_count for o in outs_c]
             res["cold_reasons"] += [int(o.termination_reason) for o in outs_c]
-            for k, o in enumerate(outs_c):
-                uc, vc = canonical_duals(o.dual_source_solution, o.dual_target_solution)
-                ref = np.concatenate([uc, vc])
-                res["dual_rel_error"].append(float(np.linalg.norm(np.concatenate([u[k], v[k]]) - ref)
-                                                   / np.linalg.norm(ref - ref.mean())))
+            cold_duals = [(o.dual_source_solution, o.dual_target_solution) for o in outs_c]
+        else:
+            sel = slice(k0, k0 + len(chunk))
+            res["cold_iterations"] += [int(x) for x in cold["iterations"][sel]]
+            res["cold_reasons"] += [int(x) for x in cold["reasons"][sel]]
+            cold_duals = list(zip(np.asarray(cold["u"][sel], dtype=np.float64),
+                                  np.asarray(cold["v"][sel], dtype=np.float64)))
+        for k, (uc, vc) in enumerate(cold_duals):
+            ref = np.concatenate(tight_duals(uc, vc, C))
+            res["dual_rel_error"].append(float(np.linalg.norm(np.concatenate([u[k], v[k]]) - ref)
+                                               / np.linalg.norm(ref - ref.mean())))
         if log:
             log(f"evaluate: {k0 + len(chunk)}/{len(seeds)}: warm {np.mean(res['warm_iterations']):.0f} it, "
-                f"cold {np.mean(res['cold_iterations']) if res['cold_iterations'] else float('nan'):.0f} it")
+                f"cold {np.mean(res['cold_iterations']):.0f} it")
     return res
+
+
+def summarize(res: dict) -> dict:
+    cold = np.asarray(res["cold_iterations"], dtype=float)
+    warm = np.asarray(res["warm_iterations"], dtype=float)
+    return {
+        "instances": int(cold.size),
+        "cold_mean_iterations": float(cold.mean()), "warm_mean_iterations": float(warm.mean()),
+        "cold_median_iterations": float(np.median(cold)), "warm_median_iterations": float(np.median(warm)),
+        "cold_p90_iterations": float(np.percentile(cold, 90)), "warm_p90_iterations": float(np.percentile(warm, 90)),
+        "warm_better_fraction": float(np.mean(warm < cold)),
+        "cold_seconds": float(res["cold_seconds"]), "warm_seconds": float(res["warm_seconds"]),
+        "predict_seconds": float(res["predict_seconds"]),
+        "cold_optimal": int(sum(1 for r in res["cold_reasons"] if r == 1)),
+        "warm_optimal": int(sum(1 for r in res["warm_reasons"] if r == 1)),
+        "dual_rel_error_median": float(np.median(res["dual_rel_error"])),
+    }
 
 
 # ------------------------------------------------------------------ command line
@@ -373,56 +437,63 @@ def _load_data(paths):
 
 
 def _cmd_train(args):
+    import json
+
     data = _load_data(args.data)
     data["u"] = data["u"].astype(np.float64)
     data["v"] = data["v"].astype(np.float64)
-    hist, duals = dataset(data, augment_symmetries=not args.no_augment)
+    nval = int(args.val_instances)
+    keep = len(data["seeds"]) - nval
+    tr = {k: (v[:keep] if np.ndim(v) else v) for k, v in data.items()}
+    va = {k: (v[keep:] if np.ndim(v) else v) for k, v in data.items()}
+    hist, duals = dataset(tr, augment_symmetries=not args.no_augment)
     mean, scale = float(duals.mean()), float(duals.std())
     targets = ((duals - mean) / scale).astype(np.float32)
-    print(f"train: {hist.shape[0]} pairs from {len(data['seeds'])} solved instances; target mean {mean:.4f} "
-          f"scale {scale:.4f}")
+    validation = None
+    if nval > 0:
+        vh, vd = dataset(va, augment_symmetries=False)
+        validation = (vh, (vd - mean) / scale)
+    print(f"train: {hist.shape[0]} pairs from {keep} solved instances ({nval} kept for validation); "
+          f"target mean {mean:.4f} scale {scale:.4f}")
     mlp = MLP(max_batch=args.batch, seed=args.seed)
     t0 = time.perf_counter()
-    losses = train(mlp, hist, targets, epochs=args.epochs, batch=args.batch, lr=args.lr,
-                   weight_decay=args.weight_decay, seed=args.seed)
+    losses, val = train(mlp, hist, targets, epochs=args.epochs, batch=args.batch, lr=args.lr,
+                        weight_decay=args.weight_decay, seed=args.seed, validation=validation)
     secs = time.perf_counter() - t0
     model = WarmStartModel(mlp.get_parameters(), mean, scale, hidden_dim=mlp.dims[1])
     model.save(args.model)
-    print(f"train: {args.epochs} epochs in {secs:.1f} s; final loss {losses[-1][2]:.5f}")
+    print(f"train: {args.epochs} epochs in {secs:.1f} s; final loss {losses[-1][2]:.5f}"
+          + (f", validation {val[-1]:.5f}" if val else ""))
     if args.log:
-        import json
-
         with open(args.log, "w") as f:
-            json.dump({"pairs": int(hist.shape[0]), "instances": int(len(data["seeds"])), "epochs": args.epochs,
-                       "batch": args.batch, "lr": args.lr, "seconds": secs, "target_mean": mean,
-                       "target_scale": scale, "losses": losses}, f)
+            json.dump({"pairs": int(hist.shape[0]), "instances": keep, "validation_instances": nval,
+                       "epochs": args.epochs, "batch": args.batch, "lr": args.lr, "weight_decay": args.weight_decay,
+                       "seconds": secs, "target_mean": mean, "target_scale": scale, "losses": losses,
+                       "validation": val}, f)
 
 
 def _cmd_evaluate(args):
     import json
 
     model = WarmStartModel.load(args.model)
-    mlp = MLP(hidden_dim=model.hidden_dim, max_batch=args.batch)
+    mlp = MLP(hidden_dim=model.hidden_dim, max_batch=min(args.batch, 1024))
     mlp.set_parameters(model.parameters)
     seeds = list(range(args.first, args.first + args.count))
-    res = evaluate(mlp, model, seeds, _params(iteration_limit=args.iteration_limit), batch=args.batch)
-    cold = np.asarray(res["cold_iterations"], dtype=float)
-    warm = np.asarray(res["warm_iterations"], dtype=float)
-    summary = {
-        "instances": len(seeds),
-        "cold_mean_iterations": float(cold.mean()), "warm_mean_iterations": float(warm.mean()),
-        "cold_median_iterations": float(np.median(cold)), "warm_median_iterations": float(np.median(warm)),
-        "warm_better_fraction": float(np.mean(warm < cold)),
-        "cold_seconds": res["cold_seconds"], "warm_seconds": res["warm_seconds"],
-        "predict_seconds": res["predict_seconds"],
-        "cold_optimal": int(sum(1 for r in res["cold_reasons"] if r == 1)),
-        "warm_optimal": int(sum(1 for r in res["warm_reasons"] if r == 1)),
-        "dual_rel_error_median": float(np.median(res["dual_rel_error"])),
-    }
+    cold = None
+    if args.cold:
+        cold = _load_data([args.cold])
+        if [int(x) for x in cold["seeds"][: len(seeds)]] != seeds:
+            raise SystemExit("the cold data does not hold these seeds")
+    res = evaluate(mlp, model, seeds, _params(iteration_limit=args.iteration_limit), batch=args.batch, cold=cold,
+                   recover_plan=(args.recover_eps, args.recover_rounds), tighten=args.tight)
+    if cold is not None:
+        res["cold_seconds"] = float(cold["seconds"])
+    summary = summarize(res)
+    summary.update({"recover_eps": args.recover_eps, "recover_rounds": args.recover_rounds, "tight": args.tight})
     print(json.dumps(summary, indent=1))
     if args.out:
         with open(args.out, "w") as f:
-            json.dump({"summary": summary, "per_instance": {k: v for k, v in res.items()}}, f)
+            json.dump({"summary": summary, "per_instance": res}, f)
 
 
 def main(argv=None):
@@ -445,13 +516,18 @@ def main(argv=None):
     t.add_argument("--weight-decay", type=float, default=1e-4)
     t.add_argument("--seed", type=int, default=0)
     t.add_argument("--no-augment", action="store_true")
+    t.add_argument("--val-instances", type=int, default=256, help="last instances of --data kept for validation")
     t.add_argument("--log")
     e = sub.add_parser("evaluate")
     e.add_argument("--model", required=True)
     e.add_argument("--first", type=int, default=HELDOUT_SEED0)
     e.add_argument("--count", type=int, default=1024)
-    e.add_argument("--batch", type=int, default=256)
+    e.add_argument("--batch", type=int, default=512)
     e.add_argument("--iteration-limit", type=int, default=400_000)
+    e.add_argument("--cold", help="generate's output for the same seeds (solved with the same --batch)")
+    e.add_argument("--recover-eps", type=float, default=RECOVER_PLAN[0])
+    e.add_argument("--recover-rounds", type=int, default=RECOVER_PLAN[1])
+    e.add_argument("--tight", action="store_true", help="c-transform the predicted duals first")
     e.add_argument("--out")
     args = ap.parse_args(argv)
     {"generate": _cmd_generate, "train": _cmd_train, "evaluate": _cmd_evaluate}[args.cmd](args)

@@ -336,6 +336,11 @@ typedef struct pdot_batch_problem {
   const double* const* warm_dual_sources;
   const double* const* warm_dual_targets;
   const double* const* warm_primals;
+  /* Racing (NULL: none): race_groups[k] in 0..num_instances-1, or -1. Once an
+   * instance ends optimal, the other members of its group stop with
+   * PDOT_TERMINATION_REASON_OTHER at the same evaluation; a warm start and a
+   * cold start of one problem raced this way finish as soon as the faster one. */
+  const int32_t* race_groups;
 } pdot_batch_problem;
 
 typedef struct pdot_batch_output {          /* one per instance; arrays may be NULL */

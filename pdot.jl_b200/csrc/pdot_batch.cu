@@ -76,6 +76,8 @@ struct BatchBuffers {
   double* evpart;          // (grid + num) * kEvalSums
   double* vecpart;         // total vector blocks * kVecSums
   const int* warm;         // per instance: 1 when it starts from a warm start
+  const int* race;         // per instance: race group (-1: none), or null
+  int* winner;             // per group: lowest index of an optimal member (INT_MAX-like when none)
   DevState* st;            // per instance
   pdot_iteration_stats* rec;  // per instance: the latest evaluation record
   BatchActive* act;
@@ -494,6 +496,24 @@ __global__ void kb_compact(BatchBuffers B) {
   __shared__ int flags[1024];
   __shared__ int base;
   if (threadIdx.x == 0) base = 0;
+  if (B.race) {
+    // racing instances: once a member of a group is optimal, the others stop
+    for (int k = threadIdx.x; k < B.num; k += blockDim.x) {
+      const int g = B.race[k];
+      if (g >= 0 && B.st[k].done && B.st[k].termination_reason == PDOT_TERMINATION_REASON_OPTIMAL)
+        atomicMin(B.winner + g, k);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < B.num; k += blockDim.x) {
+      const int g = B.race[k];
+      if (g < 0 || B.st[k].done) continue;
+      const int w = __ldcg(B.winner + g);
+      if (w < B.num && w != k) {
+        B.st[k].done = 1;
+        B.st[k].termination_reason = PDOT_TERMINATION_REASON_OTHER;
+      }
+    }
+  }
   __syncthreads();
   long long units = 0, panels = 0, vblocks = 0;
   for (int off = 0; off < B.num; off += 1024) {
@@ -856,6 +876,18 @@ class BatchSolver {
       BCK(cudaMemcpy(warm_r_, hr.data(), ro * sizeof(double), cudaMemcpyHostToDevice));
       BCK(cudaMemcpy(warm_c_, hc.data(), co * sizeof(double), cudaMemcpyHostToDevice));
     }
+    // race groups: an instance stops (reason OTHER) once another member of
+    // its group has ended optimal
+    if (P.race_groups) {
+      std::vector<int> rg(B);
+      for (int k = 0; k < B; ++k) {
+        rg[k] = P.race_groups[k];
+        if (rg[k] < -1 || rg[k] >= B)
+          bfail(PDOT_ERR_INVALID_ARGUMENT, "instance %d: race group %d is not in -1..num_instances-1", k, rg[k]);
+      }
+      D_.race = upload(rg.data(), B);
+      D_.winner = alloc<int>(B);
+    }
     // plans recovered from the warm duals of the instances given no warm plan
     const double peps = opt ? opt->warm_plan_epsilon : 0.0;
     if (opt && (!(peps >= 0.0) || !std::isfinite(peps) || opt->warm_plan_iterations < 0 ||
@@ -1019,6 +1051,7 @@ class BatchSolver {
       BCK(cudaMemsetAsync(D_.c[0], 0, cols_ * sizeof(double), stream_));
     }
     BCK(cudaMemsetAsync(D_.st, 0, num_ * sizeof(pdot::DevState), stream_));
+    if (D_.winner) BCK(cudaMemsetAsync(D_.winner, 0x7F, num_ * sizeof(int), stream_));  // no winner yet
     pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_);
     BCK(cudaGetLastError());
     PDOT_BATCH_VARIANT(kind_, pdot::kb_norms, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));

@@ -136,6 +136,7 @@ class BatchProblemC(ct.Structure):
         ("warm_dual_sources", ct.POINTER(ct.c_void_p)),
         ("warm_dual_targets", ct.POINTER(ct.c_void_p)),
         ("warm_primals", ct.POINTER(ct.c_void_p)),
+        ("race_groups", ct.POINTER(ct.c_int32)),
     ]
 
 

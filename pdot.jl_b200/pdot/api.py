@@ -532,7 +532,7 @@ class Solver:
 
 def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", points=None, device: int = 0,
                      use_cuda_graph: bool = True, ctas_per_sm: int = 0, warm_starts=None,
-                     return_primal: bool = True, recover_plan=None):
+                     return_primal: bool = True, recover_plan=None, race_groups=None):
     """Solve many independent instances at once (pdot_optimize_batched).
 
     problems     a list of OptimalTransportProblem (cost_matrix may be None for
@@ -542,6 +542,8 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
     warm_starts  None, or per instance None / (u0, v0) / (u0, v0, X0)
     recover_plan (eps, rounds): plans recovered from the warm duals of the
                  instances given no plan (see _options)
+    race_groups  None, or a group id per instance (-1: none): once an
+                 instance ends optimal, the rest of its group stop (reason OTHER)
     return_primal  False leaves every primal_solution None (no m x n copies)
     Returns (outputs, seconds): a SaddlePointOutput per instance (its
     iteration_stats holds the final evaluation record) and the device time.
@@ -617,6 +619,12 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
     else:
         bp.source_points = xs_p
         bp.target_points = ys_p
+    if race_groups is not None:
+        rg = np.ascontiguousarray(race_groups, dtype=np.int32)
+        if rg.shape != (B,):
+            raise ValueError("race_groups needs one entry per instance")
+        keep.append(rg)
+        bp.race_groups = rg.ctypes.data_as(ct.POINTER(ct.c_int32))
     if warm_starts is not None:
         bp.warm_dual_sources = wu
         bp.warm_dual_targets = wv

@@ -106,7 +106,7 @@ def augment(a, b, u, v, side: int = SIDE):
 
 
 def solve_grid_batch(seeds, params: api.PdhgParameters, *, device: int = 0, warm_starts=None,
-                     recover_plan=None):
+                     recover_plan=None, race_groups=None):
     """Solve the grid instances of `seeds` in one batched launch with the
     on-the-fly squared-Euclidean cost. Returns (outputs, device seconds)."""
     pts = grid_points()
@@ -115,7 +115,8 @@ def solve_grid_batch(seeds, params: api.PdhgParameters, *, device: int = 0, warm
         a, b = grid_pair(int(s))
         probs.append(api.OptimalTransportProblem(None, a, b))
     return api.optimize_batched(params, probs, cost="sqeuclid", points=[(pts, pts)] * len(probs), device=device,
-                                warm_starts=warm_starts, return_primal=False, recover_plan=recover_plan)
+                                warm_starts=warm_starts, return_primal=False, recover_plan=recover_plan,
+                                race_groups=race_groups)
 
 
 def generate(seeds, params: api.PdhgParameters, *, batch: int = 256, device: int = 0, log=print):
@@ -317,11 +318,32 @@ def train(mlp: MLP, hist: np.ndarray, targets: np.ndarray, *, epochs: int = 60, 
     return losses, val
 
 
-def predict(mlp: MLP, model: WarmStartModel, a_rows: np.ndarray, b_rows: np.ndarray):
-    """Predicted canonical duals (u, v) for instances given row-wise."""
-    out = forward_rows(mlp, np.concatenate([a_rows, b_rows], axis=1))
-    duals = out.astype(np.float64) * model.target_scale + model.target_mean
-    return duals[:, :BINS], duals[:, BINS:]
+def predict(mlp: MLP, model: WarmStartModel, a_rows: np.ndarray, b_rows: np.ndarray, symmetrize: bool = False):
+    """Predicted canonical duals (u, v) for instances given row-wise. With
+    `symmetrize`, the prediction is the mean over the 16 images of each
+    instance under the grid cost's symmetries, each mapped back (the exact
+    duals map exactly, so this only averages the network's error)."""
+    if not symmetrize:
+        out = forward_rows(mlp, np.concatenate([a_rows, b_rows], axis=1))
+        duals = out.astype(np.float64) * model.target_scale + model.target_mean
+        return duals[:, :BINS], duals[:, BINS:]
+    n = a_rows.shape[0]
+    U = np.zeros((n, BINS))
+    V = np.zeros((n, BINS))
+    maps = grid_symmetries()
+    rows = []
+    for p in maps:
+        rows.append(np.concatenate([a_rows[:, p], b_rows[:, p]], axis=1))
+        rows.append(np.concatenate([b_rows[:, p], a_rows[:, p]], axis=1))
+    out = forward_rows(mlp, np.concatenate(rows, axis=0)).astype(np.float64) * model.target_scale + model.target_mean
+    for k, p in enumerate(maps):
+        d = out[(2 * k) * n:(2 * k + 1) * n]
+        U[:, p] += d[:, :BINS]
+        V[:, p] += d[:, BINS:]
+        d = out[(2 * k + 1) * n:(2 * k + 2) * n]   # the exchanged image: its source duals are v
+        V[:, p] += d[:, :BINS]
+        U[:, p] += d[:, BINS:]
+    return U / (2 * len(maps)), V / (2 * len(maps))
 
 
 def dataset(data: dict, augment_symmetries: bool = True):
@@ -343,31 +365,53 @@ def dataset(data: dict, augment_symmetries: bool = True):
 
 def evaluate(mlp: MLP, model: WarmStartModel, seeds, params: api.PdhgParameters, *, batch: int = 256,
              device: int = 0, cold: Optional[dict] = None, recover_plan=RECOVER_PLAN, tighten: bool = False,
-             log=print):
+             symmetrize: bool = False, race: bool = False, log=print):
     """Cold and learned-warm batched solves of the held-out `seeds`:
     iterations, device seconds, and the network's time (inference). `cold`,
     when given, holds the cold solves already made (generate()'s output for
     the same seeds, solved in chunks of the same `batch`). `tighten` replaces
     the predicted duals by their double c-transform (on the host) before the
-    warm start."""
+    warm start; `symmetrize` averages the prediction over the symmetries;
+    `race` solves a cold copy of every instance beside its warm start in the
+    same batch, the two in one race group, and takes whichever ends optimal
+    first (the warm iteration counts are then the winner's, and
+    warm_work_iterations adds both copies' iterations)."""
     seeds = list(seeds)
     C = grid_cost()
     res = {"cold_iterations": [], "warm_iterations": [], "cold_seconds": 0.0, "warm_seconds": 0.0,
-           "predict_seconds": 0.0, "cold_reasons": [], "warm_reasons": [], "dual_rel_error": []}
+           "predict_seconds": 0.0, "cold_reasons": [], "warm_reasons": [], "dual_rel_error": [],
+           "warm_work_iterations": [], "race_winner_warm": []}
     for k0 in range(0, len(seeds), batch):
         chunk = seeds[k0 : k0 + batch]
         ab = [grid_pair(int(s)) for s in chunk]
         t0 = time.perf_counter()
-        u, v = predict(mlp, model, np.asarray([x[0] for x in ab]), np.asarray([x[1] for x in ab]))
+        u, v = predict(mlp, model, np.asarray([x[0] for x in ab]), np.asarray([x[1] for x in ab]),
+                       symmetrize=symmetrize)
         res["predict_seconds"] += time.perf_counter() - t0
         if tighten:
             for k in range(len(chunk)):
                 u[k], v[k] = tight_duals(u[k], v[k], C)
         warm = [(u[k], v[k]) for k in range(len(chunk))]
-        outs_w, sec_w = solve_grid_batch(chunk, params, device=device, warm_starts=warm, recover_plan=recover_plan)
+        if race:
+            n = len(chunk)
+            outs, sec_w = solve_grid_batch(list(chunk) + list(chunk), params, device=device,
+                                           warm_starts=warm + [None] * n, recover_plan=recover_plan,
+                                           race_groups=list(range(n)) * 2)
+            opt = int(api.TerminationReason.TERMINATION_REASON_OPTIMAL)
+            for k in range(n):
+                w, c = outs[k], outs[n + k]
+                win = w if (int(w.termination_reason) == opt or int(c.termination_reason) != opt) else c
+                res["warm_iterations"].append(win.iteration_count)
+                res["warm_reasons"].append(int(win.termination_reason))
+                res["warm_work_iterations"].append(w.iteration_count + c.iteration_count)
+                res["race_winner_warm"].append(win is w)
+        else:
+            outs_w, sec_w = solve_grid_batch(chunk, params, device=device, warm_starts=warm,
+                                             recover_plan=recover_plan)
+            res["warm_iterations"] += [o.iteration_count for o in outs_w]
+            res["warm_work_iterations"] += [o.iteration_count for o in outs_w]
+            res["warm_reasons"] += [int(o.termination_reason) for o in outs_w]
         res["warm_seconds"] += sec_w
-        res["warm_iterations"] += [o.iteration_count for o in outs_w]
-        res["warm_reasons"] += [int(o.termination_reason) for o in outs_w]
         if cold is None:
             outs_c, sec_c = solve_grid_batch(chunk, params, device=device)
             res["cold_seconds"] += sec_c
@@ -399,6 +443,8 @@ def summarize(res: dict) -> dict:
         "cold_median_iterations": float(np.median(cold)), "warm_median_iterations": float(np.median(warm)),
         "cold_p90_iterations": float(np.percentile(cold, 90)), "warm_p90_iterations": float(np.percentile(warm, 90)),
         "warm_better_fraction": float(np.mean(warm < cold)),
+        "warm_work_mean_iterations": float(np.mean(res["warm_work_iterations"])),
+        "race_warm_wins": int(sum(res["race_winner_warm"])),
         "cold_seconds": float(res["cold_seconds"]), "warm_seconds": float(res["warm_seconds"]),
         "predict_seconds": float(res["predict_seconds"]),
         "cold_optimal": int(sum(1 for r in res["cold_reasons"] if r == 1)),
@@ -485,11 +531,13 @@ def _cmd_evaluate(args):
         if [int(x) for x in cold["seeds"][: len(seeds)]] != seeds:
             raise SystemExit("the cold data does not hold these seeds")
     res = evaluate(mlp, model, seeds, _params(iteration_limit=args.iteration_limit), batch=args.batch, cold=cold,
-                   recover_plan=(args.recover_eps, args.recover_rounds), tighten=args.tight)
+                   recover_plan=(args.recover_eps, args.recover_rounds), tighten=args.tight,
+                   symmetrize=args.symmetrize, race=args.race)
     if cold is not None:
         res["cold_seconds"] = float(cold["seconds"])
     summary = summarize(res)
-    summary.update({"recover_eps": args.recover_eps, "recover_rounds": args.recover_rounds, "tight": args.tight})
+    summary.update({"recover_eps": args.recover_eps, "recover_rounds": args.recover_rounds, "tight": args.tight,
+                    "symmetrize": args.symmetrize, "race": args.race})
     print(json.dumps(summary, indent=1))
     if args.out:
         with open(args.out, "w") as f:
@@ -528,6 +576,8 @@ def main(argv=None):
     e.add_argument("--recover-eps", type=float, default=RECOVER_PLAN[0])
     e.add_argument("--recover-rounds", type=int, default=RECOVER_PLAN[1])
     e.add_argument("--tight", action="store_true", help="c-transform the predicted duals first")
+    e.add_argument("--symmetrize", action="store_true", help="average the prediction over the 16 symmetries")
+    e.add_argument("--race", action="store_true", help="race a cold copy beside every warm start")
     e.add_argument("--out")
     args = ap.parse_args(argv)
     {"generate": _cmd_generate, "train": _cmd_train, "evaluate": _cmd_evaluate}[args.cmd](args)

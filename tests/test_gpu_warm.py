@@ -103,3 +103,24 @@ def test_batched_warm_and_cold_instances(cuda):
             assert abs(ow - oc) <= 2e-4 * (1 + abs(oc))
         else:
             assert w.iteration_count == 0
+
+
+def test_race_groups_stop_the_slower_member(cuda):
+    """An exact warm start and a cold start of the same problem in one race
+    group: the warm one is optimal at the first evaluation and the cold one
+    stops there (reason OTHER); an instance outside the group is unaffected."""
+    probs, pts = instances.batched_l1(2, 50, 90, seed=11)
+    params = pdot.default_parameters(1e-4)
+    cold, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts)
+    o = cold[0]
+    batch = [probs[0], probs[0], probs[1]]
+    bpts = [pts[0], pts[0], pts[1]]
+    warm = [(o.dual_source_solution, o.dual_target_solution, o.primal_solution), None, None]
+    out, _ = pdot.optimize_batched(params, batch, cost="l1", points=bpts, warm_starts=warm,
+                                   race_groups=[0, 0, -1])
+    assert out[0].termination_reason == OPTIMAL and out[0].iteration_count == 0
+    assert out[1].termination_reason == pdot.TerminationReason.TERMINATION_REASON_OTHER
+    assert out[1].iteration_count == 0
+    assert out[2].termination_reason == OPTIMAL and out[2].iteration_count == cold[1].iteration_count
+    with pytest.raises(pdot._abi.PdotError):
+        pdot.optimize_batched(params, batch, cost="l1", points=bpts, race_groups=[0, 3, -1])

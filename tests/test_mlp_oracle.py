@@ -63,3 +63,17 @@ def test_augmented_duals_solve_the_images():
     for aa, bb, uu, vv in imgs:
         assert aa @ uu + bb @ vv == pytest.approx(obj, rel=1e-12)
         assert np.min(C - uu[:, None] - vv[None, :]) >= np.min(C - u[:, None] - v[None, :]) - 1e-15
+
+
+def test_symmetrized_prediction_maps_images_back(monkeypatch):
+    """With an equivariant stand-in for the network (its 'duals' are the
+    input histograms), the prediction averaged over the 16 images returns
+    exactly that equivariant answer for the original instance."""
+    rng = np.random.default_rng(5)
+    a = rng.dirichlet(np.ones(learned.BINS), size=3)
+    b = rng.dirichlet(np.ones(learned.BINS), size=3)
+    monkeypatch.setattr(learned, "forward_rows", lambda mlp, hist: hist.astype(np.float32))
+    model = learned.WarmStartModel(np.zeros(1, np.float32), 0.0, 1.0)
+    u, v = learned.predict(None, model, a, b, symmetrize=True)
+    np.testing.assert_allclose(u, a.astype(np.float32), rtol=1e-6)
+    np.testing.assert_allclose(v, b.astype(np.float32), rtol=1e-6)

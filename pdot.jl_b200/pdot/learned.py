@@ -245,6 +245,52 @@ class WarmStartModel:
                               float(z["target_mean"]), float(z["target_scale"]), int(z["hidden_dim"]))
 
 
+MODEL_PATH = __import__("os").path.join(__import__("os").path.dirname(__file__), "models", "grid32_warmstart.npz")
+
+
+class WarmStarter:
+    """The packaged (or a given) trained network, ready to warm-start solves
+    of 32 x 32 grid instances."""
+
+    def __init__(self, model_path: Optional[str] = None, *, device: int = 0, max_batch: int = 512):
+        self.model = WarmStartModel.load(model_path or MODEL_PATH)
+        self.mlp = MLP(hidden_dim=self.model.hidden_dim, max_batch=max_batch, device=device)
+        self.mlp.set_parameters(self.model.parameters)
+        self.device = device
+
+    def predict(self, sources: np.ndarray, targets: np.ndarray):
+        return predict(self.mlp, self.model, np.atleast_2d(sources), np.atleast_2d(targets))
+
+    def solve(self, sources: np.ndarray, targets: np.ndarray, params: api.PdhgParameters, *, race: bool = True,
+              recover_plan=RECOVER_PLAN):
+        """Solve the grid instances (rows of `sources`, `targets`) in one
+        batched launch from the network's warm starts; with `race`, each next
+        to a cold start of itself in one race group, keeping whichever ends
+        optimal first. Returns (outputs, device seconds, warm_won flags)."""
+        sources, targets = np.atleast_2d(sources), np.atleast_2d(targets)
+        n = sources.shape[0]
+        u, v = self.predict(sources, targets)
+        pts = grid_points()
+        probs = [api.OptimalTransportProblem(None, sources[k], targets[k]) for k in range(n)]
+        warm = [(u[k], v[k]) for k in range(n)]
+        if not race:
+            outs, sec = api.optimize_batched(params, probs, cost="sqeuclid", points=[(pts, pts)] * n,
+                                             device=self.device, warm_starts=warm, return_primal=False,
+                                             recover_plan=recover_plan)
+            return outs, sec, [True] * n
+        outs, sec = api.optimize_batched(params, probs + probs, cost="sqeuclid", points=[(pts, pts)] * (2 * n),
+                                         device=self.device, warm_starts=warm + [None] * n, return_primal=False,
+                                         recover_plan=recover_plan, race_groups=list(range(n)) * 2)
+        opt = api.TerminationReason.TERMINATION_REASON_OPTIMAL
+        won, best = [], []
+        for k in range(n):
+            w, c = outs[k], outs[n + k]
+            take_w = w.termination_reason == opt or c.termination_reason != opt
+            best.append(w if take_w else c)
+            won.append(bool(take_w))
+        return best, sec, won
+
+
 def _bf16_bits(u32: np.ndarray) -> np.ndarray:
     u = u32.astype(np.uint64)
     u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16

@@ -77,3 +77,11 @@ def test_symmetrized_prediction_maps_images_back(monkeypatch):
     u, v = learned.predict(None, model, a, b, symmetrize=True)
     np.testing.assert_allclose(u, a.astype(np.float32), rtol=1e-6)
     np.testing.assert_allclose(v, b.astype(np.float32), rtol=1e-6)
+
+
+def test_packaged_model_loads():
+    model = learned.WarmStartModel.load(learned.MODEL_PATH)
+    I, H, O = 2 * learned.BINS, model.hidden_dim, 2 * learned.BINS
+    assert model.parameters.size == H * I + H + H * H + H + O * H + O
+    assert np.all(np.isfinite(model.parameters))
+    assert 0 < model.target_scale < 1

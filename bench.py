@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--n", type=int, default=N_COLS)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ttk", action="store_true", help="skip the time-to-KKT solve")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-solver line (512 instances)")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start line (64 instances)")
     ap.add_argument("--no-mp", action="store_true", help="skip the mixed-precision variants")
     ap.add_argument("--precision", choices=["f64", "f32"], default="f64",
                     help="plan precision of the primary workload (f64: the drop-in)")
@@ -356,6 +358,67 @@ def run_mixed(args, params, m, n, Ct, a, b, xs_d, ys_d, device, local, fp64_obj)
     return out
 
 
+def run_batched(args, device):
+    """The batched solver on 512 uneven instances (m, n log-uniform in
+    [64, 2048], points U[0,1]^2, L1 cost / max, Dirichlet(1) marginals, FP32
+    plan), all to relative KKT 1e-4 in one lockstep solve. Effective bandwidth:
+    16 B per entry per iteration (plan and average read and written; the cost
+    comes from the coordinates) summed over the iterations each instance ran,
+    divided by the device time of the whole solve."""
+    import pdot
+    from pdot import instances
+
+    probs, pts = instances.batched_l1(512, 64, 2048, seed=SEED)
+    params = pdot.default_parameters(TOL, iteration_limit=200_000)
+    outs, sec = pdot.optimize_batched(params, probs, cost="l1", points=pts, device=device.index,
+                                      return_primal=False)
+    its = np.array([o.iteration_count for o in outs], dtype=float)
+    mn = np.array([p.source_distribution.size * p.target_distribution.size for p in probs], dtype=float)
+    alg = float(np.sum(its * mn) * 16.0)
+    peak, _ = read_peak()
+    opt = pdot.TerminationReason.TERMINATION_REASON_OPTIMAL
+    return {"workload": "512 instances, m,n log-uniform [64,2048], L1 cost from U[0,1]^2 points, Dirichlet(1), "
+                        "FP32 plan, tol 1e-4",
+            "seconds": sec, "instances_per_sec": len(probs) / sec, "optimal": int(sum(o.termination_reason == opt
+                                                                                        for o in outs)),
+            "mean_iterations": float(its.mean()), "max_iterations": float(its.max()),
+            "total_entries": float(mn.sum()), "effective_gbs": alg / sec / 1e9, "peak": peak,
+            "effective_frac": alg / sec / 1e9 / peak}
+
+
+def run_learned(args, device):
+    """The learned warm start on 64 grid instances outside its training,
+    validation and evaluation seeds: one batched cold solve, and one batched
+    solve of the network's warm starts each raced against a cold start of the
+    same instance (a cold start is the fallback). Both to relative KKT 1e-4."""
+    import time
+
+    import pdot
+    from pdot import learned
+
+    seeds = list(range(9_200_000, 9_200_064))
+    params = pdot.default_parameters(TOL, iteration_limit=400_000)
+    pairs = [learned.grid_pair(s) for s in seeds]
+    A = np.asarray([p[0] for p in pairs])
+    B = np.asarray([p[1] for p in pairs])
+    cold, cold_sec = learned.solve_grid_batch(seeds, params, device=device.index)
+    ws = learned.WarmStarter(device=device.index, max_batch=128)
+    ws.predict(A[:1], B[:1])  # first-call setup outside the timing
+    t0 = time.perf_counter()
+    u, v = ws.predict(A, B)
+    pred_sec = time.perf_counter() - t0
+    warm, warm_sec, won = ws.solve(A, B, params, race=True)
+    ci = np.array([o.iteration_count for o in cold], dtype=float)
+    wi = np.array([o.iteration_count for o in warm], dtype=float)
+    opt = pdot.TerminationReason.TERMINATION_REASON_OPTIMAL
+    return {"workload": "64 held-out 32x32 grid instances (C5 distribution), sq-euclid grid cost, FP32 plan, tol 1e-4",
+            "cold_seconds": cold_sec, "learned_seconds": warm_sec + pred_sec, "network_seconds": pred_sec,
+            "speedup": cold_sec / (warm_sec + pred_sec),
+            "cold_mean_iterations": float(ci.mean()), "learned_mean_iterations": float(wi.mean()),
+            "cold_median_iterations": float(np.median(ci)), "learned_median_iterations": float(np.median(wi)),
+            "warm_won": int(sum(won)), "all_optimal": bool(all(o.termination_reason == opt for o in cold + warm))}
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -484,6 +547,9 @@ def run_ours(args, world, rank, local):
         fp64_obj = ttk["primal_objective"] if ttk else None
         mixed = run_mixed(args, params, m, n, Ct, a, b, xs_d, ys_d, device, local, fp64_obj)
 
+    batched = run_batched(args, device) if not args.no_batched else None
+    learned_ws = run_learned(args, device) if not args.no_learned else None
+
     cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_baseline(xs, ys, a_h, b_h, m, n, steps=20)
@@ -508,7 +574,7 @@ def run_ours(args, world, rank, local):
                      "share_of_kernel_time": k1_ms / region_kernel_ms if region_kernel_ms > 0 else None},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk.summary(), "time_to_kkt": ttk,
-        "mixed_precision": mixed,
+        "mixed_precision": mixed, "batched": batched, "learned_warm_start": learned_ws,
     }
     return line
 

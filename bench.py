@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--no-ttk", action="store_true", help="skip the time-to-KKT solve")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-solver line (512 instances)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start line (64 instances)")
+    ap.add_argument("--batched-only", action="store_true", help="run only the batched-solver line and print it")
     ap.add_argument("--no-mp", action="store_true", help="skip the mixed-precision variants")
     ap.add_argument("--precision", choices=["f64", "f32"], default="f64",
                     help="plan precision of the primary workload (f64: the drop-in)")
@@ -584,6 +585,10 @@ def main():
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         line = run_reference(args, world, rank)
+    elif args.batched_only:
+        import torch
+
+        line = run_batched(args, torch.device("cuda", local))
     else:
         line = run_ours(args, world, rank, local)
     if rank == 0 and line is not None:

@@ -37,6 +37,7 @@ namespace {
 constexpr int kBR = 4;                       // FP32 rows per lane load
 constexpr int kBRPL = kPanelRows / (32 * kBR);  // loads per lane per unit
 constexpr int kMaxBatch = 1 << 16;
+constexpr int kJU = 2;  // columns per warp step of the batched primal pass
 
 struct BatchInstance {
   int64_t m, n, ld;  // rows, columns, padded leading dimension
@@ -186,7 +187,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
       const long long je = (ql1 < (p + 1) * I.n ? ql1 : (p + 1) * I.n) - p * I.n;
       const long long row0 = p * kPanelRows;
       double acc[kBRPL][kBR];
-      double ur[kBRPL][kBR];
+      float ur[kBRPL][kBR];  // the FP32 plan's entry arithmetic takes the duals in FP32
       bool ok[kBRPL];
 #pragma unroll
       for (int kq = 0; kq < kBRPL; ++kq) {
@@ -195,51 +196,66 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
 #pragma unroll
         for (int e = 0; e < kBR; ++e) {
           acc[kq][e] = 0.0;
-          ur[kq][e] = (ok[kq] && i + e < I.m && !zero_g) ? __ldg(u + i + e) : 0.0;
+          ur[kq][e] = (ok[kq] && i + e < I.m && !zero_g) ? (float)__ldg(u + i + e) : 0.0f;
         }
       }
       cost.panel(row0, lane, I.m, ok);
-      for (long long j = jb + warp; j < je; j += kWarps) {
-        const double vj = zero_g ? 0.0 : __ldg(v + j);
-        cost.column(j);
-        const long long col = j * I.ld + row0 + lane * kBR;
-        typename CostReader<CK, kBR, kBRPL>::value_t cv[kBRPL][kBR];
-        float xv[kBRPL][kBR], av[kBRPL][kBR];
+      // kJU columns per warp step: every load of the step is issued before any
+      // entry is computed, so a warp keeps kJU units of plan and average in
+      // flight (an FP32 plan with a coordinate cost has little else to load)
+      for (long long j = jb + warp; j < je; j += kWarps * kJU) {
+        typename CostReader<CK, kBR, kBRPL>::value_t cv[kJU][kBRPL][kBR];
+        float xv[kJU][kBRPL][kBR], av[kJU][kBRPL][kBR];
+        float vj[kJU];
 #pragma unroll
-        for (int kq = 0; kq < kBRPL; ++kq) {
-          if (ok[kq]) {
-            const long long idx = col + kq * 32 * kBR;
-            cost.get(idx, kq, cv[kq]);
-            vld<float, kBR>(X + idx, xv[kq]);
-            if (!first) vld<float, kBR>(Xa + idx, av[kq]);
-          }
-        }
-        double cs = 0.0;
+        for (int ju = 0; ju < kJU; ++ju) {
+          const long long jj = j + ju * kWarps;
+          if (jj >= je) continue;
+          vj[ju] = zero_g ? 0.0f : (float)__ldg(v + jj);
+          cost.column(jj);
+          const long long col = jj * I.ld + row0 + lane * kBR;
 #pragma unroll
-        for (int kq = 0; kq < kBRPL; ++kq) {
-          if (ok[kq]) {
-            const long long i = row0 + kq * 32 * kBR + lane * kBR;
-#pragma unroll
-            for (int e = 0; e < kBR; ++e) {
-              if (i + e < I.m) {
-                double d;
-                primal_entry<float>(widen(cv[kq][e]), ur[kq][e], vj, s, nw, aw, zero_g, first, xv[kq][e],
-                                    av[kq][e], d);
-                acc[kq][e] += d;
-                cs += d;
-                sq += d * d;
-              } else {  // padded row
-                xv[kq][e] = 0.0f;
-                av[kq][e] = 0.0f;
-              }
+          for (int kq = 0; kq < kBRPL; ++kq) {
+            if (ok[kq]) {
+              const long long idx = col + kq * 32 * kBR;
+              cost.get(idx, kq, cv[ju][kq]);
+              vld<float, kBR>(X + idx, xv[ju][kq]);
+              if (!first) vld<float, kBR>(Xa + idx, av[ju][kq]);
             }
-            const long long idx = col + kq * 32 * kBR;
-            vst<float, kBR>(X + idx, xv[kq]);
-            vst<float, kBR>(Xa + idx, av[kq]);
           }
         }
-        cs = warp_sum(cs);
-        if (lane == 0) B.colpart[base_u + p * I.n + j] = cs;
+#pragma unroll
+        for (int ju = 0; ju < kJU; ++ju) {
+          const long long jj = j + ju * kWarps;
+          if (jj >= je) continue;
+          const long long col = jj * I.ld + row0 + lane * kBR;
+          double cs = 0.0;
+#pragma unroll
+          for (int kq = 0; kq < kBRPL; ++kq) {
+            if (ok[kq]) {
+              const long long i = row0 + kq * 32 * kBR + lane * kBR;
+#pragma unroll
+              for (int e = 0; e < kBR; ++e) {
+                if (i + e < I.m) {
+                  double d;
+                  primal_entry<float>(widen(cv[ju][kq][e]), ur[kq][e], vj[ju], s, nw, aw, zero_g, first,
+                                      xv[ju][kq][e], av[ju][kq][e], d);
+                  acc[kq][e] += d;
+                  cs += d;
+                  sq += d * d;
+                } else {  // padded row
+                  xv[ju][kq][e] = 0.0f;
+                  av[ju][kq][e] = 0.0f;
+                }
+              }
+              const long long idx = col + kq * 32 * kBR;
+              vst<float, kBR>(X + idx, xv[ju][kq]);
+              vst<float, kBR>(Xa + idx, av[ju][kq]);
+            }
+          }
+          cs = warp_sum(cs);
+          if (lane == 0) B.colpart[base_u + p * I.n + jj] = cs;
+        }
       }
 #pragma unroll
       for (int kq = 0; kq < kBRPL; ++kq)

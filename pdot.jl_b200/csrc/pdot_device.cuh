@@ -280,27 +280,39 @@ struct CostReader<PDOT_COST_BF16, R, RPL> : StoredCost<__nv_bfloat16, R, RPL> {
   using StoredCost<__nv_bfloat16, R, RPL>::StoredCost;
 };
 
-// One entry of the primal pass (see the fused pass below). With an FP32 plan
-// the new value is rounded to its stored precision first and the step d is
-// taken between stored values.
+// One entry of the primal pass (see the fused pass below).
+//
+// FP64 plan (the drop-in): the reference's statement order with explicit
+// round-to-nearest FP64 operations, bit for bit as the oracle computes it.
+//
+// FP32 plan (mixed precision): the entry's arithmetic runs in FP32, the
+// plan's own precision (the cost entry is FP32 or BF16 storage or computed in
+// FP32; the duals and step weights are rounded to FP32 once). The step d
+// between the two stored values is formed exactly in FP64, so the FP64 row,
+// column and squared-norm sums the caller accumulates add exactly what was
+// stored.
+__device__ __forceinline__ float jl_max0f(float x) { return x > 0.0f ? x : (x != x ? x : 0.0f); }
+
 template <typename TX>
 __device__ __forceinline__ void primal_entry(double c, double ui, double vj, double s, double nw, double aw,
                                              bool zero_g, bool first, TX& xs, TX& xas, double& d) {
-  const double x = widen(xs);
-  const double gg = zero_g ? 0.0 : __dsub_rn(__dsub_rn(c, ui), vj);
-  const double t = jl_max0(__dsub_rn(x, __dmul_rn(s, gg)));
-  double xn;
   if constexpr (sizeof(TX) == 8) {
+    const double x = xs;
+    const double gg = zero_g ? 0.0 : __dsub_rn(__dsub_rn(c, ui), vj);
+    const double t = jl_max0(__dsub_rn(x, __dmul_rn(s, gg)));
     d = __dsub_rn(t, x);
-    xn = __dadd_rn(x, d);
+    const double xn = __dadd_rn(x, d);
+    xs = xn;
+    xas = first ? xn : __dmul_rn(__dadd_rn(xas, __dmul_rn(xn, nw)), aw);
   } else {
-    xn = (double)__double2float_rn(t);
-    d = __dsub_rn(xn, x);
+    const float x = xs;
+    const float gg = zero_g ? 0.0f : __fsub_rn(__fsub_rn((float)c, (float)ui), (float)vj);
+    const float t = jl_max0f(__fsub_rn(x, __fmul_rn((float)s, gg)));
+    d = __dsub_rn((double)t, (double)x);
+    xs = t;
+    xas = first ? t : __fmul_rn(__fadd_rn(xas, __fmul_rn(t, (float)nw)), (float)aw);
   }
-  xs = narrow<TX>(xn);
-  xas = narrow<TX>(first ? xn : __dmul_rn(__dadd_rn(widen(xas), __dmul_rn(xn, nw)), aw));
 }
-
 
 constexpr int kSpinLimit = 1 << 22;
 

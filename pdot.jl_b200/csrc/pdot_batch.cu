@@ -286,6 +286,276 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// The batched primal pass with bulk-copy staging (the single solver's staged
+// pass, over the concatenated unit line). Each warp keeps an S-stage ring in
+// shared memory; lane 0 issues cp.async.bulk copies of the plan, average and
+// stored cost of the warp's next units, which may lie in the next panel or the
+// next instance, so the bytes in flight do not depend on registers. A unit is
+// copied with the padded leading dimension (rows up to ld, a multiple of 4),
+// so every copy starts and ends on a 16-byte boundary; the padded rows are
+// zero in the plan and in the stored cost. Every wait is bounded: on a timeout
+// the kernel sets kernel_error of the instance at hand, drains (bounded) the
+// copies in flight and leaves its remaining units alone.
+template <int CK>
+struct BatchStagedLayout {
+  static constexpr bool kPts = is_point_cost(CK);
+  static constexpr int kCBytes = kPts ? 0 : kPanelRows * 4;
+  static constexpr int kXBytes = kPanelRows * 4;
+  static constexpr int kStageBytes = kCBytes + 2 * kXBytes;
+  static constexpr int S0 = (96 * 1024) / (kWarps * kStageBytes);
+  static constexpr int S = S0 > 6 ? 6 : (S0 < 2 ? 2 : S0);
+  static constexpr int kRingBytes = kWarps * S * kStageBytes;
+  static constexpr int kSmem = kRingBytes + kWarps * S * 8;
+};
+
+// The units of warp w in a CTA's range [q0, q1) of the active unit line, in
+// the order the pass consumes them: by instance, by panel, columns w, w+8, ...
+struct BatchCursor {
+  int kk, k, buf;
+  bool first, valid;
+  long long ql1, n, p, j, je, ld, x_off;  // the current instance, as its copies need it
+  __device__ __forceinline__ void init(const BatchBuffers& B, int count, long long q0, long long q1, int w) {
+    kk = find_segment(B.unit_prefix, count, q0);
+    valid = true;
+    enter(B, count, q0, q1, w, true);
+  }
+  // the instance of segment kk: its local range and first column of this warp
+  __device__ __forceinline__ void enter(const BatchBuffers& B, int count, long long q0, long long q1, int w,
+                                        bool first_segment) {
+    for (;;) {
+      if (kk >= count) {
+        valid = false;
+        return;
+      }
+      const long long base = B.unit_prefix[kk];
+      if (base >= q1) {
+        valid = false;
+        return;
+      }
+      k = B.ids[kk];
+      const BatchInstance& I = B.inst[k];
+      n = I.n;
+      ld = I.ld;
+      x_off = I.x_off;
+      buf = B.st[k].buf;
+      first = !(B.st[k].sum_weights > 0.0);
+      const long long ql0 = (first_segment ? q0 : base) - base;
+      const long long end = B.unit_prefix[kk + 1];
+      ql1 = (q1 < end ? q1 : end) - base;
+      p = ql0 / n;
+      const long long jb = ql0 - p * n;
+      je = (ql1 < (p + 1) * n ? ql1 : (p + 1) * n) - p * n;
+      j = jb + w;
+      if (normalize_panels(w)) return;
+      ++kk;
+      first_segment = false;
+    }
+  }
+  // true while (p, j) is a unit of the current instance
+  __device__ __forceinline__ bool normalize_panels(int w) {
+    while (j >= je) {
+      ++p;
+      if (p * n >= ql1) return false;
+      je = (ql1 < (p + 1) * n ? ql1 : (p + 1) * n) - p * n;
+      j = w;
+    }
+    return true;
+  }
+  __device__ __forceinline__ void advance(const BatchBuffers& B, int count, long long q0, long long q1, int w) {
+    j += kWarps;
+    if (normalize_panels(w)) return;
+    ++kk;
+    enter(B, count, q0, q1, w, false);
+  }
+};
+
+template <int CK>
+__global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) {
+  using L = BatchStagedLayout<CK>;
+  static_assert(L::kSmem <= 100 * 1024, "two CTAs per SM hold their rings");
+  constexpr int S = L::S;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ double red[kWarps][kPanelRows];
+  __shared__ double sqw[kWarps];
+  const BatchActive act = *B.act;
+  if (act.count == 0) return;
+  const long long U = act.total_units;
+  const int G = gridDim.x;
+  const long long cta = blockIdx.x;
+  const long long q0 = bunit_begin(U, G, cta), q1 = bunit_begin(U, G, cta + 1);
+  if (q0 >= q1) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned char* ring = smem + (size_t)warp * S * L::kStageBytes;
+  const uint32_t bar0 = smem_u32(smem + L::kRingBytes) + (uint32_t)(warp * S * 8);
+  if (lane == 0) {
+    for (int t = 0; t < S; ++t) mbar_init(bar0 + 8 * t, 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+
+  // lane 0 fills stage t with the producer cursor's unit
+  auto issue = [&](const BatchCursor& c, int t) {
+    const long long row0 = c.p * kPanelRows;
+    const long long rows = (c.ld - row0) < kPanelRows ? (c.ld - row0) : kPanelRows;
+    const uint32_t xb = (uint32_t)(rows * 4);
+    const uint32_t cb = L::kPts ? 0u : xb;
+    const uint32_t bar = bar0 + 8 * t;
+    unsigned char* stg = ring + (size_t)t * L::kStageBytes;
+    const long long off = c.j * c.ld + row0;
+    mbar_expect_tx(bar, cb + xb + (c.first ? 0u : xb));
+    if (!L::kPts) bulk_g2s(smem_u32(stg), B.C + c.x_off + off, cb, bar);
+    bulk_g2s(smem_u32(stg + L::kCBytes), B.X[c.buf] + c.x_off + off, xb, bar);
+    if (!c.first) bulk_g2s(smem_u32(stg + L::kCBytes + L::kXBytes), B.X[c.buf ^ 1] + c.x_off + off, xb, bar);
+  };
+
+  BatchCursor prod, cons;
+  prod.init(B, act.count, q0, q1, warp);
+  cons.init(B, act.count, q0, q1, warp);
+  long long issued = 0, consumed = 0;
+  for (int t = 0; t < S && prod.valid; ++t) {
+    if (lane == 0) issue(prod, t);
+    prod.advance(B, act.count, q0, q1, warp);
+    ++issued;
+  }
+  bool failed = false;
+  int kk = find_segment(B.unit_prefix, act.count, q0);
+  long long q = q0;
+  while (q < q1) {
+    const int k = B.ids[kk];
+    const BatchInstance I = B.inst[k];
+    DevState* st = B.st + k;
+    const long long base_u = B.unit_prefix[kk];
+    const long long seg_end = min(q1, (long long)B.unit_prefix[kk + 1]);
+    const int buf = st->buf;
+    const double tau = st->step_size, omega = st->primal_weight, Ssum = st->sum_weights;
+    const bool zero_g = st->g_is_zero != 0;
+    const bool first = !(Ssum > 0.0);
+    const double s = __ddiv_rn(tau, omega);
+    const double nw = first ? 1.0 : __ddiv_rn(tau, Ssum);
+    const double aw = first ? 1.0 : __ddiv_rn(Ssum, __dadd_rn(Ssum, tau));
+    float* __restrict__ X = B.X[buf] + I.x_off;
+    float* __restrict__ Xa = B.X[buf ^ 1] + I.x_off;
+    const double* __restrict__ u = B.u[buf] + I.row_off;
+    const double* __restrict__ v = B.v[buf] + I.col_off;
+    CostSource csrc;
+    csrc.C = nullptr;
+    csrc.xs = B.xs ? B.xs + I.pts_off * B.dim : nullptr;
+    csrc.ys = B.ys ? B.ys + I.tpts_off * B.dim : nullptr;
+    csrc.dim = B.dim;
+    CostReader<CK, kBR, kBRPL> cost(csrc, (float)st->cost_scale);
+    double sq = 0.0;
+    const long long ql0 = q - base_u, ql1 = seg_end - base_u;
+    for (long long p = ql0 / I.n; p * I.n < ql1; ++p) {
+      const long long row0 = p * kPanelRows;
+      double acc[kBRPL][kBR];
+      float ur[kBRPL][kBR];
+      bool ok[kBRPL];
+#pragma unroll
+      for (int kq = 0; kq < kBRPL; ++kq) {
+        const long long i = row0 + kq * 32 * kBR + lane * kBR;
+        ok[kq] = i < I.m;
+#pragma unroll
+        for (int e = 0; e < kBR; ++e) {
+          acc[kq][e] = 0.0;
+          ur[kq][e] = (ok[kq] && i + e < I.m && !zero_g) ? (float)__ldg(u + i + e) : 0.0f;
+        }
+      }
+      cost.panel(row0, lane, I.m, ok);
+      while (!failed && cons.valid && cons.kk == kk && cons.p == p) {
+        const long long j = cons.j;
+        const int stage = (int)(consumed % S);
+        const uint32_t parity = (uint32_t)((consumed / S) & 1);
+        if (!mbar_wait_bounded(bar0 + 8 * stage, parity)) {
+          failed = true;
+          if (lane == 0) atomicExch(&st->kernel_error, 1);
+          break;
+        }
+        const unsigned char* stg = ring + (size_t)stage * L::kStageBytes;
+        const float* sC = reinterpret_cast<const float*>(stg);
+        const float* sX = reinterpret_cast<const float*>(stg + L::kCBytes);
+        const float* sXa = reinterpret_cast<const float*>(stg + L::kCBytes + L::kXBytes);
+        const float vj = zero_g ? 0.0f : (float)__ldg(v + j);
+        cost.column(j);
+        const long long col = j * I.ld + row0 + lane * kBR;
+        double cs = 0.0;
+#pragma unroll
+        for (int kq = 0; kq < kBRPL; ++kq) {
+          if (ok[kq]) {
+            const int r = kq * 32 * kBR + lane * kBR;
+            typename CostReader<CK, kBR, kBRPL>::value_t cv[kBR];
+            if constexpr (L::kPts)
+              cost.get(0, kq, cv);
+            else
+              vld<float, kBR>(sC + r, cv);
+            float xv[kBR], av[kBR];
+            vld<float, kBR>(sX + r, xv);
+            if (!first) vld<float, kBR>(sXa + r, av);
+            const long long i = row0 + r;
+#pragma unroll
+            for (int e = 0; e < kBR; ++e) {
+              if (i + e < I.m) {
+                double d;
+                primal_entry<float>(widen(cv[e]), ur[kq][e], vj, s, nw, aw, zero_g, first, xv[e], av[e], d);
+                acc[kq][e] += d;
+                cs += d;
+                sq += d * d;
+              } else {  // padded row
+                xv[e] = 0.0f;
+                av[e] = 0.0f;
+              }
+            }
+            vst<float, kBR>(X + col + kq * 32 * kBR, xv);
+            vst<float, kBR>(Xa + col + kq * 32 * kBR, av);
+          }
+        }
+        cs = warp_sum(cs);
+        if (lane == 0) B.colpart[base_u + p * I.n + j] = cs;
+        __syncwarp();
+        ++consumed;
+        cons.advance(B, act.count, q0, q1, warp);
+        if (prod.valid) {
+          if (lane == 0) issue(prod, stage);
+          prod.advance(B, act.count, q0, q1, warp);
+          ++issued;
+        }
+      }
+#pragma unroll
+      for (int kq = 0; kq < kBRPL; ++kq)
+#pragma unroll
+        for (int e = 0; e < kBR; ++e) red[warp][kq * 32 * kBR + lane * kBR + e] = acc[kq][e];
+      __syncthreads();
+      const long long gp = B.panel_prefix[kk] + p;
+      for (int t = threadIdx.x; t < kPanelRows; t += kThreads) {
+        double s2 = red[0][t];
+#pragma unroll
+        for (int w = 1; w < kWarps; ++w) s2 += red[w][t];
+        B.rowpart[(cta + gp) * kPanelRows + t] = s2;
+      }
+      __syncthreads();
+    }
+    sq = warp_sum(sq);
+    if (lane == 0) sqw[warp] = sq;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s2 = sqw[0];
+#pragma unroll
+      for (int w = 1; w < kWarps; ++w) s2 += sqw[w];
+      B.sqpart[cta + kk] = s2;
+    }
+    __syncthreads();
+    q = seg_end;
+    ++kk;
+  }
+  if (consumed < issued) {
+    // only after a timeout: drain the copies still in flight (bounded) before
+    // the shared memory goes away, and report
+    if (!failed && lane == 0) atomicExch(&B.st[B.ids[find_segment(B.unit_prefix, act.count, q0)]].kernel_error, 1);
+    for (long long c = consumed; c < issued; ++c)
+      mbar_wait_bounded(bar0 + 8 * (int)(c % S), (uint32_t)((c / S) & 1));
+  }
+}
+
 // Batched dual step + per-instance step control (last CTA of each instance).
 __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConfig cfg, int grid) {
   const BatchActive act = *B.act;
@@ -784,10 +1054,25 @@ class BatchSolver {
     total_vblocks_ = vblocks;
     int sms = 148;
     BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+    // the primal pass: staged by bulk copies for the coordinate costs (whose
+    // plan and average are all there is to load), direct 16-byte loads for the
+    // stored FP32 cost; primal_pass overrides
+    const int pass = opt ? opt->primal_pass : PDOT_PASS_AUTO;
+    staged_ = pass == PDOT_PASS_STAGED || (pass == PDOT_PASS_AUTO && dim_ > 0);
     int occ = 1;
-    PDOT_BATCH_VARIANT(kind_, pdot::kb_primal,
-                       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, pdot::kThreads, 0) != cudaSuccess ||
-                           occ < 1) occ = 1);
+    if (staged_) {
+      PDOT_BATCH_VARIANT(kind_, pdot::kb_primal_staged, {
+        const int smem = staged_smem(kind_);
+        if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, pdot::kThreads, smem) != cudaSuccess || occ < 1)
+          occ = 1;
+      });
+    } else {
+      PDOT_BATCH_VARIANT(kind_, pdot::kb_primal,
+                         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, pdot::kThreads, 0) !=
+                                 cudaSuccess ||
+                             occ < 1) occ = 1);
+    }
     cudaGetLastError();
     grid_ = (int)std::min<int64_t>((int64_t)sms * occ, std::max<int64_t>(units, 1));
     if (opt && opt->ctas_per_sm > 0)
@@ -1043,7 +1328,9 @@ class BatchSolver {
     c.time_sec_limit = p.termination_criteria.time_sec_limit;
     c.iteration_limit = p.termination_criteria.iteration_limit;
     c.kkt_matrix_pass_limit = p.termination_criteria.kkt_matrix_pass_limit;
-    c.record_iteration_stats = 0;
+    // every evaluation overwrites the instance's one record, so an instance
+    // stopped by its race group keeps its last evaluation
+    c.record_iteration_stats = 1;
     c.scale_invariant_initial_primal_weight = p.scale_invariant_initial_primal_weight != 0;
     c.primal_importance = p.primal_importance;
     c.cost_scale = 0.0;
@@ -1068,6 +1355,7 @@ class BatchSolver {
     }
     BCK(cudaMemsetAsync(D_.st, 0, num_ * sizeof(pdot::DevState), stream_));
     if (D_.winner) BCK(cudaMemsetAsync(D_.winner, 0x7F, num_ * sizeof(int), stream_));  // no winner yet
+    BCK(cudaMemsetAsync(D_.rec, 0, num_ * sizeof(pdot_iteration_stats), stream_));
     pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_);
     BCK(cudaGetLastError());
     PDOT_BATCH_VARIANT(kind_, pdot::kb_norms, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
@@ -1090,8 +1378,19 @@ class BatchSolver {
     pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_);
     BCK(cudaGetLastError());
   }
+  static int staged_smem(int kind) {
+    // the stored FP32 cost adds a plane to every stage; the coordinate costs do not
+    return kind == PDOT_COST_F32 ? pdot::BatchStagedLayout<PDOT_COST_F32>::kSmem
+                                 : pdot::BatchStagedLayout<pdot::kCostSqBase + 1>::kSmem;
+  }
+
   void launch_step() {
-    PDOT_BATCH_VARIANT(kind_, pdot::kb_primal, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
+    if (staged_) {
+      const int smem = staged_smem(kind_);
+      PDOT_BATCH_VARIANT(kind_, pdot::kb_primal_staged, (kfn<<<grid_, pdot::kThreads, smem, stream_>>>(D_)));
+    } else {
+      PDOT_BATCH_VARIANT(kind_, pdot::kb_primal, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
+    }
     pdot::kb_dual<<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_);
     BCK(cudaGetLastError());
   }
@@ -1134,6 +1433,9 @@ class BatchSolver {
     std::vector<pdot_iteration_stats> rec(num_);
     BCK(cudaMemcpy(st.data(), D_.st, num_ * sizeof(pdot::DevState), cudaMemcpyDeviceToHost));
     BCK(cudaMemcpy(rec.data(), D_.rec, num_ * sizeof(pdot_iteration_stats), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < num_; ++k)
+      if (st[k].kernel_error)
+        bfail(PDOT_ERR_CUDA, "instance %d: the staged primal pass gave up waiting for its copies", k);
     double* tmp = nullptr;
     size_t cap = 0;
     for (int k = 0; k < num_; ++k) {
@@ -1164,7 +1466,7 @@ class BatchSolver {
   }
 
   int device_ = 0, num_ = 0, dim_ = 0, kind_ = 0, grid_ = 1;
-  bool use_graph_ = true, any_warm_ = false, recover_plans_ = false;
+  bool use_graph_ = true, any_warm_ = false, recover_plans_ = false, staged_ = false;
   int plan_iters_ = 0;
   pdot::WarmPlanArgs wp_{};
   float* warm_x_ = nullptr;

@@ -532,7 +532,8 @@ class Solver:
 
 def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", points=None, device: int = 0,
                      use_cuda_graph: bool = True, ctas_per_sm: int = 0, warm_starts=None,
-                     return_primal: bool = True, recover_plan=None, race_groups=None):
+                     return_primal: bool = True, recover_plan=None, race_groups=None,
+                     primal_pass: str = "auto"):
     """Solve many independent instances at once (pdot_optimize_batched).
 
     problems     a list of OptimalTransportProblem (cost_matrix may be None for
@@ -544,6 +545,7 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
                  instances given no plan (see _options)
     race_groups  None, or a group id per instance (-1: none): once an
                  instance ends optimal, the rest of its group stop (reason OTHER)
+    primal_pass  "auto" (staged for coordinate costs), "staged" or "direct"
     return_primal  False leaves every primal_solution None (no m x n copies)
     Returns (outputs, seconds): a SaddlePointOutput per instance (its
     iteration_stats holds the final evaluation record) and the device time.
@@ -633,6 +635,7 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
     if cost != "f32":
         opts.point_dim = dim
     opts.ctas_per_sm = int(ctas_per_sm)
+    opts.primal_pass = {"auto": _abi.PASS_AUTO, "staged": _abi.PASS_STAGED, "direct": _abi.PASS_DIRECT}[primal_pass]
     cp = marshal_params(params)
     sec = ct.c_double(0.0)
     rc = lib.pdot_optimize_batched(ct.byref(bp), ct.byref(cp), ct.byref(opts), outs, ct.byref(sec))

@@ -96,3 +96,24 @@ def test_batched_is_deterministic(cuda):
     for x, y in zip(o1, o2):
         assert x.iteration_count == y.iteration_count
         assert np.array_equal(x.primal_solution, y.primal_solution)
+
+
+@pytest.mark.parametrize("cost", ["l1", "f32"])
+def test_batched_staged_and_direct_passes_agree(cuda, cost):
+    """The bulk-copy staged pass and the direct pass do the same arithmetic in
+    the same order over the same CTA partition (two CTAs per SM each), so the
+    solves agree bit for bit. Sizes include partial panels and rows that are
+    not a multiple of 4."""
+    probs, pts = instances.batched_l1(count=20, lo=3, hi=700, seed=9)
+    if cost == "f32":
+        probs = [pdot.OptimalTransportProblem(instances.l1_cost(*pt), p.source_distribution, p.target_distribution)
+                 for p, pt in zip(probs, pts)]
+    params = pdot.default_parameters(1e-4)
+    kw = {} if cost == "f32" else {"points": pts}
+    st, _ = pdot.optimize_batched(params, probs, cost=cost, primal_pass="staged", **kw)
+    di, _ = pdot.optimize_batched(params, probs, cost=cost, primal_pass="direct", **kw)
+    for x, y in zip(st, di):
+        assert x.termination_reason == OPTIMAL
+        assert x.iteration_count == y.iteration_count
+        assert np.array_equal(x.primal_solution, y.primal_solution)
+        assert np.array_equal(x.dual_source_solution, y.dual_source_solution)

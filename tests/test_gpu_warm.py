@@ -121,6 +121,9 @@ def test_race_groups_stop_the_slower_member(cuda):
     assert out[0].termination_reason == OPTIMAL and out[0].iteration_count == 0
     assert out[1].termination_reason == pdot.TerminationReason.TERMINATION_REASON_OTHER
     assert out[1].iteration_count == 0
+    # the stopped member keeps its last evaluation record (the first one here)
+    assert out[1].iteration_stats[-1].iteration_number == 1
+    assert out[1].iteration_stats[-1].convergence_information[0].l2_primal_residual > 0
     assert out[2].termination_reason == OPTIMAL and out[2].iteration_count == cold[1].iteration_count
     with pytest.raises(pdot._abi.PdotError):
         pdot.optimize_batched(params, batch, cost="l1", points=bpts, race_groups=[0, 3, -1])

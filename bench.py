@@ -371,8 +371,10 @@ def run_batched(args, device):
 
     probs, pts = instances.batched_l1(512, 64, 2048, seed=SEED)
     params = pdot.default_parameters(TOL, iteration_limit=200_000)
+    # the autotuner picks the launch configuration from the first 256 iterations
+    best, timings = pdot.tune_batched(params, probs, cost="l1", points=pts, device=device.index)
     outs, sec = pdot.optimize_batched(params, probs, cost="l1", points=pts, device=device.index,
-                                      return_primal=False)
+                                      return_primal=False, **best)
     its = np.array([o.iteration_count for o in outs], dtype=float)
     mn = np.array([p.source_distribution.size * p.target_distribution.size for p in probs], dtype=float)
     alg = float(np.sum(its * mn) * 16.0)
@@ -384,7 +386,8 @@ def run_batched(args, device):
                                                                                         for o in outs)),
             "mean_iterations": float(its.mean()), "max_iterations": float(its.max()),
             "total_entries": float(mn.sum()), "effective_gbs": alg / sec / 1e9, "peak": peak,
-            "effective_frac": alg / sec / 1e9 / peak}
+            "effective_frac": alg / sec / 1e9 / peak, "configuration": best,
+            "autotune_256_iterations": [{**c, "seconds": t} for c, t in timings]}
 
 
 def run_learned(args, device):

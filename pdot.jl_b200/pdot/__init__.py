@@ -34,5 +34,6 @@ from .api import (  # noqa: F401
     optimize,
     optimize_batched,
     termination_reason_to_string,
+    tune_batched,
 )
 from .solve import default_parameters, rounding, solve_instance_and_output, warm_up, write_vector_to_file  # noqa: F401

@@ -646,3 +646,26 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
         out.append(SaddlePointOutput(X, u, v, reason, termination_reason_to_string(reason),
                                      int(outs[k].iteration_count), [stats_from_c(outs[k].final_stats)]))
     return out, sec.value
+
+
+BATCH_TUNING_CANDIDATES = [{"primal_pass": pp, "ctas_per_sm": c} for pp in ("staged", "direct") for c in (2, 1)]
+
+
+def tune_batched(params: PdhgParameters, problems, *, cost: str = "f32", points=None, device: int = 0,
+                 iterations: int = 256, candidates=None):
+    """The batched solver's autotuner: times the first `iterations` iterations
+    of the batch under every candidate launch configuration (the primal pass,
+    staged by bulk copies or direct, and the resident CTAs per SM of the
+    matrix passes) and returns (best configuration, [(configuration,
+    seconds)]). Pass the configuration's keys to optimize_batched."""
+    import copy
+
+    p = copy.deepcopy(params)
+    p.termination_criteria.iteration_limit = int(iterations)
+    timings = []
+    for cand in candidates or BATCH_TUNING_CANDIDATES:
+        _, sec = optimize_batched(p, problems, cost=cost, points=points, device=device, return_primal=False,
+                                  **cand)
+        timings.append((dict(cand), sec))
+    best = min(timings, key=lambda t: t[1])[0]
+    return best, timings

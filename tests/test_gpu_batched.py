@@ -117,3 +117,12 @@ def test_batched_staged_and_direct_passes_agree(cuda, cost):
         assert x.iteration_count == y.iteration_count
         assert np.array_equal(x.primal_solution, y.primal_solution)
         assert np.array_equal(x.dual_source_solution, y.dual_source_solution)
+
+
+def test_autotuner_times_every_candidate_and_picks_the_fastest(cuda):
+    probs, pts = instances.batched_l1(count=12, lo=32, hi=400, seed=2)
+    best, timings = pdot.tune_batched(pdot.default_parameters(1e-4), probs, cost="l1", points=pts, iterations=64)
+    assert len(timings) == len(pdot.api.BATCH_TUNING_CANDIDATES)
+    assert best == min(timings, key=lambda t: t[1])[0]
+    outs, _ = pdot.optimize_batched(pdot.default_parameters(1e-4), probs, cost="l1", points=pts, **best)
+    assert all(o.termination_reason == OPTIMAL for o in outs)

@@ -15,6 +15,7 @@ import json
 import math
 import os
 import sys
+from decimal import Decimal
 from dataclasses import asdict
 
 import numpy as np
@@ -23,23 +24,29 @@ from . import api
 
 
 def julia_float_str(x: float) -> str:
-    """Float64 text as Julia's `println` writes it: shortest round-trip digits,
-    scientific below 1e-4 with Julia's exponent style (0.25, 1.0e-5, 3.0).
-    Python's repr uses the same digits and the same small-number threshold."""
+    """Float64 text as Julia writes it (`println`, and JSON3 through the same
+    `Base.Ryu.writeshortest`): the shortest round-trip digits, in fixed
+    notation when 1e-4 <= |x| < 1e6 (decimal point position pt with
+    -4 < pt <= 6) and as d.ddde±x otherwise (0.25, 100000.0, 1.0e6, 1.0e-5,
+    1.234567e8); `Inf`, `-Inf`, `NaN`. Python's repr gives the same digits."""
     x = float(x)
     if math.isnan(x):
         return "NaN"
     if math.isinf(x):
         return "Inf" if x > 0 else "-Inf"
-    r = repr(x)
-    if "e" in r:
-        mant, ex = r.split("e")
-        if "." not in mant:
-            mant += ".0"
-        return f"{mant}e{int(ex)}"
-    if "." not in r:
-        r += ".0"
-    return r
+    if x == 0.0:
+        return "-0.0" if math.copysign(1.0, x) < 0 else "0.0"
+    sign, digits, exponent = Decimal(repr(x)).normalize().as_tuple()
+    ds = "".join(str(d) for d in digits)
+    pt = len(ds) + exponent  # digits before the decimal point
+    neg = "-" if sign else ""
+    if -4 < pt <= 6:
+        if pt <= 0:
+            return f"{neg}0.{'0' * (-pt)}{ds}"
+        if pt >= len(ds):
+            return f"{neg}{ds}{'0' * (pt - len(ds))}.0"
+        return f"{neg}{ds[:pt]}.{ds[pt:]}"
+    return f"{neg}{ds[0]}.{ds[1:] or '0'}e{pt - 1}"
 
 
 def write_vector_to_file(filename: str, vector) -> None:
@@ -97,18 +104,31 @@ def warm_up(ot: api.OptimalTransportProblem, tolerance: float = 1.0e-4) -> None:
     api.optimize(params, ot)
 
 
-def _jsonable(obj):
+def _json3(obj) -> str:
+    """JSON text as JSON3.write(x; allow_inf = true) writes it: compact, fields
+    in declaration order, enums by name, floats in Julia's shortest form."""
     if isinstance(obj, dict):
-        return {k: _jsonable(v) for k, v in obj.items()}
-    if isinstance(obj, list):
-        return [_jsonable(v) for v in obj]
+        return "{" + ",".join(f"{json.dumps(k, ensure_ascii=False)}:{_json3(v)}" for k, v in obj.items()) + "}"
+    if isinstance(obj, (list, tuple)):
+        return "[" + ",".join(_json3(v) for v in obj) + "]"
+    if isinstance(obj, bool):
+        return "true" if obj else "false"
     if hasattr(obj, "name") and hasattr(obj, "value") and isinstance(obj, int):
-        return obj.name  # enums serialise as their names (StructTypes' StringType)
-    return obj
+        return json.dumps(obj.name)  # enums serialise as their names (StructTypes' StringType)
+    if isinstance(obj, (int, np.integer)):
+        return str(int(obj))
+    if isinstance(obj, (float, np.floating)):
+        return julia_float_str(float(obj))
+    if isinstance(obj, str):
+        return json.dumps(obj, ensure_ascii=False)
+    if obj is None:
+        return "null"
+    raise TypeError(f"cannot write {type(obj).__name__} as JSON")
 
 
 def solve_log_json(log: api.SolveLog) -> str:
-    return json.dumps(_jsonable(asdict(log)), allow_nan=True)
+    """src/solve_log.jl:256-327 serialised as scripts/solve.jl:100-112 writes it."""
+    return _json3(asdict(log))
 
 
 def solve_instance_and_output(output_directory: str, instance_name: str,

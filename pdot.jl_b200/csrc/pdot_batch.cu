@@ -314,7 +314,8 @@ struct BatchStagedLayout {
 struct BatchCursor {
   int kk, k, buf;
   bool first, valid;
-  long long ql1, n, p, j, je, ld, x_off;  // the current instance, as its copies need it
+  int n, p, j, je, ld, ql1;  // local to the current instance (units of one instance fit 32 bits)
+  long long x_off;
   __device__ __forceinline__ void init(const BatchBuffers& B, int count, long long q0, long long q1, int w) {
     kk = find_segment(B.unit_prefix, count, q0);
     valid = true;
@@ -335,16 +336,16 @@ struct BatchCursor {
       }
       k = B.ids[kk];
       const BatchInstance& I = B.inst[k];
-      n = I.n;
-      ld = I.ld;
+      n = (int)I.n;
+      ld = (int)I.ld;
       x_off = I.x_off;
       buf = B.st[k].buf;
       first = !(B.st[k].sum_weights > 0.0);
       const long long ql0 = (first_segment ? q0 : base) - base;
       const long long end = B.unit_prefix[kk + 1];
-      ql1 = (q1 < end ? q1 : end) - base;
-      p = ql0 / n;
-      const long long jb = ql0 - p * n;
+      ql1 = (int)((q1 < end ? q1 : end) - base);
+      p = (int)(ql0 / n);
+      const int jb = (int)(ql0 - (long long)p * n);
       je = (ql1 < (p + 1) * n ? ql1 : (p + 1) * n) - p * n;
       j = jb + w;
       if (normalize_panels(w)) return;
@@ -396,22 +397,23 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
 
   // lane 0 fills stage t with the producer cursor's unit
   auto issue = [&](const BatchCursor& c, int t) {
-    const long long row0 = c.p * kPanelRows;
-    const long long rows = (c.ld - row0) < kPanelRows ? (c.ld - row0) : kPanelRows;
+    const long long row0 = (long long)c.p * kPanelRows;
+    const long long rows = ((long long)c.ld - row0) < kPanelRows ? ((long long)c.ld - row0) : kPanelRows;
     const uint32_t xb = (uint32_t)(rows * 4);
     const uint32_t cb = L::kPts ? 0u : xb;
     const uint32_t bar = bar0 + 8 * t;
     unsigned char* stg = ring + (size_t)t * L::kStageBytes;
-    const long long off = c.j * c.ld + row0;
+    const long long off = (long long)c.j * c.ld + row0;
     mbar_expect_tx(bar, cb + xb + (c.first ? 0u : xb));
     if (!L::kPts) bulk_g2s(smem_u32(stg), B.C + c.x_off + off, cb, bar);
     bulk_g2s(smem_u32(stg + L::kCBytes), B.X[c.buf] + c.x_off + off, xb, bar);
     if (!c.first) bulk_g2s(smem_u32(stg + L::kCBytes + L::kXBytes), B.X[c.buf ^ 1] + c.x_off + off, xb, bar);
   };
 
-  BatchCursor prod, cons;
+  // the producer walks the warp's units ahead of the consumer, which visits
+  // them in the same order through the structured loops below
+  BatchCursor prod;
   prod.init(B, act.count, q0, q1, warp);
-  cons.init(B, act.count, q0, q1, warp);
   long long issued = 0, consumed = 0;
   for (int t = 0; t < S && prod.valid; ++t) {
     if (lane == 0) issue(prod, t);
@@ -431,9 +433,10 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
     const double tau = st->step_size, omega = st->primal_weight, Ssum = st->sum_weights;
     const bool zero_g = st->g_is_zero != 0;
     const bool first = !(Ssum > 0.0);
-    const double s = __ddiv_rn(tau, omega);
-    const double nw = first ? 1.0 : __ddiv_rn(tau, Ssum);
-    const double aw = first ? 1.0 : __ddiv_rn(Ssum, __dadd_rn(Ssum, tau));
+    // the FP32 plan's entry arithmetic takes its step weights in FP32
+    const float s = (float)__ddiv_rn(tau, omega);
+    const float nw = first ? 1.0f : (float)__ddiv_rn(tau, Ssum);
+    const float aw = first ? 1.0f : (float)__ddiv_rn(Ssum, __dadd_rn(Ssum, tau));
     float* __restrict__ X = B.X[buf] + I.x_off;
     float* __restrict__ Xa = B.X[buf ^ 1] + I.x_off;
     const double* __restrict__ u = B.u[buf] + I.row_off;
@@ -462,8 +465,9 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
         }
       }
       cost.panel(row0, lane, I.m, ok);
-      while (!failed && cons.valid && cons.kk == kk && cons.p == p) {
-        const long long j = cons.j;
+      const long long jb = (ql0 > p * I.n ? ql0 : p * I.n) - p * I.n;
+      const long long je = (ql1 < (p + 1) * I.n ? ql1 : (p + 1) * I.n) - p * I.n;
+      for (long long j = jb + warp; !failed && j < je; j += kWarps) {
         const int stage = (int)(consumed % S);
         const uint32_t parity = (uint32_t)((consumed / S) & 1);
         if (!mbar_wait_bounded(bar0 + 8 * stage, parity)) {
@@ -513,7 +517,6 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
         if (lane == 0) B.colpart[base_u + p * I.n + j] = cs;
         __syncwarp();
         ++consumed;
-        cons.advance(B, act.count, q0, q1, warp);
         if (prod.valid) {
           if (lane == 0) issue(prod, stage);
           prod.advance(B, act.count, q0, q1, warp);

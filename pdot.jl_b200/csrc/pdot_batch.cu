@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
                                       xv[ju][kq][e], av[ju][kq][e], d);
                   acc[kq][e] += d;
                   cs += d;
-                  sq += d * d;
+                  sq = __fma_rn(d, d, sq);
                 } else {  // padded row
                   xv[ju][kq][e] = 0.0f;
                   av[ju][kq][e] = 0.0f;
@@ -503,7 +503,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
                 primal_entry<float>(widen(cv[e]), ur[kq][e], vj, s, nw, aw, zero_g, first, xv[e], av[e], d);
                 acc[kq][e] += d;
                 cs += d;
-                sq += d * d;
+                sq = __fma_rn(d, d, sq);
               } else {  // padded row
                 xv[e] = 0.0f;
                 av[e] = 0.0f;

@@ -251,7 +251,7 @@ struct CostReader {
 #pragma unroll
       for (int d = 0; d < DIM; ++d) {
         const float t = xr[k][e][d] - yr[d];
-        acc = kL1 ? acc + fabsf(t) : acc + t * t;
+        acc = kL1 ? acc + fabsf(t) : __fmaf_rn(t, t, acc);  // coordinate costs serve FP32 plans only
       }
       c[e] = acc * scale;
     }
@@ -287,11 +287,21 @@ struct CostReader<PDOT_COST_BF16, R, RPL> : StoredCost<__nv_bfloat16, R, RPL> {
 //
 // FP32 plan (mixed precision): the entry's arithmetic runs in FP32, the
 // plan's own precision (the cost entry is FP32 or BF16 storage or computed in
-// FP32; the duals and step weights are rounded to FP32 once). The step d
-// between the two stored values is formed exactly in FP64, so the FP64 row,
-// column and squared-norm sums the caller accumulates add exactly what was
-// stored.
+// FP32; the duals and step weights are rounded to FP32 once), with fused
+// multiply-adds where the drop-in rounds twice. The step d between the two
+// stored values is formed exactly in FP64, so the FP64 row, column and
+// squared-norm sums the caller accumulates add exactly what was stored.
 __device__ __forceinline__ float jl_max0f(float x) { return x > 0.0f ? x : (x != x ? x : 0.0f); }
+
+// The sum of squared steps: the FP64 plan rounds the product and the sum as
+// the reference does; an FP32 plan's sum takes one fused multiply-add.
+template <typename TX>
+__device__ __forceinline__ void add_sq(double& sq, double d) {
+  if constexpr (sizeof(TX) == 8)
+    sq += d * d;
+  else
+    sq = __fma_rn(d, d, sq);
+}
 
 template <typename TX>
 __device__ __forceinline__ void primal_entry(double c, double ui, double vj, double s, double nw, double aw,
@@ -307,10 +317,10 @@ __device__ __forceinline__ void primal_entry(double c, double ui, double vj, dou
   } else {
     const float x = xs;
     const float gg = zero_g ? 0.0f : __fsub_rn(__fsub_rn((float)c, (float)ui), (float)vj);
-    const float t = jl_max0f(__fsub_rn(x, __fmul_rn((float)s, gg)));
+    const float t = jl_max0f(__fmaf_rn(-(float)s, gg, x));
     d = __dsub_rn((double)t, (double)x);
     xs = t;
-    xas = first ? t : __fmul_rn(__fadd_rn(xas, __fmul_rn(t, (float)nw)), (float)aw);
+    xas = first ? t : __fmul_rn(__fmaf_rn(t, (float)nw, xas), (float)aw);
   }
 }
 

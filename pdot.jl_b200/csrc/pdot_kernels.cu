@@ -101,7 +101,7 @@ __device__ __forceinline__ void primal_pass_body(const CostSource& csrc, float s
             primal_entry<TX>(widen(cv[k][e]), ur[k][e], vj, s, nw, aw, zero_g, first, xv[k][e], av[k][e], d);
             acc[k][e] += d;
             cs += d;
-            sq += d * d;
+            add_sq<TX>(sq, d);
           }
           const int64_t idx = base + k * 32 * R;
           vst<TX, R>(X + idx, xv[k]);
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(kThreads, 2) k1_primal_staged(Buffers B, Geome
             primal_entry<TX>(widen(cv[e]), ur[k][e], vj, s, nw, aw, zero_g, first, xv[e], av[e], d);
             acc[k][e] += d;
             cs += d;
-            sq += d * d;
+            add_sq<TX>(sq, d);
           }
           vst<TX, R>(X + base + k * 32 * R, xv);
           vst<TX, R>(Xa + base + k * 32 * R, av);

@@ -529,6 +529,8 @@ def run_ours(args, world, rank, local):
         else:
             prob = pdot.OptimalTransportProblem(C_host.numpy().T, a_h, b_h)
         eparams = pdot.default_parameters(TOL, iteration_limit=args.steps)
+        # one untimed call first, as the warm-up steps of the primary region
+        pdot.optimize(pdot.default_parameters(TOL, iteration_limit=max(args.warmup, 1)), prob, device=local, **ekw)
         torch.cuda.synchronize()
         barrier(world)
         w0 = time.perf_counter()
@@ -542,8 +544,9 @@ def run_ours(args, world, rank, local):
                "h2d_bytes_per_step": h2d / max(out.iteration_count, 1),
                "d2h_bytes_per_step": (8 * N + vec_bytes) / max(out.iteration_count, 1),
                "iterations_per_call": out.iteration_count, "seconds_per_call": e_sec,
-               "note": "one pdot.optimize call: H2D of C, a, b from pinned memory, the solve, "
-                       "D2H of the returned plan and duals; bytes amortised per iteration"}
+               "note": "one pdot.optimize call after one untimed call: H2D of C, a, b from pinned memory, "
+                       "the solve, D2H of the returned plan and duals into fresh host arrays; bytes "
+                       "amortised per iteration"}
         del C_host
 
     mixed = None

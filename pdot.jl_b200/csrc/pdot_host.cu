@@ -10,6 +10,7 @@
 // device state record (a 200-byte copy) and the new iteration-stats records,
 // and stops once the device has set `done`. All decisions (step size, restart,
 // primal weight, termination) are taken on the device.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -17,6 +18,7 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "pdot_common.cuh"
@@ -543,8 +545,33 @@ class Solver {
     sync_all(issued, completed);
   }
 
+  // The caller's plan buffer is overwritten in full; fresh host memory (a
+  // numpy zeros array, a plain malloc) pays a page fault per 4 KB page on its
+  // first write, which for a large plan costs more than the copy itself. Host
+  // threads therefore write it once while the GPU iterates; the copy back
+  // then finds the pages present.
+  struct Prefault {
+    std::vector<std::thread> threads;
+    Prefault(double* p, size_t count) {
+      if (!p || count < (size_t(1) << 22)) return;  // small plans: not worth a thread
+      const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+      const size_t parts = std::min<size_t>(8, std::max<size_t>(1, hw / 2));
+      const size_t per = (count + parts - 1) / parts;
+      for (size_t k = 0; k < parts; ++k) {
+        const size_t lo = k * per, hi = std::min(count, lo + per);
+        if (lo < hi) threads.emplace_back([p, lo, hi] { memset(p + lo, 0, (hi - lo) * sizeof(double)); });
+      }
+    }
+    ~Prefault() {
+      for (std::thread& t : threads) t.join();
+    }
+  };
+
   void finish(pdot_saddle_point_output* out) {
-    while (!status_.done) iterate(int64_t(1) << 40);
+    {
+      Prefault touch(out->primal_solution, (size_t)g_.m * (size_t)g_.n);
+      while (!status_.done) iterate(int64_t(1) << 40);
+    }
     // gpu_to_cpu!, src/io.jl:41-53 (average, or current if no average exists)
     const int xb = status_.out_current ? status_.buf : (status_.buf ^ 1);
     const size_t N = (size_t)g_.m * (size_t)g_.n;

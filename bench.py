@@ -39,9 +39,10 @@ METRIC = "time-to-KKT≤1e-4 and PDHG iters/s at n=20000 (plain vs MP+warm-start
 UNIT = "iters/s"
 M_ROWS, N_COLS, SEED, TOL = 20000, 15000, 0, 1e-4
 FALLBACK_HBM_GBS = 6650.0
-# DRAM bytes per matrix entry of one fused primal pass, from the ncu capture
-# summarised in profiles/k1_primal_fp64.md (None until captured).
-K1_DRAM_BYTES_PER_ENTRY = None
+# DRAM bytes over algorithmic bytes of one full-size fused primal pass, from the
+# one-pass ncu capture in profiles/dram_traffic_full_size.md (9.578 GB measured for
+# 9.600 GB algorithmic, FP64; 3.554 GB for 3.600 GB, FP32 plan with coordinate cost).
+K1_TRAFFIC_RATIO = {"f64": 9578004224 / 9.6e9, "sqeuclid": 3554418944 / 3.6e9}
 CPU_SAMPLE_ROWS = 500  # row slice of the instance timed on the host cores
 
 
@@ -515,7 +516,8 @@ def run_ours(args, world, rank, local):
     k1_avg_s = k1_ms / 1000.0 / max(k1_launches, 1)
     achieved = per_launch_bytes / k1_avg_s / 1e9
     peak, peak_kind = read_peak()
-    traffic = (K1_DRAM_BYTES_PER_ENTRY * N) if K1_DRAM_BYTES_PER_ENTRY else None
+    ratio = K1_TRAFFIC_RATIO.get("f64" if precision == "f64" else cost) if (m, n) == (M_ROWS, N_COLS) else None
+    traffic = per_launch_bytes * ratio if ratio else None
 
     # ---- end to end through the public API, host buffers ----
     e2e = None
@@ -574,6 +576,9 @@ def run_ours(args, world, rank, local):
                    "cuda_graph_chunks": True},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch "
+                                       "(profiles/dram_traffic_full_size.md): measured/algorithmic ratio times "
+                                       "this region's algorithmic bytes per launch" if traffic else None,
                      "kernel": "k1_primal (fused primal pass)",
                      "algorithmic_bytes_per_entry": full_bytes,
                      "algorithmic_bytes_per_launch": per_launch_bytes,

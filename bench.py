@@ -352,9 +352,10 @@ def run_mixed(args, params, m, n, Ct, a, b, xs_d, ys_d, device, local, fp64_obj)
             alg = N * (16.0 * (passes - fresh) + 12.0 * fresh) / max(passes, 1)
             avg_s = k1_ms / 1000.0 / max(launches, 1)
             peak, _ = read_peak()
+            ratio = K1_TRAFFIC_RATIO["sqeuclid"] if (m, n) == (M_ROWS, N_COLS) else None
             entry["roofline"] = {"achieved": alg / avg_s / 1e9, "peak": peak, "unit": "GB/s",
                                  "frac": alg / avg_s / 1e9 / peak, "algorithmic_bytes_per_launch": alg,
-                                 "avg_launch_ms": avg_s * 1000.0}
+                                 "avg_launch_ms": avg_s * 1000.0, "traffic": alg * ratio if ratio else None}
         entry["bytes_per_entry"] = bytes_per_entry[cost]
         out[cost] = entry
     return out

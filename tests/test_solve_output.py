@@ -50,17 +50,33 @@ def test_vector_file_is_column_major_julia_text(tmp_path):
     assert f.read_text() == "1.0\n3.0e6\n2.5e-6\n-0.5\n"
 
 
+def _julia_json(text):
+    """json.loads of JSON3 text with allow_inf (bare Inf / -Inf / NaN)."""
+    import re
+
+    text = re.sub(r'(?<=[:\[,])(-?)Inf(?=[,\]}])', r'\1Infinity', text)
+    return json.loads(text)
+
+
+def test_julia_json_reader_reads_non_finite_values():
+    log = api.SolveLog()
+    log.solve_time_sec = math.inf
+    text = solve.solve_log_json(log)
+    assert '"solve_time_sec":Inf,' in text
+    assert _julia_json(text)["solve_time_sec"] == math.inf
+
+
 @pytest.mark.gpu
 def test_solve_instance_and_output_writes_the_scripts_files(cuda, tmp_path):
     prob = instances.uniform_sqeuclid(30, 20, seed=1)
     out = pdot.solve_instance_and_output(str(tmp_path), "t", prob, tolerance=1e-4)
     names = sorted(os.listdir(tmp_path))
     assert names == ["t_dual.txt", "t_full_log.json.gz", "t_primal.txt", "t_primal_rounded.txt", "t_summary.json"]
-    summary = json.loads((tmp_path / "t_summary.json").read_text())
+    summary = _julia_json((tmp_path / "t_summary.json").read_text())
     assert summary["termination_reason"] == "TERMINATION_REASON_OPTIMAL"
     assert summary["iteration_count"] == out.iteration_count and summary["iteration_stats"] == []
     with gzip.open(tmp_path / "t_full_log.json.gz", "rt") as io:
-        full = json.loads(io.read())
+        full = _julia_json(io.read())
     assert len(full["iteration_stats"]) == len(out.iteration_stats)
     primal = np.loadtxt(tmp_path / "t_primal.txt")
     np.testing.assert_array_equal(primal, out.primal_solution.ravel(order="F"))

@@ -85,3 +85,63 @@ def test_packaged_model_loads():
     assert model.parameters.size == H * I + H + H * H + H + O * H + O
     assert np.all(np.isfinite(model.parameters))
     assert 0 < model.target_scale < 1
+
+
+def test_tight_duals_are_feasible_and_c_conjugate():
+    side = 6
+    rng = np.random.default_rng(11)
+    C = pdot.instances.grid_cost(side)
+    u = rng.normal(0, 0.1, side * side)
+    v = rng.normal(0, 0.1, side * side)
+    v[3] = -50.0  # a loose dual, as PDHG leaves them on rows of tiny mass
+    ut, vt = learned.tight_duals(u, v, C)
+    G = C - ut[:, None] - vt[None, :]
+    assert G.min() >= -1e-12                                   # feasible
+    np.testing.assert_allclose(ut, (C - vt[None, :]).min(axis=1), atol=1e-12)  # u = v^c
+    np.testing.assert_allclose(vt, (C - ut[:, None]).min(axis=0), atol=1e-12)  # v = u^c
+    assert abs(ut.mean() - vt.mean()) < 1e-12                  # canonical shift
+    assert np.abs(np.concatenate([ut, vt])).max() <= C.max() + 1.0
+
+
+def test_dataset_expands_each_optimal_instance_into_16_images():
+    data = {"seeds": np.array([5, 6, 7]), "reasons": np.array([1, 3, 1]),
+            "u": np.zeros((3, learned.BINS)), "v": np.zeros((3, learned.BINS)),
+            "iterations": np.array([1, 2, 3]), "seconds": 0.0}
+    hist, duals = learned.dataset(data)
+    assert hist.shape == (32, 2 * learned.BINS) and duals.shape == (32, 2 * learned.BINS)  # instance 6 dropped
+    a, b = learned.grid_pair(5)
+    np.testing.assert_array_equal(hist[0], np.concatenate([a, b]))
+    np.testing.assert_array_equal(hist[1], np.concatenate([b, a]))
+
+
+def test_model_save_load_roundtrip(tmp_path):
+    I, H, O = 2 * learned.BINS, 128, 2 * learned.BINS
+    P = H * I + H + H * H + H + O * H + O
+    rng = np.random.default_rng(0)
+    theta = rng.standard_normal(P).astype(np.float32) * 0.02
+    model = learned.WarmStartModel(theta, -0.03, 0.11, hidden_dim=H)
+    path = str(tmp_path / "m.npz")
+    model.save(path)
+    back = learned.WarmStartModel.load(path)
+    assert back.hidden_dim == H and back.target_mean == -0.03 and back.target_scale == 0.11
+    sizes = [H * I, H, H * H, H, O * H, O]
+    off = 0
+    for k, s in enumerate(sizes):
+        seg, got = theta[off:off + s], back.parameters[off:off + s]
+        if k % 2 == 0:  # weights: their BF16 values
+            np.testing.assert_array_equal(got, mo.bf16(seg).astype(np.float32))
+        else:           # biases: FP32 as they were
+            np.testing.assert_array_equal(got, seg)
+        off += s
+
+
+def test_summarize_counts_race_results():
+    res = {"cold_iterations": [100, 200, 300, 400], "warm_iterations": [50, 250, 100, 400],
+           "cold_seconds": 2.0, "warm_seconds": 1.0, "predict_seconds": 0.1,
+           "cold_reasons": [1, 1, 1, 1], "warm_reasons": [1, 1, 1, 3],
+           "dual_rel_error": [0.1, 0.2, 0.3, 0.4], "warm_work_iterations": [100, 400, 200, 800],
+           "race_winner_warm": [True, False, True, False]}
+    s = learned.summarize(res)
+    assert s["cold_mean_iterations"] == 250 and s["warm_mean_iterations"] == 200
+    assert s["warm_better_fraction"] == 0.5 and s["race_warm_wins"] == 2
+    assert s["warm_optimal"] == 3 and s["warm_work_mean_iterations"] == 375

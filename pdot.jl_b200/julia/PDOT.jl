@@ -12,7 +12,6 @@ GPU with no Julia-side device code and no CPU fallback.
 """
 module PDOT
 
-import LinearAlgebra
 import Printf
 import StructTypes
 
@@ -244,6 +243,50 @@ struct CIterationStats
     time_spent_doing_basic_algorithm::Float64
 end
 
+struct CSolverOptions                           # pdot_solver_options
+    device::Int32
+    use_cuda_graph::Int32
+    time_kernels::Int32
+    plan_precision::Int32
+    cost_storage::Int32
+    point_dim::Int32
+    source_points::Ptr{Float32}
+    target_points::Ptr{Float32}
+    cost_scale::Float64
+    warm_dual_source::Ptr{Float64}
+    warm_dual_target::Ptr{Float64}
+    primal_pass::Int32
+    ctas_per_sm::Int32
+    warm_primal::Ptr{Float64}
+    warm_plan_epsilon::Float64
+    warm_plan_iterations::Int32
+    reserved::NTuple{1,Int32}
+end
+
+struct CBatchProblem                            # pdot_batch_problem
+    num_instances::Int64
+    num_rows::Ptr{Int64}
+    num_cols::Ptr{Int64}
+    cost_matrices::Ptr{Ptr{Float64}}
+    source_distributions::Ptr{Ptr{Float64}}
+    target_distributions::Ptr{Ptr{Float64}}
+    source_points::Ptr{Ptr{Float32}}
+    target_points::Ptr{Ptr{Float32}}
+    warm_dual_sources::Ptr{Ptr{Float64}}
+    warm_dual_targets::Ptr{Ptr{Float64}}
+    warm_primals::Ptr{Ptr{Float64}}
+    race_groups::Ptr{Int32}
+end
+
+struct CBatchOutput                             # pdot_batch_output
+    primal_solution::Ptr{Float64}
+    dual_source_solution::Ptr{Float64}
+    dual_target_solution::Ptr{Float64}
+    termination_reason::Int32
+    iteration_count::Int32
+    final_stats::CIterationStats
+end
+
 mutable struct COutput
     primal_solution::Ptr{Float64}
     dual_source_solution::Ptr{Float64}
@@ -288,20 +331,56 @@ end
 
 last_error() = unsafe_string(ccall((:pdot_last_error, libpdot), Cstring, ()))
 
+# Options of this implementation beyond the reference (include/pdot.h):
+# precision :f64 (the drop-in) or :f32 (FP32 plan); cost :f64, :f32, :bf16,
+# :sqeuclid or :l1 (the last two from `points`, a tuple of Float32 matrices
+# m x dim and n x dim, one point per row); warm_start (u0, v0) or (u0, v0, X0);
+# recover_plan (eps, rounds) recovers X0 from (u0, v0).
+const PRECISIONS = Dict(:f64 => Int32(0), :f32 => Int32(1))
+const COSTS = Dict(:f64 => Int32(0), :f32 => Int32(1), :bf16 => Int32(2), :sqeuclid => Int32(3), :l1 => Int32(4))
+
+function solver_options(; device::Integer = 0, precision::Symbol = :f64, cost::Union{Symbol,Nothing} = nothing,
+                        point_dim::Integer = 0, source_points::Ptr{Float32} = Ptr{Float32}(0),
+                        target_points::Ptr{Float32} = Ptr{Float32}(0), u0::Ptr{Float64} = Ptr{Float64}(0),
+                        v0::Ptr{Float64} = Ptr{Float64}(0), X0::Ptr{Float64} = Ptr{Float64}(0),
+                        recover_plan = nothing, primal_pass::Integer = 0, ctas_per_sm::Integer = 0)
+    c = cost === nothing ? (precision == :f64 ? :f64 : :f32) : cost
+    eps, rounds = recover_plan === nothing ? (0.0, 0) : (Float64(recover_plan[1]), Int(recover_plan[2]))
+    return CSolverOptions(Int32(device), Int32(1), Int32(0), PRECISIONS[precision], COSTS[c], Int32(point_dim),
+                          source_points, target_points, 0.0, u0, v0, Int32(primal_pass), Int32(ctas_per_sm), X0,
+                          eps, Int32(rounds), (Int32(0),))
+end
+
+# points are given one per row (m x dim); the C ABI reads them row-major
+row_major(P::AbstractMatrix) = Matrix{Float32}(permutedims(P))
+
 """
-    optimize(params::PdhgParameters, original_problem::OptimalTransportProblem) -> SaddlePointOutput
+    optimize(params::PdhgParameters, original_problem::OptimalTransportProblem; kwargs...) -> SaddlePointOutput
 
 src/solver_gpu.jl:413-720, run by libpdot.so on the GPU. Raises where the
-reference raises (`primal_importance`, src/solver_gpu.jl:420-422).
+reference raises (`primal_importance`, src/solver_gpu.jl:420-422). Without
+keywords this is the FP64 drop-in; the keywords (`precision`, `cost`,
+`points`, `warm_start`, `recover_plan`, `device`) select this implementation's
+mixed precision and warm starts.
 """
-function optimize(params::PdhgParameters, original_problem::OptimalTransportProblem)
+function optimize(params::PdhgParameters, original_problem::OptimalTransportProblem;
+                  precision::Symbol = :f64, cost::Union{Symbol,Nothing} = nothing, points = nothing,
+                  warm_start = nothing, recover_plan = nothing, device::Integer = 0)
     if params.primal_importance <= 0 || !isfinite(params.primal_importance)
         error("primal_importance must be positive and finite")
     end
     C = original_problem.cost_matrix
     a = original_problem.source_distribution
     b = original_problem.target_distribution
-    nrow, ncol = size(C)
+    nrow, ncol = length(a), length(b)
+    plain = precision == :f64 && cost === nothing && points === nothing && warm_start === nothing &&
+            recover_plan === nothing && device == 0
+    xs = points === nothing ? Float32[] : row_major(points[1])
+    ys = points === nothing ? Float32[] : row_major(points[2])
+    dim = points === nothing ? 0 : size(points[1], 2)
+    u0 = warm_start === nothing ? Float64[] : Vector{Float64}(warm_start[1])
+    v0 = warm_start === nothing ? Float64[] : Vector{Float64}(warm_start[2])
+    X0 = (warm_start === nothing || length(warm_start) < 3) ? Float64[] : Matrix{Float64}(warm_start[3])
     primal = zeros(nrow, ncol)
     dual_source = zeros(nrow)
     dual_target = zeros(ncol)
@@ -310,16 +389,28 @@ function optimize(params::PdhgParameters, original_problem::OptimalTransportProb
     stats = Vector{CIterationStats}(undef, capacity)
     out = COutput()
     cparams = to_c(params)
-    GC.@preserve C a b primal dual_source dual_target stats begin
-        cprob = CProblem(nrow, ncol, pointer(C), pointer(a), pointer(b))
+    GC.@preserve C a b primal dual_source dual_target stats xs ys u0 v0 X0 begin
+        cprob = CProblem(nrow, ncol, isempty(C) ? Ptr{Float64}(0) : pointer(C), pointer(a), pointer(b))
         out.primal_solution = pointer(primal)
         out.dual_source_solution = pointer(dual_source)
         out.dual_target_solution = pointer(dual_target)
         out.iteration_stats = pointer(stats)
         out.iteration_stats_capacity = capacity
-        rc = ccall((:pdot_optimize, libpdot), Cint,
-                   (Ref{CProblem}, Ref{CPdhgParameters}, Ptr{Cvoid}, Ref{COutput}),
-                   cprob, cparams, C_NULL, out)
+        if plain
+            rc = ccall((:pdot_optimize, libpdot), Cint,
+                       (Ref{CProblem}, Ref{CPdhgParameters}, Ptr{Cvoid}, Ref{COutput}),
+                       cprob, cparams, C_NULL, out)
+        else
+            opts = solver_options(device = device, precision = precision, cost = cost, point_dim = dim,
+                                  source_points = isempty(xs) ? Ptr{Float32}(0) : pointer(xs),
+                                  target_points = isempty(ys) ? Ptr{Float32}(0) : pointer(ys),
+                                  u0 = isempty(u0) ? Ptr{Float64}(0) : pointer(u0),
+                                  v0 = isempty(v0) ? Ptr{Float64}(0) : pointer(v0),
+                                  X0 = isempty(X0) ? Ptr{Float64}(0) : pointer(X0), recover_plan = recover_plan)
+            rc = ccall((:pdot_optimize, libpdot), Cint,
+                       (Ref{CProblem}, Ref{CPdhgParameters}, Ref{CSolverOptions}, Ref{COutput}),
+                       cprob, cparams, opts, out)
+        end
         rc == 0 || error("pdot_optimize failed ($rc): ", last_error())
     end
     n = min(out.iteration_stats_count, capacity)
@@ -336,21 +427,87 @@ end
     rounding(problem, primal_solution)
 
 src/utils_gpu.jl:296-318: scale rows, then columns, onto the marginals and add
-the rank-one correction, making the plan feasible.
+the rank-one correction, making the plan feasible. Runs on the GPU
+(`pdot_rounding_host`), in place on `primal_solution`, which it returns, as the
+reference's `feas_solution` aliases it.
 """
-function rounding(problem::OptimalTransportProblem, primal_solution::Matrix{Float64})
-    feas_solution = primal_solution
-    tmp = map(x -> isnan(x) ? 0.0 : x, problem.source_distribution ./ vec(sum(feas_solution, dims = 2)))
-    feas_solution .= LinearAlgebra.Diagonal(vec(min.(tmp, 1.0))) * feas_solution
-    tmp = map(x -> isnan(x) ? 0.0 : x, problem.target_distribution ./ vec(sum(feas_solution, dims = 1)))
-    feas_solution .= feas_solution * LinearAlgebra.Diagonal(vec(min.(tmp, 1.0)))
-    err_r = problem.source_distribution .- vec(sum(feas_solution, dims = 2))
-    if LinearAlgebra.norm(err_r, 1) != 0.0
-        err_r ./= LinearAlgebra.norm(err_r, 1)
+function rounding(problem::OptimalTransportProblem, primal_solution::Matrix{Float64}; device::Integer = 0)
+    a, b = problem.source_distribution, problem.target_distribution
+    m, n = size(primal_solution)
+    GC.@preserve a b primal_solution begin
+        rc = ccall((:pdot_rounding_host, libpdot), Cint,
+                   (Int64, Int64, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int32),
+                   m, n, pointer(a), pointer(b), pointer(primal_solution), Int32(device))
+        rc == 0 || error("pdot_rounding_host failed ($rc): ", last_error())
     end
-    err_c = problem.target_distribution .- vec(sum(feas_solution, dims = 1))
-    feas_solution .+= err_r * err_c'
-    return feas_solution
+    return primal_solution
+end
+
+"""
+    optimize_batched(params, problems; cost = :f32, points = nothing, warm_starts = nothing,
+                     race_groups = nothing, recover_plan = nothing, device = 0)
+        -> (Vector{SaddlePointOutput}, seconds)
+
+Many independent instances of uneven sizes in one lockstep solve on the GPU
+(`pdot_optimize_batched`), each with its own step size, restarts and
+termination. `cost = :f32` stores each instance's cost matrix in FP32;
+`:sqeuclid` and `:l1` compute it from `points[k] = (xs, ys)` (one point per row).
+`warm_starts[k]` is `nothing`, `(u0, v0)` or `(u0, v0, X0)`; instances with the
+same `race_groups` id stop once one of them ends optimal. Each output's
+`iteration_stats` holds its final evaluation.
+"""
+function optimize_batched(params::PdhgParameters, problems::Vector{OptimalTransportProblem};
+                          cost::Symbol = :f32, points = nothing, warm_starts = nothing, race_groups = nothing,
+                          recover_plan = nothing, device::Integer = 0)
+    B = length(problems)
+    rows = Int64[length(p.source_distribution) for p in problems]
+    cols = Int64[length(p.target_distribution) for p in problems]
+    keep = Any[]
+    null64, null32 = Ptr{Float64}(0), Ptr{Float32}(0)
+    ptr(x) = (push!(keep, x); isempty(x) ? (eltype(x) == Float32 ? null32 : null64) : pointer(x))
+    costs = Ptr{Float64}[cost == :f32 ? ptr(p.cost_matrix) : null64 for p in problems]
+    srcs = Ptr{Float64}[ptr(p.source_distribution) for p in problems]
+    tgts = Ptr{Float64}[ptr(p.target_distribution) for p in problems]
+    xs = Ptr{Float32}[points === nothing ? null32 : ptr(row_major(points[k][1])) for k in 1:B]
+    ys = Ptr{Float32}[points === nothing ? null32 : ptr(row_major(points[k][2])) for k in 1:B]
+    dim = points === nothing ? 0 : size(points[1][1], 2)
+    wu = Ptr{Float64}[warm_starts === nothing || warm_starts[k] === nothing ? null64 :
+                      ptr(Vector{Float64}(warm_starts[k][1])) for k in 1:B]
+    wv = Ptr{Float64}[warm_starts === nothing || warm_starts[k] === nothing ? null64 :
+                      ptr(Vector{Float64}(warm_starts[k][2])) for k in 1:B]
+    wx = Ptr{Float64}[warm_starts === nothing || warm_starts[k] === nothing || length(warm_starts[k]) < 3 ?
+                      null64 : ptr(Matrix{Float64}(warm_starts[k][3])) for k in 1:B]
+    groups = race_groups === nothing ? Int32[] : Int32.(race_groups)
+    primals = [zeros(rows[k], cols[k]) for k in 1:B]
+    us = [zeros(rows[k]) for k in 1:B]
+    vs = [zeros(cols[k]) for k in 1:B]
+    outs = CBatchOutput[CBatchOutput(pointer(primals[k]), pointer(us[k]), pointer(vs[k]), Int32(0), Int32(0),
+                                     CIterationStats(Int32(0), CConvergenceInformation(Int32(0), ntuple(_ -> 0.0, 16)),
+                                                     0.0, Int32(0), 0.0, Int32(0), 0.0, 0.0, 0.0)) for k in 1:B]
+    seconds = Ref{Float64}(0.0)
+    opts = solver_options(device = device, precision = :f32, cost = cost, point_dim = dim,
+                          recover_plan = recover_plan)
+    GC.@preserve keep rows cols costs srcs tgts xs ys wu wv wx groups primals us vs outs begin
+        bp = CBatchProblem(B, pointer(rows), pointer(cols), cost == :f32 ? pointer(costs) : Ptr{Ptr{Float64}}(0),
+                           pointer(srcs), pointer(tgts),
+                           points === nothing ? Ptr{Ptr{Float32}}(0) : pointer(xs),
+                           points === nothing ? Ptr{Ptr{Float32}}(0) : pointer(ys),
+                           warm_starts === nothing ? Ptr{Ptr{Float64}}(0) : pointer(wu),
+                           warm_starts === nothing ? Ptr{Ptr{Float64}}(0) : pointer(wv),
+                           warm_starts === nothing ? Ptr{Ptr{Float64}}(0) : pointer(wx),
+                           isempty(groups) ? Ptr{Int32}(0) : pointer(groups))
+        rc = ccall((:pdot_optimize_batched, libpdot), Cint,
+                   (Ref{CBatchProblem}, Ref{CPdhgParameters}, Ref{CSolverOptions}, Ptr{CBatchOutput}, Ref{Float64}),
+                   bp, to_c(params), opts, outs, seconds)
+        rc == 0 || error("pdot_optimize_batched failed ($rc): ", last_error())
+    end
+    results = SaddlePointOutput[]
+    for k in 1:B
+        reason = TerminationReason(outs[k].termination_reason)
+        push!(results, SaddlePointOutput(primals[k], us[k], vs[k], reason, termination_reason_to_string(reason),
+                                         outs[k].iteration_count, [from_c(outs[k].final_stats)]))
+    end
+    return results, seconds[]
 end
 
 end # module PDOT

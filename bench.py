@@ -68,17 +68,10 @@ def parse():
 
 
 def host_instance(m, n, seed):
-    """Points and marginals (host, seeded), as pdot.instances.gauss_mixture draws them."""
-    import numpy as np
-
+    """Points and marginals (host, seeded): pdot.instances.gauss_mixture_instance."""
     from pdot import instances
 
-    rng = np.random.default_rng(seed)
-    xs = instances.gauss_mixture_points(rng, m)
-    ys = instances.gauss_mixture_points(rng, n)
-    a = rng.uniform(0.1, 1.0, size=m)
-    b = rng.uniform(0.1, 1.0, size=n)
-    return xs, ys, a / a.sum(), b / b.sum()
+    return instances.gauss_mixture_instance(m, n, seed)
 
 
 def device_cost(xs, ys, device):

@@ -49,6 +49,18 @@ def gauss_mixture_points(rng, k: int, components: int = 8, sigma: float = 0.05):
     return means[lab] + sigma * rng.standard_normal(size=(k, 2))
 
 
+def gauss_mixture_instance(m: int, n: int, seed: int = 0):
+    """(xs, ys, a, b) of the mixed-precision benchmark instance: points from a
+    2-D mixture of 8 Gaussians (sigma 0.05, means U[0,1]^2), marginals
+    U(0.1, 1) normalised; C = ||x - y||^2 / max, built from the points."""
+    rng = np.random.default_rng(seed)
+    xs = gauss_mixture_points(rng, m)
+    ys = gauss_mixture_points(rng, n)
+    a = rng.uniform(0.1, 1.0, size=m)
+    b = rng.uniform(0.1, 1.0, size=n)
+    return xs, ys, a / a.sum(), b / b.sum()
+
+
 def gauss_mixture(m: int, n: int, seed: int = 0) -> OptimalTransportProblem:
     rng = np.random.default_rng(seed)
     xs = gauss_mixture_points(rng, m)

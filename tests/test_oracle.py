@@ -171,3 +171,64 @@ def test_trajectory_sensitivity_to_one_ulp(built):
     assert pert.termination_reason == OPTIMAL
     assert pert.iteration_count != base.iteration_count
     assert abs(p - b) <= 2 * tol * (1 + abs(b))
+
+
+def _highs_objective(C, a, b):
+    """The exact OT optimum by scipy's HiGHS (an independent known answer)."""
+    from scipy.optimize import linprog
+
+    m, n = C.shape
+    A_eq = np.zeros((m + n, m * n))
+    for i in range(m):
+        A_eq[i, i::m] = 1.0           # column-major: entry (i, j) at i + j*m
+    for j in range(n):
+        A_eq[m + j, j * m:(j + 1) * m] = 1.0
+    res = linprog(C.ravel(order="F"), A_eq=A_eq, b_eq=np.concatenate([a, b]), bounds=(0, None), method="highs")
+    assert res.status == 0
+    return res.fun
+
+
+def test_zero_mass_rows_and_columns_reach_the_optimum(built):
+    """Marginals with zero entries (sources or targets that carry nothing)."""
+    rng = np.random.default_rng(21)
+    prob = instances.uniform_sqeuclid(14, 11, seed=21)
+    a = prob.source_distribution.copy()
+    b = prob.target_distribution.copy()
+    a[[2, 7]] = 0.0
+    b[[0, 5, 10]] = 0.0
+    a /= a.sum()
+    b /= b.sum()
+    tol = 1e-6
+    out = oracle.optimize(pdot.default_parameters(tol), pdot.OptimalTransportProblem(prob.cost_matrix, a, b))
+    assert out.termination_reason == OPTIMAL
+    opt = _highs_objective(prob.cost_matrix, a, b)
+    fin = out.iteration_stats[-1].convergence_information[0]
+    assert abs(fin.primal_objective - opt) <= 4 * tol * (1 + abs(opt))
+    del rng
+
+
+def test_l_inf_optimality_norm_reaches_the_optimum(built):
+    prob = instances.uniform_sqeuclid(12, 9, seed=5)
+    params = pdot.default_parameters(1e-6)
+    params.termination_criteria.optimality_norm = pdot.L_INF
+    out = oracle.optimize(params, prob)
+    assert out.termination_reason == OPTIMAL
+    opt = _highs_objective(prob.cost_matrix, prob.source_distribution, prob.target_distribution)
+    fin = out.iteration_stats[-1].convergence_information[0]
+    assert abs(fin.primal_objective - opt) <= 4e-6 * (1 + abs(opt))
+    assert fin.relative_l_inf_primal_residual <= 1e-6
+
+
+def test_exact_warm_start_ends_at_the_first_evaluation(built):
+    prob = instances.uniform_sqeuclid(20, 16, seed=6)
+    params = pdot.default_parameters(1e-5)
+    cold = oracle.optimize(params, prob)
+    warm = oracle.optimize_warm(params, prob, cold.dual_source_solution, cold.dual_target_solution,
+                                cold.primal_solution)
+    assert warm.termination_reason == OPTIMAL and warm.iteration_count == 0
+    # duals only: the plan starts at zero, the solve still ends at the optimum
+    duals = oracle.optimize_warm(params, prob, cold.dual_source_solution, cold.dual_target_solution)
+    assert duals.termination_reason == OPTIMAL
+    oc = cold.iteration_stats[-1].convergence_information[0].primal_objective
+    od = duals.iteration_stats[-1].convergence_information[0].primal_objective
+    assert abs(od - oc) <= 4e-5 * (1 + abs(oc))

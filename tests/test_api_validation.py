@@ -1,0 +1,60 @@
+"""Argument checks of the Python API that run before any device work (no GPU
+needed): shapes of warm starts and race groups, and how the options reach the
+C struct."""
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+import pdot
+from pdot import _abi, api, instances
+
+
+def _probs():
+    probs, pts = instances.batched_l1(3, 8, 20, seed=1)
+    return probs, pts
+
+
+def test_batched_warm_start_shape_is_checked():
+    probs, pts = _probs()
+    m = probs[0].source_distribution.size
+    bad = [(np.zeros(m + 1), np.zeros(probs[0].target_distribution.size)), None, None]
+    with pytest.raises(ValueError):
+        api.optimize_batched(pdot.default_parameters(1e-4), probs, cost="l1", points=pts, warm_starts=bad)
+
+
+def test_batched_race_groups_need_one_entry_per_instance():
+    probs, pts = _probs()
+    with pytest.raises(ValueError):
+        api.optimize_batched(pdot.default_parameters(1e-4), probs, cost="l1", points=pts, race_groups=[0, 0])
+
+
+def test_warm_plan_shape_is_checked():
+    with pytest.raises(ValueError):
+        api._options(0, True, warm_start=(np.zeros(4), np.zeros(3), np.zeros((3, 4))))
+
+
+def test_recovered_plan_and_warm_start_reach_the_options():
+    opts, keep = api._options(0, True, warm_start=(np.ones(4), np.ones(3)), recover_plan=(3e-4, 100))
+    assert opts.warm_plan_epsilon == 3e-4 and opts.warm_plan_iterations == 100
+    assert bool(opts.warm_dual_source) and bool(opts.warm_dual_target) and not bool(opts.warm_primal)
+    assert list(opts.reserved) == [0]
+    u0 = np.ctypeslib.as_array(opts.warm_dual_source, shape=(4,))
+    assert np.all(u0 == 1.0)
+    del keep
+
+
+def test_warm_plan_without_duals_is_rejected_before_device_work(built):
+    """The C entry validates options before it touches a device."""
+    prob = instances.uniform_sqeuclid(4, 3, seed=0)
+    lib = _abi.load()
+    mp = api.MarshalledProblem(prob)
+    cp = api.marshal_params(pdot.default_parameters(1e-4))
+    X0 = np.zeros((4, 3), order="F")
+    opts = _abi.SolverOptionsC()
+    opts.use_cuda_graph = 1
+    opts.warm_primal = X0.ctypes.data_as(ct.POINTER(ct.c_double))
+    ob = api.OutputBuffers(4, 3, 16)
+    rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
+    assert rc == _abi.PDOT_ERR_INVALID_ARGUMENT
+    assert "warm" in _abi.last_error(lib)

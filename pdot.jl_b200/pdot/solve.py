@@ -62,8 +62,6 @@ def rounding(problem: api.OptimalTransportProblem, primal_solution: np.ndarray, 
     """src/utils_gpu.jl:296-318, run on the GPU (pdot_rounding_host): scale the
     rows, then the columns, onto the marginals and add the rank-one correction.
     Like the reference it modifies `primal_solution` in place and returns it."""
-    import ctypes as ct
-
     from . import _abi
 
     X = primal_solution

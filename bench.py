@@ -39,11 +39,12 @@ METRIC = "time-to-KKT≤1e-4 and PDHG iters/s at n=20000 (plain vs MP+warm-start
 UNIT = "iters/s"
 M_ROWS, N_COLS, SEED, TOL = 20000, 15000, 0, 1e-4
 FALLBACK_HBM_GBS = 6650.0
-# DRAM bytes over algorithmic bytes of one full-size fused primal pass, from the
-# one-pass ncu capture in profiles/dram_traffic_full_size.md (9.578 GB measured for
-# 9.600 GB algorithmic, FP64; 3.554 GB for 3.600 GB, FP32 plan with coordinate cost).
+# DRAM bytes over algorithmic bytes of one full-size fused primal pass, from a
+# one-pass ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) on B200:
+# 9.578 GB measured for 9.600 GB algorithmic (FP64), 3.554 GB for 3.600 GB
+# (FP32 plan with the coordinate cost).
 K1_TRAFFIC_RATIO = {"f64": 9578004224 / 9.6e9, "sqeuclid": 3554418944 / 3.6e9}
-CPU_SAMPLE_ROWS = 500  # row slice of the instance timed on the host cores
+C1_SIZE, C2_SIZE = 1000, 10000  # the square configurations: U[0,1]^2 and U[0,1]^3 points
 
 
 def parse():
@@ -60,6 +61,8 @@ def parse():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start line (64 instances)")
     ap.add_argument("--batched-only", action="store_true", help="run only the batched-solver line and print it")
     ap.add_argument("--no-mp", action="store_true", help="skip the mixed-precision variants")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the m=n=1000 and m=n=10000 configuration blocks (c1, c2)")
     ap.add_argument("--precision", choices=["f64", "f32"], default="f64",
                     help="plan precision of the primary workload (f64: the drop-in)")
     ap.add_argument("--cost", choices=["f64", "f32", "bf16", "sqeuclid"], default=None,
@@ -155,42 +158,31 @@ def read_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def cpu_sample_problem(xs, ys, a, b, rows):
-    """Rows [0, rows) of the instance (the same cost entries, source marginal
-    renormalised), for timing on the host cores."""
-    import numpy as np
+def full_problem_host(xs, ys, a, b):
+    """The full FP64 instance on the host (C column-major, 2.4 GB at
+    20000 x 15000): the same entries the device cost builder writes."""
+    from pdot import api, instances
 
-    from pdot import api
-
-    x, y = xs[:rows], ys
-    C = np.zeros((rows, y.shape[0]), order="F")
-    for k in range(x.shape[1]):
-        C += (x[:, k : k + 1] - y[None, :, k]) ** 2
-    full_max = 0.0
-    for k0 in range(0, xs.shape[0], 2000):  # max over the full instance, in blocks
-        blk = np.zeros((min(2000, xs.shape[0] - k0), y.shape[0]))
-        for k in range(x.shape[1]):
-            blk += (xs[k0 : k0 + 2000, k : k + 1] - y[None, :, k]) ** 2
-        full_max = max(full_max, float(blk.max()))
-    C /= full_max
-    return api.OptimalTransportProblem(C, a[:rows] / a[:rows].sum(), b)
+    return api.OptimalTransportProblem(instances.sqeuclid_cost(xs, ys), a, b)
 
 
-def cpu_baseline(xs, ys, a, b, m, n, steps):
+def time_oracle_steps(prob, steps, warmup):
+    """Full-size PDHG iterations of the FP64 oracle on all host cores: `warmup`
+    untimed iterations, then `steps` timed ones in the same state."""
     import oracle
     import pdot
 
-    prob = cpu_sample_problem(xs, ys, a, b, CPU_SAMPLE_ROWS)
     cores = os.cpu_count() or 1
-    sec = oracle.time_steps(pdot.default_parameters(TOL), prob, steps, cores)
-    scale = (CPU_SAMPLE_ROWS * n) / float(m * n)
-    return {"value": steps / sec * scale, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{steps} PDHG iterations of the FP64 oracle on rows 0..{CPU_SAMPLE_ROWS - 1} of the "
-                      f"{m}x{n} instance ({CPU_SAMPLE_ROWS * n} entries), per-iteration time scaled by "
-                      f"{m}/{CPU_SAMPLE_ROWS} to the full size",
-            "seconds": sec}
+    sec = oracle.time_steps(pdot.default_parameters(TOL), prob, steps, cores, warmup=warmup)
+    return sec, cores
 
 
+def cpu_baseline(prob, m, n, steps, warmup):
+    sec, cores = time_oracle_steps(prob, steps, warmup)
+    return {"value": steps / float(sec.sum()), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} full-size PDHG iterations (take_step!) of the FP64 oracle on the {m}x{n} "
+                      f"instance after {warmup} untimed ones in the same state; no extrapolation",
+            "seconds": float(sec.sum()), "step_seconds": [round(float(x), 4) for x in sec]}
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -227,32 +219,28 @@ def barrier(world):
 
 def run_reference(args, world, rank):
     """CPU implementation of the path on the host cores (the oracle port; the
-    reference is Julia and no Julia toolchain is installed)."""
+    reference is Julia and no Julia toolchain is installed): each step is one
+    full-size PDHG iteration of the FP64 oracle on the benchmark instance."""
     if rank != 0:
         return None
-    import oracle
-    import pdot
-
     xs, ys, a, b = host_instance(args.m, args.n, SEED)
-    prob = cpu_sample_problem(xs, ys, a, b, CPU_SAMPLE_ROWS)
-    cores = os.cpu_count() or 1
-    params = pdot.default_parameters(TOL)
-    if args.warmup > 0:
-        oracle.time_steps(params, prob, args.warmup, cores)
-    sec = oracle.time_steps(params, prob, args.steps, cores)
-    scale = (CPU_SAMPLE_ROWS * args.n) / float(args.m * args.n)
-    value = args.steps / sec * scale
+    prob = full_problem_host(xs, ys, a, b)
+    sec, cores = time_oracle_steps(prob, args.steps, args.warmup)
+    total = float(sec.sum())
+    value = args.steps / total
+    sample = (f"each step one full-size PDHG iteration (take_step!) of the FP64 oracle on the "
+              f"{args.m}x{args.n} instance, after {args.warmup} untimed iterations in the same state")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / max(args.steps, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"PDHG-OT m={args.m} n={args.n} gauss-mixture sq-euclid/max FP64, tol {TOL}",
+        "config": {"workload": f"PDHG-OT m={args.m} n={args.n} gauss-mixture(8, sigma 0.05) sq-euclid/max, "
+                               f"FP64 drop-in, reference script parameters, tol {TOL}",
                    "implementation": "FP64 CPU restatement of the reference algorithm (OpenMP), "
                                      "the reference itself is Julia and cannot run here"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"each step one PDHG iteration on rows 0..{CPU_SAMPLE_ROWS - 1} of the "
-                                   f"instance, time scaled by {args.m}/{CPU_SAMPLE_ROWS}"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+                         "seconds": total, "step_seconds": [round(float(x), 4) for x in sec]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     return line
@@ -352,6 +340,112 @@ def run_mixed(args, params, m, n, Ct, a, b, xs_d, ys_d, device, local, fp64_obj)
         entry["bytes_per_entry"] = bytes_per_entry[cost]
         out[cost] = entry
     return out
+
+
+def solve_timed(params, dev_problem, local, device, **variant):
+    """A full solve from the zero start on a resident problem, timed with CUDA
+    events on the solver's stream; returns (seconds, output)."""
+    import torch
+
+    import pdot
+
+    solver = pdot.Solver(params, device_problem=dev_problem, device=local, **variant)
+    stream = torch.cuda.ExternalStream(solver.stream, device=device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    out = solver.finish()
+    e1.record(stream)
+    e1.synchronize()
+    solver.close()
+    return e0.elapsed_time(e1) / 1000.0, out
+
+
+def ttk_record(sec, out):
+    ci = out.iteration_stats[-1].convergence_information[0]
+    return {"seconds": sec, "iterations": out.iteration_count, "termination": out.termination_string,
+            "iters_per_sec": out.iteration_count / sec if sec > 0 else None,
+            "relative_l2_primal_residual": ci.relative_l2_primal_residual,
+            "relative_l2_dual_residual": ci.relative_l2_dual_residual,
+            "relative_optimality_gap": ci.relative_optimality_gap, "primal_objective": ci.primal_objective}
+
+
+def square_instance(k, dim, seed, device):
+    """The square configurations (pdot.instances.uniform_sqeuclid): points
+    U[0,1]^dim, C = ||x - y||^2 / max built on the device, marginals
+    U(0.1, 1) normalised. Returns the host problem's vectors and device tensors."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    xs = rng.uniform(0.0, 1.0, size=(k, dim))
+    ys = rng.uniform(0.0, 1.0, size=(k, dim))
+    a = rng.uniform(0.1, 1.0, size=k)
+    b = rng.uniform(0.1, 1.0, size=k)
+    a, b = a / a.sum(), b / b.sum()
+    Ct = device_cost(xs, ys, device)
+    return xs, ys, a, b, Ct, torch.from_numpy(a).to(device), torch.from_numpy(b).to(device)
+
+
+def run_c1(args, device, local, cpu_too):
+    """m = n = 1000 (points U[0,1]^2), FP64, tol 1e-4: a full solve on the GPU
+    (resident problem, device time) and, beside it, the FP64 oracle's full solve
+    on the host cores (wall time)."""
+    import oracle
+    import pdot
+    from pdot import api, instances
+
+    xs, ys, a, b, Ct, ad, bd = square_instance(C1_SIZE, 2, 0, device)
+    params = pdot.default_parameters(TOL)
+    dev_problem = (C1_SIZE, C1_SIZE, Ct.data_ptr(), ad.data_ptr(), bd.data_ptr())
+    solve_timed(params, dev_problem, local, device)  # first-call set-up outside the timing
+    sec, out = solve_timed(params, dev_problem, local, device)
+    res = {"workload": "m=n=1000, U[0,1]^2 points, sq-euclid/max, FP64 drop-in, tol 1e-4",
+           "gpu": ttk_record(sec, out)}
+    if cpu_too:
+        prob = api.OptimalTransportProblem(instances.sqeuclid_cost(xs, ys), a, b)
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        r = oracle.optimize(params, prob, num_threads=cores)
+        wall = time.perf_counter() - t0
+        rec = ttk_record(wall, r)
+        rec.update({"cores": cores, "kind": "port", "timing": "wall time of the oracle's whole optimize call"})
+        res["cpu_oracle"] = rec
+        res["gpu_speedup_over_cpu"] = wall / sec
+    return res
+
+
+def run_c2(args, device, local):
+    """m = n = 10000 (points U[0,1]^3), the FP64 drop-in: iterations/s with the
+    fused pass's roofline, and time to relative KKT 1e-4 and 1e-6."""
+    import pdot
+
+    k = C2_SIZE
+    _, _, _, _, Ct, ad, bd = square_instance(k, 3, 0, device)
+    dev_problem = (k, k, Ct.data_ptr(), ad.data_ptr(), bd.data_ptr())
+    params = pdot.default_parameters(TOL)
+    solver = pdot.Solver(params, device_problem=dev_problem, device=local)
+    iters, ms, _, _ = time_iterations(solver, args.warmup, args.steps, device)
+    solver.close()
+    ts = pdot.Solver(params, device_problem=dev_problem, device=local, use_cuda_graph=False, time_kernels=True)
+    t0 = ts.iterate(args.warmup)
+    t1 = ts.iterate(args.steps)
+    ts.close()
+    passes = t1["primal_passes"] - t0["primal_passes"]
+    fresh = t1["primal_passes_fresh_average"] - t0["primal_passes_fresh_average"]
+    launches = t1["timed_primal_passes"] - t0["timed_primal_passes"]
+    alg = k * k * (40.0 * (passes - fresh) + 32.0 * fresh) / max(passes, 1)
+    avg_s = (t1["primal_pass_ms"] - t0["primal_pass_ms"]) / 1000.0 / max(launches, 1)
+    peak, _ = read_peak()
+    res = {"workload": "m=n=10000, U[0,1]^3 points, sq-euclid/max, FP64 drop-in",
+           "iters_per_sec": iters / (ms / 1000.0), "ms_per_iter": ms / max(iters, 1),
+           "roofline": {"kernel": "k1_primal", "achieved": alg / avg_s / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": alg / avg_s / 1e9 / peak, "algorithmic_bytes_per_launch": alg,
+                        "avg_launch_ms": avg_s * 1000.0}}
+    for tol in (1e-4, 1e-6):
+        sec, out = solve_timed(pdot.default_parameters(tol), dev_problem, local, device)
+        res[f"tol_{tol:.0e}"] = ttk_record(sec, out)
+    return res
 
 
 def run_batched(args, device):
@@ -553,9 +647,12 @@ def run_ours(args, world, rank, local):
     batched = run_batched(args, device) if not args.no_batched else None
     learned_ws = run_learned(args, device) if not args.no_learned else None
 
+    c1 = run_c1(args, device, local, cpu_too=(rank == 0 and world == 1)) if not args.no_configs else None
+    c2 = run_c2(args, device, local) if not args.no_configs else None
+
     cpu = None
     if rank == 0 and world == 1:
-        cpu = cpu_baseline(xs, ys, a_h, b_h, m, n, steps=20)
+        cpu = cpu_baseline(full_problem_host(xs, ys, a_h, b_h), m, n, steps=5, warmup=2)
 
     value = world * iters / (ms / 1000.0)
     line = {
@@ -571,8 +668,8 @@ def run_ours(args, world, rank, local):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch "
-                                       "(profiles/dram_traffic_full_size.md): measured/algorithmic ratio times "
-                                       "this region's algorithmic bytes per launch" if traffic else None,
+                                       "on B200: measured/algorithmic ratio times this region's algorithmic "
+                                       "bytes per launch" if traffic else None,
                      "kernel": "k1_primal (fused primal pass)",
                      "algorithmic_bytes_per_entry": full_bytes,
                      "algorithmic_bytes_per_launch": per_launch_bytes,
@@ -581,6 +678,7 @@ def run_ours(args, world, rank, local):
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk.summary(), "time_to_kkt": ttk,
         "mixed_precision": mixed, "batched": batched, "learned_warm_start": learned_ws,
+        "c1": c1, "c2": c2,
     }
     return line
 

@@ -162,7 +162,11 @@ typedef struct pdot_solver_options {
    * exp((u_i + v_j - C_ij) / eps) (0 rounds: that kernel as it is) */
   double warm_plan_epsilon;
   int32_t warm_plan_iterations;
-  int32_t reserved[1];                /* must be zero */
+  /* Test hook, 0 in normal use. 1: each consumer wait of the staged fused pass
+   * reports a timeout without polling; the kernel still waits (bounded) for the
+   * copies it has in flight, sets its error word and returns, and the call
+   * fails with PDOT_ERR_CUDA. It exercises the timeout path without a fault. */
+  int32_t fail_bounded_waits;
 } pdot_solver_options;
 
 /* ---- output -------------------------------------------------------------- */
@@ -383,9 +387,10 @@ int pdot_sqeuclid_cost_f64(int64_t m, int64_t n, int32_t dim, const double* sour
  * synchronisation). It has no counterpart in the reference. Its scratch is a
  * fixed PDOT_NOALLOC_SCRATCH_BYTES array inside the library (held by every GPU
  * that loads it until exit), so the call allocates nothing; sizes whose
- * scratch would exceed it return PDOT_ERR_TOO_LARGE. The first call on a
- * device looks up the array's device address: make it before any stream
- * capture. Calls share the array: calls that overlap on the GPU race. */
+ * scratch would exceed it return PDOT_ERR_TOO_LARGE. Every call looks up the
+ * array's device address on the current device; the first call on a device
+ * loads the library's module there: make it before any stream capture. Calls
+ * share the array: calls that overlap on the GPU race. */
 #define PDOT_NOALLOC_SCRATCH_BYTES (16u << 20)
 int pdot_primal_pass_f64_noalloc(int64_t m, int64_t n,
                                  const double* cost, double* primal, double* primal_avg,

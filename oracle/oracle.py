@@ -53,8 +53,8 @@ def load():
     ]
     lib.pdot_oracle_time_steps.restype = ct.c_int
     lib.pdot_oracle_time_steps.argtypes = [
-        ct.POINTER(_abi.ProblemC), ct.POINTER(_abi.PdhgParametersC), ct.c_int, ct.c_int,
-        ct.POINTER(ct.c_double),
+        ct.POINTER(_abi.ProblemC), ct.POINTER(_abi.PdhgParametersC), ct.c_int, ct.c_int, ct.c_int,
+        ct.c_void_p,
     ]
     lib.pdot_oracle_rounding.restype = None
     lib.pdot_oracle_rounding.argtypes = [ct.c_int64, ct.c_int64, P, P, P]
@@ -120,19 +120,21 @@ def primal_pass(C, X, Xa, u, v, step_over_weight, avg_new_weight, avg_scale, fla
     return drow, dcol, float(dsq[0])
 
 
-def time_steps(params, problem, steps: int, num_threads: int = 0) -> float:
-    """Seconds the oracle takes for `steps` PDHG iterations (take_step! only)
-    from the initial state, with `num_threads` OpenMP threads (0 = all)."""
+def time_steps(params, problem, steps: int, num_threads: int = 0, warmup: int = 0):
+    """Per-step seconds of `steps` PDHG iterations of the oracle (take_step!
+    only), timed after `warmup` untimed iterations in the same state, with
+    `num_threads` OpenMP threads (0 = all). Returns a numpy array."""
     from pdot import api, _abi
 
     lib = load()
     mp = api.MarshalledProblem(problem)
     cp = api.marshal_params(params)
-    sec = ct.c_double(0.0)
-    rc = lib.pdot_oracle_time_steps(ct.byref(mp.c), ct.byref(cp), int(steps), int(num_threads), ct.byref(sec))
+    sec = np.zeros(max(int(steps), 1))
+    rc = lib.pdot_oracle_time_steps(ct.byref(mp.c), ct.byref(cp), int(warmup), int(steps), int(num_threads),
+                                    sec.ctypes.data)
     if rc != 0:
         raise _abi.PdotError(rc, f"oracle time_steps failed ({rc})")
-    return sec.value
+    return sec[: int(steps)]
 
 
 def rounding(problem, X):

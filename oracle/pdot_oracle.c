@@ -626,7 +626,8 @@ int pdot_oracle_optimize(const pdot_problem* P, const pdot_pdhg_parameters* prm,
  * src/solver_gpu.jl:428-441): initial duals u0, v0, optional initial plan X0
  * (its row and column sums become r and c) and optional initial primal weight
  * (omega0 > 0). The stored gradient is C - u0 - v0 from the start. The last
- * restart point stays the zero point, as in the CUDA solver. */
+ * restart information starts at this initial point, as the reference's does
+ * at its own (create_last_restart_info, src/saddle_point_gpu.jl:371-393). */
 int pdot_oracle_optimize_warm(const pdot_problem* P, const pdot_pdhg_parameters* prm, const double* u0,
                               const double* v0, const double* X0, double omega0,
                               pdot_saddle_point_output* out, int num_threads) {
@@ -672,6 +673,13 @@ int pdot_oracle_optimize_warm(const pdot_problem* P, const pdot_pdhg_parameters*
     }
     for (i64 j = 0; j < n; ++j)
       for (i64 i = 0; i < m; ++i) S->G[i + j * m] = (S->C[i + j * m] - S->u[i]) - S->v[j];
+    /* create_last_restart_info at the initial point */
+    memcpy(S->Xl, S->X, sizeof(double) * N);
+    memcpy(S->Gl, S->G, sizeof(double) * N);
+    memcpy(S->ul, S->u, sizeof(double) * m);
+    memcpy(S->rl, S->r, sizeof(double) * m);
+    memcpy(S->vl, S->v, sizeof(double) * n);
+    memcpy(S->cl, S->c, sizeof(double) * n);
   }
   const double smoothing = prm->restart_params.primal_weight_update_smoothing;
   const double start_time = now_sec();
@@ -805,15 +813,19 @@ void pdot_oracle_primal_pass(i64 m, i64 n, const double* C, double* X, double* X
 }
 
 /*
- * CPU baseline timing: `steps` iterations of take_step! (the per-iteration
- * work of optimize()'s loop, src/solver_gpu.jl:290-367) from the initial
- * state, with all OpenMP threads; returns the elapsed seconds (evaluations,
- * one per termination_evaluation_frequency iterations, are not included).
+ * CPU baseline timing: `warmup` untimed iterations of take_step! (the
+ * per-iteration work of optimize()'s loop, src/solver_gpu.jl:290-367) from the
+ * initial state, then `steps` timed ones in the same state, with all OpenMP
+ * threads. The warm-up touches every page of the freshly allocated state, so
+ * the timed steps measure the iteration, not first-touch page faults.
+ * step_seconds[k] receives the time of timed step k (evaluations, one per
+ * termination_evaluation_frequency iterations, are not included).
  */
-int pdot_oracle_time_steps(const pdot_problem* P, const pdot_pdhg_parameters* prm, int steps,
-                           int num_threads, double* seconds) {
+int pdot_oracle_time_steps(const pdot_problem* P, const pdot_pdhg_parameters* prm, int warmup, int steps,
+                           int num_threads, double* step_seconds) {
   int rc = pdot_oracle_validate(P, prm);
   if (rc != PDOT_OK) return rc;
+  if (warmup < 0 || steps < 0) return PDOT_ERR_INVALID_ARGUMENT;
 #ifdef _OPENMP
   if (num_threads > 0) omp_set_num_threads(num_threads);
 #else
@@ -824,14 +836,14 @@ int pdot_oracle_time_steps(const pdot_problem* P, const pdot_pdhg_parameters* pr
   if (!ostate_init(S, P)) return PDOT_ERR_OUT_OF_MEMORY;
   S->step_size = prm->step_size_policy == PDOT_STEP_SIZE_ADAPTIVE ? 1.0 : 0.8 / sqrt((double)(S->m + S->n));
   S->primal_weight = prm->primal_importance;
-  const double t0 = now_sec();
-  for (int k = 0; k < steps; ++k) {
+  for (int k = 0; k < warmup + steps; ++k) {
+    const double t0 = now_sec();
     if (prm->step_size_policy == PDOT_STEP_SIZE_ADAPTIVE)
       take_step_adaptive(S, prm->reduction_exponent, prm->growth_exponent);
     else
       take_step_constant(S);
+    if (k >= warmup) step_seconds[k - warmup] = now_sec() - t0;
   }
-  *seconds = now_sec() - t0;
   ostate_free(S);
   return PDOT_OK;
 }

@@ -722,7 +722,12 @@ __global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
 }
 
 // Batched evaluation, vector part + per-instance evaluation control.
-__global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, SolveConfig cfg, int grid) {
+// start_only: the evaluation of the initial points, run once after
+// kb_init_state when some instance starts warm; the warm instances record
+// their start point as the last restart point (record_start_point) and no
+// instance takes any other step of the evaluation block.
+__global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, SolveConfig cfg, int grid,
+                                                            int start_only) {
   const BatchActive act = *B.act;
   if (act.count == 0) return;
   const long long blk = blockIdx.x;
@@ -774,7 +779,10 @@ __global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, Solve
     if (threadIdx.x == 0) {
       const PointSums cur = point_sums(E, R, Cc, 0);
       const PointSums avg = point_sums(E, R, Cc, E_AVG);
-      eval_control(st, cfg, cur, avg, B.rec + k, 1);
+      if (!start_only)
+        eval_control(st, cfg, cur, avg, B.rec + k, 1);
+      else if (B.warm[k])
+        record_start_point(st, cur);
       st->ticket_eval = 0;
     }
   }
@@ -1371,13 +1379,20 @@ class BatchSolver {
     }
     pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_);  // drops invalid problems
     BCK(cudaGetLastError());
+    // warm instances start their restart information at the warm point, as
+    // the reference starts it at its initial point
+    if (any_warm_) {
+      PDOT_BATCH_VARIANT(kind_, pdot::kb_eval, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
+      pdot::kb_eval_vec<<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_, 1);
+      BCK(cudaGetLastError());
+    }
   }
 
   bool is_eval(long long it) const { return (it - 1) % freq_ == 0 || it == limit_ + 1 || it <= 10; }
 
   void launch_eval() {
     PDOT_BATCH_VARIANT(kind_, pdot::kb_eval, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
-    pdot::kb_eval_vec<<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_);
+    pdot::kb_eval_vec<<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_, 0);
     pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_);
     BCK(cudaGetLastError());
   }

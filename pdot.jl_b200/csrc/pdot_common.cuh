@@ -49,6 +49,8 @@ struct Geometry {
   int32_t cost_kind;   // PDOT_COST_F64 / _F32 / _BF16, or a coordinate kind (internal_cost_kind)
   int32_t tma;         // 1: the fused pass stages its operands with bulk copies
   int32_t tma_smem;    // dynamic shared memory of the staged pass (bytes)
+  int32_t fail_waits;  // test hook: the staged pass's consumer waits report a timeout at once
+  int32_t pad_;
 };
 
 // Where the cost entries come from.
@@ -178,12 +180,20 @@ struct Buffers {
 Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device, int plan_f32 = 0,
                        int cost_kind = PDOT_COST_F64, int staged_ok = 0);
 size_t workspace_doubles(const Geometry& g);
+// Scratch of the stand-alone primal pass (launch_primal_pass): its row
+// partials, column partials and per-CTA sums of squares, in that order.
+inline size_t pass_scratch_doubles(const Geometry& g) {
+  return ((size_t)g.grid + g.panels) * kPanelRows + (size_t)g.panels * g.n + (size_t)g.grid;
+}
 
 cudaError_t launch_init(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
 cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s);
 cudaError_t launch_dual(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
 cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
-cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
+// start_only = 1: a warm start's initial point becomes the last restart
+// point; nothing else of the evaluation block runs.
+cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s,
+                        int start_only = 0);
 
 // Conversions used by the host: FP64 cost to its stored precision, and an
 // FP32 plan widened to FP64 for the caller.

@@ -350,8 +350,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-  for (int it = 0; it < kSpinLimit; ++it)
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, int polls = kSpinLimit) {
+  for (int it = 0; it < polls; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -533,6 +533,22 @@ __device__ bool optimality_met(const SolveConfig& cfg, const DevState* st,
   }
   return derr < cfg.eps_abs + cfg.eps_rel * dbase && perr < cfg.eps_abs + cfg.eps_rel * pbase &&
          gap < cfg.eps_abs + cfg.eps_rel * abs_obj;
+}
+
+// A warm start's last-restart record. The reference's restart information
+// starts at the initial point (create_last_restart_info,
+// src/saddle_point_gpu.jl:371-393: copies of the initial plan, duals, sums and
+// stored gradient), so a solve started from (X0, u0, v0) keeps that point:
+// its l2 primal residual ||[a - X0 1; b - X0^T 1]||, its l2 dual residual
+// ||min(C - u0 - v0, 0)|| (the stored gradient is C - u0 - v0 from the start),
+// its gap and the norms ||X0||, ||[u0; v0]|| that the first restart measures
+// the distance from (Q3). `P` holds the start point's evaluation sums.
+__device__ __forceinline__ void record_start_point(DevState* st, const PointSums& P) {
+  st->last_rp = sqrt(P.sq_src + P.sq_tgt);
+  st->last_rd = sqrt(P.sq_g);
+  st->last_gap = fabs(P.pobj - (P.dot_src + P.dot_tgt));
+  st->last_xnorm = sqrt(P.sq_x);
+  st->last_ynorm = sqrt(P.sq_u + P.sq_v);
 }
 
 // The evaluation block of optimize(), src/solver_gpu.jl:529-696, with

@@ -131,6 +131,7 @@ struct Variant {
   double plan_eps = 0.0;  // > 0: recover the warm plan from the warm duals
   int plan_iters = 0;
   int staged = 2;  // 0 direct, 1 staged, 2 automatic
+  int fail_waits = 0;  // test hook: the staged pass's waits report timeouts
 };
 
 Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
@@ -182,7 +183,9 @@ Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
   if (o->primal_pass != PDOT_PASS_AUTO && o->primal_pass != PDOT_PASS_STAGED && o->primal_pass != PDOT_PASS_DIRECT)
     fail(PDOT_ERR_INVALID_ARGUMENT, "unknown primal_pass %d", o->primal_pass);
   v.staged = o->primal_pass == PDOT_PASS_STAGED ? 1 : (o->primal_pass == PDOT_PASS_DIRECT ? 0 : 2);
-  if (o->reserved[0] != 0) fail(PDOT_ERR_INVALID_ARGUMENT, "reserved option fields must be zero");
+  if (o->fail_bounded_waits != 0 && o->fail_bounded_waits != 1)
+    fail(PDOT_ERR_INVALID_ARGUMENT, "fail_bounded_waits must be 0 or 1");
+  v.fail_waits = o->fail_bounded_waits;
   return v;
 }
 
@@ -213,9 +216,24 @@ pdot::SolveConfig make_config(const pdot_pdhg_parameters& p) {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// A temporary device buffer freed when it goes out of scope, also when a CK
+// check throws on the way (cudaFree waits for the work that still uses it).
+struct DeviceTemp {
+  void* p = nullptr;
+  DeviceTemp() = default;
+  DeviceTemp(const DeviceTemp&) = delete;
+  DeviceTemp& operator=(const DeviceTemp&) = delete;
+  ~DeviceTemp() {
+    if (p) cudaFree(p);
+  }
+  template <typename T>
+  T* get() const {
+    return static_cast<T*>(p);
+  }
+};
+
 int64_t pass_workspace_bytes(const pdot::Geometry& g) {
-  return (int64_t)((((size_t)g.grid + g.panels) * pdot::kPanelRows + (size_t)g.panels * g.n + g.grid) *
-                   sizeof(double));
+  return (int64_t)(pdot::pass_scratch_doubles(g) * sizeof(double));
 }
 
 constexpr int kRingCap = 4096;
@@ -279,19 +297,19 @@ class Solver {
       CK(cudaMalloc(&Cs, std::max<size_t>(N, 1) * cbytes));
       allocs_.push_back(Cs);
       const double* src = P.cost_matrix;
-      void* tmp = nullptr;
+      DeviceTemp tmp;
       if (!device_inputs) {
-        CK(cudaMalloc(&tmp, N * sizeof(double)));
-        CK(cudaMemcpyAsync(tmp, P.cost_matrix, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
-        src = static_cast<const double*>(tmp);
+        CK(cudaMalloc(&tmp.p, N * sizeof(double)));
+        CK(cudaMemcpyAsync(tmp.p, P.cost_matrix, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        src = tmp.get<const double>();
       }
       CK(pdot::launch_convert_cost(src, Cs, var.cost_kind, N, stream_));
       CK(cudaStreamSynchronize(stream_));
-      if (tmp) CK(cudaFree(tmp));
       cost_.C = Cs;
     }
     const int kind = pdot::internal_cost_kind(var.cost_kind, var.point_dim);
     g_ = pdot::make_geometry(m, n, cost_aligned ? 1 : 0, device_, var.plan_f32, kind, var.staged);
+    g_.fail_waits = var.fail_waits;
     if (device_inputs) {
       a_ = P.source_distribution;
       b_ = P.target_distribution;
@@ -349,24 +367,19 @@ class Solver {
       alloc(&warm_r_, m);
       alloc(&warm_c_, n);
       const double* src = var.warm_x;
-      double* tmp = nullptr;
-      if (!device_inputs || var.plan_f32) {
-        if (!device_inputs) {
-          CK(cudaMalloc(&tmp, std::max<size_t>(N, 1) * sizeof(double)));
-          CK(cudaMemcpyAsync(tmp, var.warm_x, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
-          src = tmp;
-        }
+      DeviceTemp tmp, work;
+      if (!device_inputs) {
+        CK(cudaMalloc(&tmp.p, std::max<size_t>(N, 1) * sizeof(double)));
+        CK(cudaMemcpyAsync(tmp.p, var.warm_x, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        src = tmp.get<const double>();
       }
       if (var.plan_f32)
         CK(pdot::launch_convert_cost(src, wx, PDOT_COST_F32, N, stream_));
       else
         CK(cudaMemcpyAsync(wx, src, N * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-      double* work = nullptr;
-      CK(cudaMalloc(&work, std::max<size_t>(pdot::plan_sums_workspace_doubles(m, n), 1) * sizeof(double)));
-      CK(pdot::launch_plan_sums(m, n, wx, var.plan_f32, warm_r_, warm_c_, work, stream_));
+      CK(cudaMalloc(&work.p, std::max<size_t>(pdot::plan_sums_workspace_doubles(m, n), 1) * sizeof(double)));
+      CK(pdot::launch_plan_sums(m, n, wx, var.plan_f32, warm_r_, warm_c_, work.get<double>(), stream_));
       CK(cudaStreamSynchronize(stream_));
-      CK(cudaFree(work));
-      if (tmp) CK(cudaFree(tmp));
     }
     void* xp = nullptr;
     for (int k = 0; k < 2; ++k) {
@@ -496,6 +509,9 @@ class Solver {
       wp_.c = c_[0];
       CK(pdot::launch_warm_plan(wp_, plan_iters_, stream_));
     }
+    // a warm start's restart information starts at the warm point, as the
+    // reference's starts at its initial point
+    if (cfg_.warm_start) CK(pdot::launch_eval(B_, g_, cfg_, stream_, 1));
     CK(cudaStreamSynchronize(stream_));
     CK(cudaMemcpy(&status_, st_, sizeof(status_), cudaMemcpyDeviceToHost));
     host_it_ = 1;
@@ -581,16 +597,15 @@ class Solver {
       } else {
         // widen the FP32 plan in chunks through a small device buffer
         const size_t chunk = std::min<size_t>(N, size_t(1) << 24);
-        double* tmp = nullptr;
-        CK(cudaMalloc(&tmp, std::max<size_t>(chunk, 1) * sizeof(double)));
+        DeviceTemp tmp;
+        CK(cudaMalloc(&tmp.p, std::max<size_t>(chunk, 1) * sizeof(double)));
         for (size_t off = 0; off < N; off += chunk) {
           const size_t cnt = std::min(chunk, N - off);
-          CK(pdot::launch_widen(static_cast<const float*>(X_[xb]) + off, tmp, cnt, stream_));
-          CK(cudaMemcpyAsync(out->primal_solution + off, tmp, cnt * sizeof(double), cudaMemcpyDeviceToHost,
+          CK(pdot::launch_widen(static_cast<const float*>(X_[xb]) + off, tmp.get<double>(), cnt, stream_));
+          CK(cudaMemcpyAsync(out->primal_solution + off, tmp.p, cnt * sizeof(double), cudaMemcpyDeviceToHost,
                              stream_));
         }
         CK(cudaStreamSynchronize(stream_));
-        CK(cudaFree(tmp));
       }
     }
     if (out->dual_source_solution)

@@ -24,10 +24,10 @@
 // drop-in, float for mixed precision), the cost source (FP64 / FP32 / BF16
 // storage, or the squared-Euclidean cost computed from FP32 coordinates) and
 // the rows each lane loads at once (16 bytes of plan, or 1 on the scalar path
-// for odd sizes and unaligned buffers). Per-entry arithmetic is FP64 in every
-// variant; an FP32 plan is rounded once when stored, and the step entering the
-// row/column sums is taken between the stored values, so the FP64 sums track
-// the stored plan exactly.
+// for odd sizes and unaligned buffers). The FP64 plan's per-entry arithmetic is
+// FP64; an FP32 plan's is FP32, its own precision (primal_entry). In both, the
+// step entering the FP64 row/column sums is taken exactly between the stored
+// values, so the sums track the stored plan exactly.
 #include <cfloat>
 #include <cmath>
 
@@ -253,6 +253,9 @@ __global__ void __launch_bounds__(kThreads, 2) k1_primal_staged(Buffers B, Geome
     ++issued;
   }
   bool failed = false;
+  // consumer waits poll up to kSpinLimit times (none under the fail_waits test
+  // hook); the drain after a failure always polls up to kSpinLimit times
+  const int polls = g.fail_waits ? 0 : kSpinLimit;
   double sq = 0.0;
   for (int64_t p = q0 / n; p * n < q1; ++p) {
     const int64_t row0 = p * kPanelRows;
@@ -274,7 +277,7 @@ __global__ void __launch_bounds__(kThreads, 2) k1_primal_staged(Buffers B, Geome
       const int64_t j = cons.j;
       const int stage = (int)(consumed % S);
       const uint32_t parity = (uint32_t)((consumed / S) & 1);
-      if (!mbar_wait_bounded(bar0 + 8 * stage, parity)) {
+      if (!mbar_wait_bounded(bar0 + 8 * stage, parity, polls)) {
         failed = true;
         break;
       }
@@ -514,7 +517,10 @@ __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
   block_reduce<kEvalSums>(acc, kEvalMaxMask, B.evpart + cta * kEvalSums);
 }
 
-__global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, SolveConfig cfg) {
+// start_only: the evaluation of a warm start's initial point, run once after
+// k0_init; its last CTA records the point as the last restart point
+// (record_start_point) and takes no other step of the evaluation block.
+__global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, SolveConfig cfg, int start_only) {
   DevState* st = B.st;
   if (st->done) return;
   const int buf = st->buf;
@@ -557,7 +563,10 @@ __global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, So
     if (threadIdx.x == 0) {
       const PointSums cur = point_sums(E, R, Cc, 0);
       const PointSums avg = point_sums(E, R, Cc, E_AVG);
-      eval_control(st, cfg, cur, avg, B.ring, B.ring_cap);
+      if (start_only)
+        record_start_point(st, cur);
+      else
+        eval_control(st, cfg, cur, avg, B.ring, B.ring_cap);
       st->ticket_eval = 0;
     }
   }
@@ -567,7 +576,8 @@ __global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, So
 // Start of a solve: cached_ot_info (src/termination.jl:94-101) on the device,
 // the initial step size and primal weight (src/solver_gpu.jl:476-496,
 // src/saddle_point_gpu.jl:848-866) and the initial last-restart record (the
-// zero point, src/saddle_point_gpu.jl:371-393).
+// zero point, src/saddle_point_gpu.jl:371-393; after a warm start the host
+// replaces it with the start point's, see record_start_point).
 template <typename TX, int CK, int R>
 __global__ void __launch_bounds__(kThreads, 2) k0_init(Buffers B, Geometry g, SolveConfig cfg) {
   constexpr int RPL = kPanelRows / (32 * R);
@@ -784,6 +794,8 @@ Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device, int plan_f3
   const bool want = staged_ok == 1 || (staged_ok == 2 && (cost_kind == PDOT_COST_BF16 || is_point_cost(cost_kind)));
   g.tma = (want && g.vec > 1 && !(cost_kind == PDOT_COST_BF16 && m % 8 != 0)) ? 1 : 0;
   g.tma_smem = 0;
+  g.fail_waits = 0;
+  g.pad_ = 0;
   int occ = 1;
   if (g.tma) {
     PDOT_STAGED_VARIANT(g, {
@@ -839,9 +851,10 @@ cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& 
   return launch_dual(B, g, cfg, s);
 }
 
-cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s) {
+cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s,
+                        int start_only) {
   PDOT_VARIANT(g, k3_eval, (kfn<<<g.grid, kThreads, 0, s>>>(B, g)));
-  k4_eval<<<g.row_blocks + g.col_blocks, kVecThreads, 0, s>>>(B, g, cfg);
+  k4_eval<<<g.row_blocks + g.col_blocks, kVecThreads, 0, s>>>(B, g, cfg, start_only);
   return cudaGetLastError();
 }
 

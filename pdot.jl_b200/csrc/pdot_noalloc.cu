@@ -12,18 +12,18 @@
 // The array (kScratchBytes = 16 MiB) is part of the library's device image:
 // every GPU that loads it holds the 16 MiB until the process exits. Host code
 // cannot hand the array's name to a kernel (on the host it only names a
-// stand-in, not device memory), so the first call on each device looks up its
-// device address with cudaGetSymbolAddress, with that device current, and
-// caches it; make that first call before any stream capture. All calls on a
-// device share the array and it keeps the last call's contents; nothing needs
-// clearing, because the second stage reads only partial slots the first stage
-// of the same call wrote. Calls that overlap on the GPU (different streams,
-// or another host thread) race on the array and must be serialised by the
-// caller.
+// stand-in, not device memory), so every call looks up the array's device
+// address on the current device with cudaGetSymbolAddress (cheap once the
+// module is loaded, and never stale, even after a cudaDeviceReset reloads
+// it). The first call on a device loads the module there: make that first
+// call before any stream capture. All calls on a device share the array and it
+// keeps the last call's contents; nothing needs clearing, because the second
+// stage reads only partial slots the first stage of the same call wrote. Calls
+// that overlap on the GPU (different streams, or another host thread) race on
+// the array and must be serialised by the caller.
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
-#include <mutex>
 
 #include "pdot_common.cuh"
 
@@ -31,23 +31,15 @@ namespace {
 
 constexpr size_t kScratchBytes = size_t(16) << 20;
 constexpr size_t kScratchDoubles = kScratchBytes / sizeof(double);
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_pass_scratch[kScratchDoubles];
 
-std::mutex g_scratch_mutex;
-double* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of g_pass_scratch on the current device (looked up once).
-cudaError_t scratch_address(int device, double** out) {
-  std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_addr[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_pass_scratch);
-    if (e != cudaSuccess) return e;
-    g_scratch_addr[device] = static_cast<double*>(p);
-  }
-  *out = g_scratch_addr[device];
+// Device address of g_pass_scratch on the current device.
+cudaError_t scratch_address(double** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_pass_scratch);
+  if (e != cudaSuccess) return e;
+  *out = static_cast<double*>(p);
   return cudaSuccess;
 }
 
@@ -81,18 +73,16 @@ extern "C" int pdot_primal_pass_f64_noalloc(int64_t m, int64_t n, const double* 
   int device = 0;
   cudaError_t e = cudaGetDevice(&device);
   if (e != cudaSuccess) return report(PDOT_ERR_CUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
-  if (device < 0 || device >= kMaxDevices)
-    return report(PDOT_ERR_INVALID_ARGUMENT, "device %d beyond the %d supported", device, kMaxDevices);
   const int vec_ok = aligned16(cost) && aligned16(primal) && aligned16(primal_avg);
   const pdot::Geometry g = pdot::make_geometry(m, n, vec_ok, device);
-  const size_t need = ((size_t)g.grid + g.panels) * pdot::kPanelRows + (size_t)g.panels * g.n + g.grid;
+  const size_t need = pdot::pass_scratch_doubles(g);
   if (need > kScratchDoubles)
     return report(PDOT_ERR_TOO_LARGE,
                   "a %lld x %lld pass needs %zu bytes of scratch; the fixed scratch holds %zu bytes "
                   "(use pdot_primal_pass_f64 with a workspace)",
                   (long long)m, (long long)n, need * sizeof(double), kScratchBytes);
   double* scratch = nullptr;
-  e = scratch_address(device, &scratch);
+  e = scratch_address(&scratch);
   if (e != cudaSuccess) return report(PDOT_ERR_CUDA, "cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
   e = pdot::launch_primal_pass(g, cost, primal, primal_avg, dual_source, dual_target, step_over_weight,
                                avg_new_weight, avg_scale, flags, delta_row_sum, delta_col_sum, delta_sq_norm,

@@ -260,7 +260,7 @@ struct CSolverOptions                           # pdot_solver_options
     warm_primal::Ptr{Float64}
     warm_plan_epsilon::Float64
     warm_plan_iterations::Int32
-    reserved::NTuple{1,Int32}
+    fail_bounded_waits::Int32
 end
 
 struct CBatchProblem                            # pdot_batch_problem

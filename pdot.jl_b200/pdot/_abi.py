@@ -100,7 +100,7 @@ class SolverOptionsC(ct.Structure):
         ("warm_primal", ct.POINTER(ct.c_double)),
         ("warm_plan_epsilon", ct.c_double),
         ("warm_plan_iterations", ct.c_int32),
-        ("reserved", ct.c_int32 * 1),
+        ("fail_bounded_waits", ct.c_int32),
     ]
 
 

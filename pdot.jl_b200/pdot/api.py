@@ -370,7 +370,8 @@ _COSTS = {"f64": _abi.COST_F64, "f32": _abi.COST_F32, "bf16": _abi.COST_BF16,
 
 def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, precision: str = "f64",
              cost: Optional[str] = None, points=None, cost_scale: Optional[float] = None, warm_start=None,
-             device_pointers: bool = False, primal_pass: str = "auto", recover_plan=None):
+             device_pointers: bool = False, primal_pass: str = "auto", recover_plan=None,
+             fail_bounded_waits: bool = False):
     """Build pdot_solver_options. Returns (options, objects to keep alive).
 
     precision  "f64" (the drop-in) or "f32" (mixed precision: FP32 plan)
@@ -383,6 +384,8 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
     recover_plan  (eps, rounds): with warm duals and no plan, the plan is
                recovered from the duals by `rounds` of log-domain balancing
                of exp((u_i + v_j - C_ij) / eps)
+    fail_bounded_waits  test hook: the staged pass's waits report a timeout at
+               once (the call then fails with PDOT_ERR_CUDA)
     """
     keep = []
     opts = _abi.SolverOptionsC()
@@ -393,6 +396,7 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
     if cost is None:
         cost = "f64" if precision == "f64" else "f32"
     opts.cost_storage = _COSTS[cost]
+    opts.fail_bounded_waits = 1 if fail_bounded_waits else 0
     if recover_plan is not None:
         opts.warm_plan_epsilon = float(recover_plan[0])
         opts.warm_plan_iterations = int(recover_plan[1])
@@ -439,7 +443,7 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
 def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device: int = 0,
              use_cuda_graph: bool = True, precision: str = "f64", cost: Optional[str] = None, points=None,
              cost_scale: Optional[float] = None, warm_start=None, primal_pass: str = "auto",
-             recover_plan=None) -> SaddlePointOutput:
+             recover_plan=None, fail_bounded_waits: bool = False) -> SaddlePointOutput:
     """PDOT.optimize, src/solver_gpu.jl:413-720, run by libpdot.so on the GPU.
 
     The keyword options beyond `device` select this implementation's mixed
@@ -451,7 +455,7 @@ def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device
     cp = marshal_params(params)
     opts, _keep = _options(device, use_cuda_graph, precision=precision, cost=cost, points=points,
                            cost_scale=cost_scale, warm_start=warm_start, primal_pass=primal_pass,
-                           recover_plan=recover_plan)
+                           recover_plan=recover_plan, fail_bounded_waits=fail_bounded_waits)
     ob = OutputBuffers(mp.m, mp.n, stats_capacity_for(params))
     rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
     _abi.check(lib, rc, "pdot_optimize")

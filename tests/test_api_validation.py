@@ -38,7 +38,7 @@ def test_recovered_plan_and_warm_start_reach_the_options():
     opts, keep = api._options(0, True, warm_start=(np.ones(4), np.ones(3)), recover_plan=(3e-4, 100))
     assert opts.warm_plan_epsilon == 3e-4 and opts.warm_plan_iterations == 100
     assert bool(opts.warm_dual_source) and bool(opts.warm_dual_target) and not bool(opts.warm_primal)
-    assert list(opts.reserved) == [0]
+    assert opts.fail_bounded_waits == 0
     u0 = np.ctypeslib.as_array(opts.warm_dual_source, shape=(4,))
     assert np.all(u0 == 1.0)
     del keep
@@ -58,3 +58,18 @@ def test_warm_plan_without_duals_is_rejected_before_device_work(built):
     rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
     assert rc == _abi.PDOT_ERR_INVALID_ARGUMENT
     assert "warm" in _abi.last_error(lib)
+
+
+def test_timeout_hook_is_validated_before_device_work(built):
+    """fail_bounded_waits is 0 or 1; anything else is refused before device work."""
+    prob = instances.uniform_sqeuclid(4, 3, seed=0)
+    lib = _abi.load()
+    mp = api.MarshalledProblem(prob)
+    cp = api.marshal_params(pdot.default_parameters(1e-4))
+    opts = _abi.SolverOptionsC()
+    opts.use_cuda_graph = 1
+    opts.fail_bounded_waits = 2
+    ob = api.OutputBuffers(4, 3, 16)
+    rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
+    assert rc == _abi.PDOT_ERR_INVALID_ARGUMENT
+    assert "fail_bounded_waits" in _abi.last_error(lib)

@@ -85,12 +85,28 @@ def test_noalloc_call_allocates_nothing(cuda):
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(cuda):
+    """2^17 rows x 4096 columns need 512 x 4096 column partials (16 MiB) plus
+    the row partials: more than the fixed scratch. Every buffer is as large as
+    the request (three 4 GiB matrices), so a regression of the size check
+    would run a valid pass and fail the assertion instead of reading or
+    writing out of bounds."""
     import torch
 
     lib = _abi.load()
-    t = torch.zeros(16, dtype=torch.float64, device=cuda)
-    p = t.data_ptr()
-    # 2^20 rows x 4096 columns would need 4096 x 4096 column partials (128 MiB)
-    rc = lib.pdot_primal_pass_f64_noalloc(1 << 20, 4096, p, p, p + 8, p, p, 1.0, 1.0, 1.0, 0, p, p, p, None)
+    m, n = 1 << 17, 4096
+    mats = [torch.empty((n, m), dtype=torch.float64, device=cuda) for _ in range(3)]
+    mats[1].zero_()
+    mats[2].zero_()
+    rows = [torch.zeros(m, dtype=torch.float64, device=cuda) for _ in range(2)]
+    cols = [torch.zeros(n, dtype=torch.float64, device=cuda) for _ in range(2)]
+    mats[0].fill_(1.0)
+    dsq = torch.zeros(1, dtype=torch.float64, device=cuda)
+    torch.cuda.synchronize()
+    rc = lib.pdot_primal_pass_f64_noalloc(m, n, mats[0].data_ptr(), mats[1].data_ptr(), mats[2].data_ptr(),
+                                          rows[0].data_ptr(), cols[0].data_ptr(), 1.0, 1.0, 1.0, 0,
+                                          rows[1].data_ptr(), cols[1].data_ptr(), dsq.data_ptr(), None)
+    torch.cuda.synchronize()
     assert rc == _abi.PDOT_ERR_TOO_LARGE
     assert "scratch" in _abi.last_error(lib)
+    del mats
+    torch.cuda.empty_cache()

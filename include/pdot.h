@@ -167,6 +167,9 @@ typedef struct pdot_solver_options {
    * copies it has in flight, sets its error word and returns, and the call
    * fails with PDOT_ERR_CUDA. It exercises the timeout path without a fault. */
   int32_t fail_bounded_waits;
+  /* > 0 with warm-start duals: the initial primal weight, in place of
+   * primal_importance (or the scale-invariant choice); <= 0: that choice. */
+  double warm_primal_weight;
 } pdot_solver_options;
 
 /* ---- output -------------------------------------------------------------- */
@@ -345,6 +348,9 @@ typedef struct pdot_batch_problem {
    * PDOT_TERMINATION_REASON_OTHER at the same evaluation; a warm start and a
    * cold start of one problem raced this way finish as soon as the faster one. */
   const int32_t* race_groups;
+  /* Initial primal weights of warm instances (NULL, or entries <= 0: the
+   * parameters' choice), like pdot_solver_options.warm_primal_weight. */
+  const double* warm_primal_weights;
 } pdot_batch_problem;
 
 typedef struct pdot_batch_output {          /* one per instance; arrays may be NULL */

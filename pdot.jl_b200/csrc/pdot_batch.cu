@@ -77,6 +77,7 @@ struct BatchBuffers {
   double* evpart;          // (grid + num) * kEvalSums
   double* vecpart;         // total vector blocks * kVecSums
   const int* warm;         // per instance: 1 when it starts from a warm start
+  const double* warm_omega;// per instance: initial primal weight of a warm start (> 0), or null
   const int* race;         // per instance: race group (-1: none), or null
   int* winner;             // per group: lowest index of an optimal member (INT_MAX-like when none)
   DevState* st;            // per instance
@@ -948,6 +949,7 @@ __global__ void kb_init_state(BatchBuffers B, SolveConfig cfg, int grid) {
   } else {
     st->primal_weight = cfg.primal_importance;
   }
+  if (B.warm[k] && B.warm_omega && B.warm_omega[k] > 0.0) st->primal_weight = B.warm_omega[k];
   st->iteration = 1;
   st->last_rp = st->l2_rhs;
   st->ratio_last_trial = 1.0;
@@ -1154,6 +1156,15 @@ class BatchSolver {
     any_warm_ = false;
     for (int k = 0; k < B; ++k) any_warm_ = any_warm_ || warm[k];
     D_.warm = upload(warm.data(), B);
+    if (P.warm_primal_weights) {
+      std::vector<double> om(B, 0.0);
+      for (int k = 0; k < B; ++k) {
+        const double w = P.warm_primal_weights[k];
+        if (!std::isfinite(w)) bfail(PDOT_ERR_INVALID_ARGUMENT, "instance %d: warm_primal_weight must be finite", k);
+        om[k] = (warm[k] && w > 0.0) ? w : 0.0;
+      }
+      D_.warm_omega = upload(om.data(), B);
+    }
     if (any_warm_) {
       std::vector<double> hu(ro, 0.0), hv(co, 0.0), hr(ro, 0.0), hc(co, 0.0);
       std::vector<float> hx;

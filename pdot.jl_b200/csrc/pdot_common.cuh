@@ -22,6 +22,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <cuda_runtime.h>
 
 #include "pdot.h"
@@ -119,6 +120,7 @@ struct DevState {
   long long num_stats;       // iteration-stats records written
   long long primal_passes;   // fused primal passes that ran
   long long fresh_passes;    // of those, passes that started a new average
+  long long xsums_iter;      // loop body whose primal pass left the next evaluation's plan sums (-1: none)
   int numerical_error;
   int g_is_zero;             // the stored gradient is still its initial 0
   int done;
@@ -152,6 +154,7 @@ struct SolveConfig {
   double primal_importance;
   double cost_scale;         // given scale (> 0) or 0: normalise by the max
   int warm_start;            // duals were given: the stored gradient is C - u - v
+  double warm_primal_weight; // > 0 with a warm start: the initial primal weight
 };
 
 struct Buffers {
@@ -187,9 +190,12 @@ inline size_t pass_scratch_doubles(const Geometry& g) {
 }
 
 cudaError_t launch_init(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
-cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s);
+// xsums = 1: the next loop body evaluates; the pass also leaves that
+// evaluation's plan sums (k1_primal_xs), so the evaluation reads only the cost.
+cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s, int xsums = 0);
 cudaError_t launch_dual(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
-cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
+cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s,
+                        int xsums = 0);
 // start_only = 1: a warm start's initial point becomes the last restart
 // point; nothing else of the evaluation block runs.
 cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s,
@@ -242,6 +248,19 @@ struct WarmPlanArgs {
   double eps;
 };
 cudaError_t launch_warm_plan(const WarmPlanArgs& A, int iterations, cudaStream_t s);
+
+// Large host <-> device copies (pdot_transfer.cu): one DMA for page-locked host
+// memory, a two-buffer pinned staging pipeline with parallel host copies for
+// pageable memory. Both return after the copy has completed.
+constexpr size_t kTransferChunk = size_t(8) << 20;  // doubles per staged chunk (64 MiB)
+bool host_is_pinned(const void* p);
+cudaError_t copy_to_device(void* dst, const void* src, size_t bytes, cudaStream_t s);
+// The device data of `count` doubles from element `off` of the array being
+// copied out: the device address, after enqueueing on `s` whatever makes it
+// ready (at most kTransferChunk doubles; `slot` alternates 0 / 1 between
+// consecutive chunks, so a producer can double-buffer its own scratch).
+using ChunkSource = std::function<const double*(size_t off, size_t count, int slot, cudaStream_t s)>;
+cudaError_t copy_to_host(double* dst, size_t count, const ChunkSource& source, cudaStream_t s);
 
 // Sets the thread-local text pdot_last_error() returns (pdot_host.cu).
 void set_last_error(const char* msg);

@@ -11,6 +11,7 @@
 // and stops once the device has set `done`. All decisions (step size, restart,
 // primal weight, termination) are taken on the device.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -132,6 +133,7 @@ struct Variant {
   int plan_iters = 0;
   int staged = 2;  // 0 direct, 1 staged, 2 automatic
   int fail_waits = 0;  // test hook: the staged pass's waits report timeouts
+  double warm_omega = 0.0;  // > 0: initial primal weight of a warm start
 };
 
 Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
@@ -186,6 +188,10 @@ Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
   if (o->fail_bounded_waits != 0 && o->fail_bounded_waits != 1)
     fail(PDOT_ERR_INVALID_ARGUMENT, "fail_bounded_waits must be 0 or 1");
   v.fail_waits = o->fail_bounded_waits;
+  if (!std::isfinite(o->warm_primal_weight)) fail(PDOT_ERR_INVALID_ARGUMENT, "warm_primal_weight must be finite");
+  if (o->warm_primal_weight > 0.0 && !o->warm_dual_source)
+    fail(PDOT_ERR_INVALID_ARGUMENT, "warm_primal_weight needs the warm-start duals");
+  v.warm_omega = o->warm_primal_weight > 0.0 ? o->warm_primal_weight : 0.0;
   return v;
 }
 
@@ -288,7 +294,7 @@ class Solver {
       } else {
         double* C = nullptr;
         alloc(&C, N);
-        CK(cudaMemcpyAsync(C, P.cost_matrix, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        CK(pdot::copy_to_device(C, P.cost_matrix, N * sizeof(double), stream_));
         cost_.C = C;
       }
     } else {
@@ -300,7 +306,7 @@ class Solver {
       DeviceTemp tmp;
       if (!device_inputs) {
         CK(cudaMalloc(&tmp.p, N * sizeof(double)));
-        CK(cudaMemcpyAsync(tmp.p, P.cost_matrix, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        CK(pdot::copy_to_device(tmp.p, P.cost_matrix, N * sizeof(double), stream_));
         src = tmp.get<const double>();
       }
       CK(pdot::launch_convert_cost(src, Cs, var.cost_kind, N, stream_));
@@ -370,7 +376,7 @@ class Solver {
       DeviceTemp tmp, work;
       if (!device_inputs) {
         CK(cudaMalloc(&tmp.p, std::max<size_t>(N, 1) * sizeof(double)));
-        CK(cudaMemcpyAsync(tmp.p, var.warm_x, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        CK(pdot::copy_to_device(tmp.p, var.warm_x, N * sizeof(double), stream_));
         src = tmp.get<const double>();
       }
       if (var.plan_f32)
@@ -449,6 +455,7 @@ class Solver {
     cfg_ = make_config(prm);
     cfg_.cost_scale = var.cost_scale;
     cfg_.warm_start = warm_u_ != nullptr;
+    cfg_.warm_primal_weight = var.warm_omega;
     freq_ = prm.termination_evaluation_frequency;
     limit_ = prm.termination_criteria.iteration_limit;
     if (use_graph_ && !time_kernels_) capture_regular_chunk();
@@ -563,49 +570,64 @@ class Solver {
 
   // The caller's plan buffer is overwritten in full; fresh host memory (a
   // numpy zeros array, a plain malloc) pays a page fault per 4 KB page on its
-  // first write, which for a large plan costs more than the copy itself. Host
-  // threads therefore write it once while the GPU iterates; the copy back
-  // then finds the pages present.
+  // first write. Host threads therefore write it while the GPU iterates, in
+  // 2 MiB pieces, until the solve ends; the copy back (pdot_transfer.cu) then
+  // finds those pages present and faults the rest itself, in parallel.
+  // Page-locked buffers are resident already and are left alone.
   struct Prefault {
     std::vector<std::thread> threads;
+    std::atomic<bool> stop{false};
     Prefault(double* p, size_t count) {
-      if (!p || count < (size_t(1) << 22)) return;  // small plans: not worth a thread
+      if (!p || count < (size_t(1) << 22) || pdot::host_is_pinned(p)) return;  // small plans: not worth a thread
       const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
       const size_t parts = std::min<size_t>(8, std::max<size_t>(1, hw / 2));
       const size_t per = (count + parts - 1) / parts;
       for (size_t k = 0; k < parts; ++k) {
         const size_t lo = k * per, hi = std::min(count, lo + per);
-        if (lo < hi) threads.emplace_back([p, lo, hi] { memset(p + lo, 0, (hi - lo) * sizeof(double)); });
+        if (lo >= hi) continue;
+        threads.emplace_back([this, p, lo, hi] {
+          const size_t piece = size_t(1) << 18;  // doubles (2 MiB)
+          for (size_t a = lo; a < hi && !stop.load(std::memory_order_relaxed); a += piece)
+            memset(p + a, 0, (std::min(hi, a + piece) - a) * sizeof(double));
+        });
       }
     }
-    ~Prefault() {
+    void finish() {
+      stop.store(true);
       for (std::thread& t : threads) t.join();
+      threads.clear();
     }
+    ~Prefault() { finish(); }
   };
 
   void finish(pdot_saddle_point_output* out) {
     {
       Prefault touch(out->primal_solution, (size_t)g_.m * (size_t)g_.n);
       while (!status_.done) iterate(int64_t(1) << 40);
+      touch.finish();
     }
     // gpu_to_cpu!, src/io.jl:41-53 (average, or current if no average exists)
     const int xb = status_.out_current ? status_.buf : (status_.buf ^ 1);
     const size_t N = (size_t)g_.m * (size_t)g_.n;
     if (out->primal_solution) {
       if (!g_.plan_f32) {
-        CK(cudaMemcpy(out->primal_solution, X_[xb], N * sizeof(double), cudaMemcpyDeviceToHost));
+        const double* X = static_cast<const double*>(X_[xb]);
+        CK(pdot::copy_to_host(out->primal_solution, N,
+                              [X](size_t off, size_t, int, cudaStream_t) { return X + off; }, stream_));
       } else {
-        // widen the FP32 plan in chunks through a small device buffer
-        const size_t chunk = std::min<size_t>(N, size_t(1) << 24);
+        // widen the FP32 plan chunk by chunk into two device buffers
+        const size_t chunk = std::min<size_t>(N, pdot::kTransferChunk);
         DeviceTemp tmp;
-        CK(cudaMalloc(&tmp.p, std::max<size_t>(chunk, 1) * sizeof(double)));
-        for (size_t off = 0; off < N; off += chunk) {
-          const size_t cnt = std::min(chunk, N - off);
-          CK(pdot::launch_widen(static_cast<const float*>(X_[xb]) + off, tmp.get<double>(), cnt, stream_));
-          CK(cudaMemcpyAsync(out->primal_solution + off, tmp.p, cnt * sizeof(double), cudaMemcpyDeviceToHost,
-                             stream_));
-        }
-        CK(cudaStreamSynchronize(stream_));
+        CK(cudaMalloc(&tmp.p, 2 * std::max<size_t>(chunk, 1) * sizeof(double)));
+        const float* Xf = static_cast<const float*>(X_[xb]);
+        double* buf = tmp.get<double>();
+        CK(pdot::copy_to_host(out->primal_solution, N,
+                              [Xf, buf, chunk](size_t off, size_t cnt, int slot, cudaStream_t s) -> const double* {
+                                double* d = buf + (size_t)slot * chunk;
+                                pdot::launch_widen(Xf + off, d, cnt, s);
+                                return d;
+                              },
+                              stream_));
       }
     }
     if (out->dual_source_solution)
@@ -694,7 +716,8 @@ class Solver {
 
   void enqueue_iteration(long long it, int slot) {
     if (is_eval(it)) timed(slot, kTimedEval, [&] { return pdot::launch_eval(B_, g_, cfg_, stream_); });
-    timed(slot, kTimedPrimal, [&] { return pdot::launch_primal(B_, g_, stream_); });
+    const int xsums = is_eval(it + 1) ? 1 : 0;
+    timed(slot, kTimedPrimal, [&] { return pdot::launch_primal(B_, g_, stream_, xsums); });
     timed(slot, kTimedDual, [&] { return pdot::launch_dual(B_, g_, cfg_, stream_); });
   }
 
@@ -747,7 +770,9 @@ class Solver {
     cudaGraph_t graph = nullptr;
     CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = pdot::launch_eval(B_, g_, cfg_, stream_);
-    for (long long k = 0; k < freq_ && e == cudaSuccess; ++k) e = pdot::launch_step(B_, g_, cfg_, stream_);
+    // the chunk's last step precedes the next chunk's evaluation
+    for (long long k = 0; k < freq_ && e == cudaSuccess; ++k)
+      e = pdot::launch_step(B_, g_, cfg_, stream_, k == freq_ - 1 ? 1 : 0);
     cudaError_t e2 = cudaStreamEndCapture(stream_, &graph);
     CK(e);
     CK(e2);

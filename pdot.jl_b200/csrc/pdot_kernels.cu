@@ -41,14 +41,43 @@ namespace {
 // src/saddle_point_gpu.jl:129-130):
 //   g  = (C - u_i) - v_j ;  t = max(X - s*g, 0) ;  d = t - X ;  X' = X + d
 //   Xavg' = (Xavg + X'*nw)*aw      (Xavg' = X' after a reset of the average)
-template <typename TX, int CK, int R>
+//
+// XS: the next loop body evaluates, so the pass also accumulates that
+// evaluation's plan sums of the updated current and average plans (the
+// E_DOT, E_SQX, E_MAXX fields of k3_eval's partials, current and average) into
+// `evpart`. Each thread visits the same entries in the same order as k3_eval
+// and the block reduction is the same, so the sums are bit-identical to the
+// ones k3_eval would compute from memory; k3_eval then reads only the cost.
+constexpr int kXSums = 6;
+__device__ __forceinline__ void xsums_add(double (&xa)[kXSums], double c, double x, double xav) {
+  xa[0] += c * x;
+  xa[1] += x * x;
+  xa[2] = nanmax(xa[2], fabs(x));
+  xa[3] += c * xav;
+  xa[4] += xav * xav;
+  xa[5] = nanmax(xa[5], fabs(xav));
+}
+__device__ __forceinline__ void xsums_store(double (&xa)[kXSums], double* evpart_cta) {
+  __shared__ double xs_out[kXSums];
+  block_reduce<kXSums>(xa, (1u << 2) | (1u << 5), xs_out);
+  if (threadIdx.x == 0) {
+    evpart_cta[E_DOT] = xs_out[0];
+    evpart_cta[E_SQX] = xs_out[1];
+    evpart_cta[E_MAXX] = xs_out[2];
+    evpart_cta[E_AVG + E_DOT] = xs_out[3];
+    evpart_cta[E_AVG + E_SQX] = xs_out[4];
+    evpart_cta[E_AVG + E_MAXX] = xs_out[5];
+  }
+}
+
+template <typename TX, int CK, int R, bool XS = false>
 __device__ __forceinline__ void primal_pass_body(const CostSource& csrc, float scale, TX* __restrict__ X,
                                                  TX* __restrict__ Xa, const double* __restrict__ u,
                                                  const double* __restrict__ v, const double s,
                                                  const double nw, const double aw, const bool zero_g,
                                                  const bool first, double* __restrict__ colpart,
                                                  double* __restrict__ rowpart, double* __restrict__ sqpart,
-                                                 const Geometry g) {
+                                                 const Geometry g, double* __restrict__ evpart = nullptr) {
   constexpr int RPL = kPanelRows / (32 * R);
   __shared__ double red[kWarps][kPanelRows];
   __shared__ double sqw[kWarps];
@@ -58,6 +87,7 @@ __device__ __forceinline__ void primal_pass_body(const CostSource& csrc, float s
   const int64_t q0 = unit_begin(g, cta), q1 = unit_begin(g, cta + 1);
   CostReader<CK, R, RPL> cost(csrc, scale);
   double sq = 0.0;
+  double xa[kXSums] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   for (int64_t p = q0 / n; p * n < q1; ++p) {
     const int64_t jb = (q0 > p * n ? q0 : p * n) - p * n;
     const int64_t je = (q1 < (p + 1) * n ? q1 : (p + 1) * n) - p * n;
@@ -102,6 +132,7 @@ __device__ __forceinline__ void primal_pass_body(const CostSource& csrc, float s
             acc[k][e] += d;
             cs += d;
             add_sq<TX>(sq, d);
+            if constexpr (XS) xsums_add(xa, widen(cv[k][e]), widen(xv[k][e]), widen(av[k][e]));
           }
           const int64_t idx = base + k * 32 * R;
           vst<TX, R>(X + idx, xv[k]);
@@ -134,11 +165,12 @@ __device__ __forceinline__ void primal_pass_body(const CostSource& csrc, float s
     for (int w = 1; w < kWarps; ++w) s2 += sqw[w];
     sqpart[cta] = s2;
   }
+  if constexpr (XS) xsums_store(xa, evpart + cta * kEvalSums);
 }
 
-template <typename TX, int CK, int R>
-__global__ void __launch_bounds__(kThreads, 2) k1_primal(Buffers B, Geometry g) {
-  const DevState* st = B.st;
+template <typename TX, int CK, int R, bool XS>
+__device__ __forceinline__ void k1_primal_impl(const Buffers& B, const Geometry& g) {
+  DevState* st = B.st;
   if (st->done | st->numerical_error) return;
   const int buf = st->buf;
   const double tau = st->step_size, omega = st->primal_weight, S = st->sum_weights;
@@ -149,9 +181,20 @@ __global__ void __launch_bounds__(kThreads, 2) k1_primal(Buffers B, Geometry g) 
   const double s = __ddiv_rn(tau, omega);
   const double nw = first ? 1.0 : __ddiv_rn(tau, S);
   const double aw = first ? 1.0 : __ddiv_rn(S, __dadd_rn(S, tau));
-  primal_pass_body<TX, CK, R>(B.cost, (float)st->cost_scale, static_cast<TX*>(B.X[buf]),
-                              static_cast<TX*>(B.X[buf ^ 1]), B.u[buf], B.v[buf], s, nw, aw, zero_g, first,
-                              B.colpart, B.rowpart, B.sqpart, g);
+  primal_pass_body<TX, CK, R, XS>(B.cost, (float)st->cost_scale, static_cast<TX*>(B.X[buf]),
+                                  static_cast<TX*>(B.X[buf ^ 1]), B.u[buf], B.v[buf], s, nw, aw, zero_g, first,
+                                  B.colpart, B.rowpart, B.sqpart, g, B.evpart);
+  if (XS && blockIdx.x == 0 && threadIdx.x == 0) st->xsums_iter = st->iteration;
+}
+
+template <typename TX, int CK, int R>
+__global__ void __launch_bounds__(kThreads, 2) k1_primal(Buffers B, Geometry g) {
+  k1_primal_impl<TX, CK, R, false>(B, g);
+}
+// the same pass before an evaluation: it also leaves the evaluation's plan sums
+template <typename TX, int CK, int R>
+__global__ void __launch_bounds__(kThreads, 2) k1_primal_xs(Buffers B, Geometry g) {
+  k1_primal_impl<TX, CK, R, true>(B, g);
 }
 
 template <int R>
@@ -190,8 +233,8 @@ struct StagedLayout {
   static constexpr int kSmem = kRingBytes + kWarps * S * 8;  // plus the mbarriers
 };
 
-template <typename TX, int CK>
-__global__ void __launch_bounds__(kThreads, 2) k1_primal_staged(Buffers B, Geometry g) {
+template <typename TX, int CK, bool XS>
+__device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Geometry& g) {
   using L = StagedLayout<TX, CK>;
   constexpr int R = 16 / sizeof(TX);
   constexpr int RPL = kPanelRows / (32 * R);
@@ -257,6 +300,7 @@ __global__ void __launch_bounds__(kThreads, 2) k1_primal_staged(Buffers B, Geome
   // hook); the drain after a failure always polls up to kSpinLimit times
   const int polls = g.fail_waits ? 0 : kSpinLimit;
   double sq = 0.0;
+  double xa[kXSums] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   for (int64_t p = q0 / n; p * n < q1; ++p) {
     const int64_t row0 = p * kPanelRows;
     double acc[RPL][R];
@@ -308,6 +352,7 @@ __global__ void __launch_bounds__(kThreads, 2) k1_primal_staged(Buffers B, Geome
             acc[k][e] += d;
             cs += d;
             add_sq<TX>(sq, d);
+            if constexpr (XS) xsums_add(xa, widen(cv[e]), widen(xv[e]), widen(av[e]));
           }
           vst<TX, R>(X + base + k * 32 * R, xv);
           vst<TX, R>(Xa + base + k * 32 * R, av);
@@ -352,6 +397,20 @@ __global__ void __launch_bounds__(kThreads, 2) k1_primal_staged(Buffers B, Geome
     for (int w = 1; w < kWarps; ++w) s2 += sqw[w];
     B.sqpart[cta] = s2;
   }
+  if constexpr (XS) {
+    xsums_store(xa, B.evpart + cta * kEvalSums);
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->xsums_iter = st->iteration;
+  }
+}
+
+template <typename TX, int CK>
+__global__ void __launch_bounds__(kThreads, 2) k1_primal_staged(Buffers B, Geometry g) {
+  k1_primal_staged_impl<TX, CK, false>(B, g);
+}
+// the same pass before an evaluation: it also leaves the evaluation's plan sums
+template <typename TX, int CK>
+__global__ void __launch_bounds__(kThreads, 2) k1_primal_staged_xs(Buffers B, Geometry g) {
+  k1_primal_staged_impl<TX, CK, true>(B, g);
 }
 
 // Second stage of the row sum of row i / column sum of column j.
@@ -430,6 +489,12 @@ __global__ void __launch_bounds__(kVecThreads) k2_dual(Buffers B, Geometry g, So
 // before the first accepted step) and, when an average exists, the average
 // point, the sums <C,X>, ||X||^2, max|X|, ||min(G,0)||^2, max|min(G,0)|
 // (src/utils_gpu.jl:84,102-103,39,52,108; src/saddle_point_gpu.jl:313,325).
+//
+// When the primal pass of the previous loop body already left the plan sums
+// (k1_primal_xs: xsums_iter is the previous loop body), only the cost is read
+// and only the reduced-cost sums are written; otherwise every sum is computed
+// here (the first evaluation, a warm start's initial point, an evaluation
+// after a numerical error stopped the step kernels).
 template <typename TX, int CK, int R>
 __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
   DevState* st = B.st;
@@ -439,6 +504,7 @@ __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
   const int buf = st->buf;
   const bool have_avg = st->avg_count > 0;
   const bool zero_g = st->g_is_zero != 0;
+  const bool need_x = st->xsums_iter != st->iteration - 1;
   CostReader<CK, R, RPL> cost(B.cost, (float)st->cost_scale);
   const TX* __restrict__ X = static_cast<const TX*>(B.X[buf]);
   const TX* __restrict__ Xa = static_cast<const TX*>(B.X[buf ^ 1]);
@@ -482,8 +548,10 @@ __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
         if (ok[k]) {
           const int64_t idx = base + k * 32 * R;
           cost.get(idx, k, cv[k]);
-          vldg<TX, R>(X + idx, xv[k]);
-          if (have_avg) vldg<TX, R>(Xa + idx, av[k]);
+          if (need_x) {
+            vldg<TX, R>(X + idx, xv[k]);
+            if (have_avg) vldg<TX, R>(Xa + idx, av[k]);
+          }
         }
       }
 #pragma unroll
@@ -491,21 +559,26 @@ __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
         if (ok[k]) {
 #pragma unroll
           for (int e = 0; e < R; ++e) {
-            const double c = widen(cv[k][e]), x = widen(xv[k][e]);
+            const double c = widen(cv[k][e]);
             const double gg = zero_g ? 0.0 : __dsub_rn(__dsub_rn(c, ur[k][e]), vj);
             const double mg = neg_part(gg);
-            acc[E_DOT] += c * x;
-            acc[E_SQX] += x * x;
-            acc[E_MAXX] = nanmax(acc[E_MAXX], fabs(x));
+            if (need_x) {
+              const double x = widen(xv[k][e]);
+              acc[E_DOT] += c * x;
+              acc[E_SQX] += x * x;
+              acc[E_MAXX] = nanmax(acc[E_MAXX], fabs(x));
+            }
             acc[E_SQG] += mg * mg;
             acc[E_MAXG] = nanmax(acc[E_MAXG], mg);
             if (have_avg) {
-              const double xa = widen(av[k][e]);
               const double ga = __dsub_rn(__dsub_rn(c, uar[k][e]), vaj);
               const double mga = neg_part(ga);
-              acc[E_AVG + E_DOT] += c * xa;
-              acc[E_AVG + E_SQX] += xa * xa;
-              acc[E_AVG + E_MAXX] = nanmax(acc[E_AVG + E_MAXX], fabs(xa));
+              if (need_x) {
+                const double xa = widen(av[k][e]);
+                acc[E_AVG + E_DOT] += c * xa;
+                acc[E_AVG + E_SQX] += xa * xa;
+                acc[E_AVG + E_MAXX] = nanmax(acc[E_AVG + E_MAXX], fabs(xa));
+              }
               acc[E_AVG + E_SQG] += mga * mga;
               acc[E_AVG + E_MAXG] = nanmax(acc[E_AVG + E_MAXG], mga);
             }
@@ -514,7 +587,21 @@ __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
       }
     }
   }
-  block_reduce<kEvalSums>(acc, kEvalMaxMask, B.evpart + cta * kEvalSums);
+  if (need_x) {
+    block_reduce<kEvalSums>(acc, kEvalMaxMask, B.evpart + cta * kEvalSums);
+  } else {
+    // the plan sums are already in place; the same reduction of the rest
+    __shared__ double gout[4];
+    double gacc[4] = {acc[E_SQG], acc[E_MAXG], acc[E_AVG + E_SQG], acc[E_AVG + E_MAXG]};
+    block_reduce<4>(gacc, (1u << 1) | (1u << 3), gout);
+    if (threadIdx.x == 0) {
+      double* out = B.evpart + cta * kEvalSums;
+      out[E_SQG] = gout[0];
+      out[E_MAXG] = gout[1];
+      out[E_AVG + E_SQG] = gout[2];
+      out[E_AVG + E_MAXG] = gout[3];
+    }
+  }
 }
 
 // start_only: the evaluation of a warm start's initial point, run once after
@@ -648,6 +735,7 @@ __global__ void __launch_bounds__(kThreads, 2) k0_init(Buffers B, Geometry g, So
       } else {
         st->primal_weight = cfg.primal_importance;
       }
+      if (cfg.warm_start && cfg.warm_primal_weight > 0.0) st->primal_weight = cfg.warm_primal_weight;
       st->kkt_passes = 0.0;
       st->sum_weights = 0.0;
       st->avg_count = 0;
@@ -670,6 +758,7 @@ __global__ void __launch_bounds__(kThreads, 2) k0_init(Buffers B, Geometry g, So
       st->num_stats = 0;
       st->primal_passes = 0;
       st->fresh_passes = 0;
+      st->xsums_iter = -1;
       st->eval_time_sec = 0.0;
       st->done = 0;
       st->termination_reason = 0;
@@ -748,30 +837,31 @@ __global__ void k_widen(const float* __restrict__ src, double* __restrict__ dst,
     }                                                                                      \
   } while (0)
 
-// The staged fused pass exists for the 16-byte path of every variant.
-#define PDOT_STAGED_VARIANT(g, LAUNCH)                                                              \
+// The staged fused pass exists for the 16-byte path of every variant
+// (KERNEL: k1_primal_staged or k1_primal_staged_xs).
+#define PDOT_STAGED_VARIANT(g, KERNEL, LAUNCH)                                                      \
   do {                                                                                            \
-    if (!(g).plan_f32) { auto kfn = k1_primal_staged<double, PDOT_COST_F64>;                     \
+    if (!(g).plan_f32) { auto kfn = KERNEL<double, PDOT_COST_F64>;                               \
       constexpr int smem = StagedLayout<double, PDOT_COST_F64>::kSmem; LAUNCH; }                 \
-    else if ((g).cost_kind == PDOT_COST_F32) { auto kfn = k1_primal_staged<float, PDOT_COST_F32>; \
+    else if ((g).cost_kind == PDOT_COST_F32) { auto kfn = KERNEL<float, PDOT_COST_F32>;           \
       constexpr int smem = StagedLayout<float, PDOT_COST_F32>::kSmem; LAUNCH; }                  \
-    else if ((g).cost_kind == PDOT_COST_BF16) { auto kfn = k1_primal_staged<float, PDOT_COST_BF16>; \
+    else if ((g).cost_kind == PDOT_COST_BF16) { auto kfn = KERNEL<float, PDOT_COST_BF16>;         \
       constexpr int smem = StagedLayout<float, PDOT_COST_BF16>::kSmem; LAUNCH; }                 \
-    else if ((g).cost_kind == kCostSqBase + 1) { auto kfn = k1_primal_staged<float, kCostSqBase + 1>; \
+    else if ((g).cost_kind == kCostSqBase + 1) { auto kfn = KERNEL<float, kCostSqBase + 1>;       \
       constexpr int smem = StagedLayout<float, kCostSqBase + 1>::kSmem; LAUNCH; }                \
-    else if ((g).cost_kind == kCostSqBase + 2) { auto kfn = k1_primal_staged<float, kCostSqBase + 2>; \
+    else if ((g).cost_kind == kCostSqBase + 2) { auto kfn = KERNEL<float, kCostSqBase + 2>;       \
       constexpr int smem = StagedLayout<float, kCostSqBase + 2>::kSmem; LAUNCH; }                \
-    else if ((g).cost_kind == kCostSqBase + 3) { auto kfn = k1_primal_staged<float, kCostSqBase + 3>; \
+    else if ((g).cost_kind == kCostSqBase + 3) { auto kfn = KERNEL<float, kCostSqBase + 3>;       \
       constexpr int smem = StagedLayout<float, kCostSqBase + 3>::kSmem; LAUNCH; }                \
-    else if ((g).cost_kind == kCostSqBase + 4) { auto kfn = k1_primal_staged<float, kCostSqBase + 4>; \
+    else if ((g).cost_kind == kCostSqBase + 4) { auto kfn = KERNEL<float, kCostSqBase + 4>;       \
       constexpr int smem = StagedLayout<float, kCostSqBase + 4>::kSmem; LAUNCH; }                \
-    else if ((g).cost_kind == kCostL1Base + 1) { auto kfn = k1_primal_staged<float, kCostL1Base + 1>; \
+    else if ((g).cost_kind == kCostL1Base + 1) { auto kfn = KERNEL<float, kCostL1Base + 1>;       \
       constexpr int smem = StagedLayout<float, kCostL1Base + 1>::kSmem; LAUNCH; }                \
-    else if ((g).cost_kind == kCostL1Base + 2) { auto kfn = k1_primal_staged<float, kCostL1Base + 2>; \
+    else if ((g).cost_kind == kCostL1Base + 2) { auto kfn = KERNEL<float, kCostL1Base + 2>;       \
       constexpr int smem = StagedLayout<float, kCostL1Base + 2>::kSmem; LAUNCH; }                \
-    else if ((g).cost_kind == kCostL1Base + 3) { auto kfn = k1_primal_staged<float, kCostL1Base + 3>; \
+    else if ((g).cost_kind == kCostL1Base + 3) { auto kfn = KERNEL<float, kCostL1Base + 3>;       \
       constexpr int smem = StagedLayout<float, kCostL1Base + 3>::kSmem; LAUNCH; }                \
-    else { auto kfn = k1_primal_staged<float, kCostL1Base + 4>;                                   \
+    else { auto kfn = KERNEL<float, kCostL1Base + 4>;                                             \
       constexpr int smem = StagedLayout<float, kCostL1Base + 4>::kSmem; LAUNCH; }                \
   } while (0)
 
@@ -798,7 +888,7 @@ Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device, int plan_f3
   g.pad_ = 0;
   int occ = 1;
   if (g.tma) {
-    PDOT_STAGED_VARIANT(g, {
+    PDOT_STAGED_VARIANT(g, k1_primal_staged, {
       g.tma_smem = smem;
       if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, kThreads, smem) != cudaSuccess || occ < 1) {
@@ -807,6 +897,19 @@ Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device, int plan_f3
         occ = 1;
       }
     });
+    // the variant before an evaluation runs on the same grid
+    if (g.tma) {
+      int occ_xs = 0;
+      PDOT_STAGED_VARIANT(g, k1_primal_staged_xs, {
+        if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_xs, kfn, kThreads, smem) != cudaSuccess)
+          cudaGetLastError();
+      });
+      if (occ_xs < 1) {
+        g.tma = 0;
+        occ = 1;
+      }
+    }
   }
   if (!g.tma) PDOT_VARIANT(g, k1_primal, occ = blocks_per_sm(kfn));
   int64_t grid = (int64_t)sms * occ;
@@ -832,9 +935,13 @@ cudaError_t launch_init(const Buffers& B, const Geometry& g, const SolveConfig& 
   return cudaGetLastError();
 }
 
-cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s) {
-  if (g.tma)
-    PDOT_STAGED_VARIANT(g, (kfn<<<g.grid, kThreads, smem, s>>>(B, g)));
+cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s, int xsums) {
+  if (g.tma && xsums)
+    PDOT_STAGED_VARIANT(g, k1_primal_staged_xs, (kfn<<<g.grid, kThreads, smem, s>>>(B, g)));
+  else if (g.tma)
+    PDOT_STAGED_VARIANT(g, k1_primal_staged, (kfn<<<g.grid, kThreads, smem, s>>>(B, g)));
+  else if (xsums)
+    PDOT_VARIANT(g, k1_primal_xs, (kfn<<<g.grid, kThreads, 0, s>>>(B, g)));
   else
     PDOT_VARIANT(g, k1_primal, (kfn<<<g.grid, kThreads, 0, s>>>(B, g)));
   return cudaGetLastError();
@@ -845,8 +952,8 @@ cudaError_t launch_dual(const Buffers& B, const Geometry& g, const SolveConfig& 
   return cudaGetLastError();
 }
 
-cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s) {
-  cudaError_t e = launch_primal(B, g, s);
+cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s, int xsums) {
+  cudaError_t e = launch_primal(B, g, s, xsums);
   if (e != cudaSuccess) return e;
   return launch_dual(B, g, cfg, s);
 }

@@ -261,6 +261,7 @@ struct CSolverOptions                           # pdot_solver_options
     warm_plan_epsilon::Float64
     warm_plan_iterations::Int32
     fail_bounded_waits::Int32
+    warm_primal_weight::Float64
 end
 
 struct CBatchProblem                            # pdot_batch_problem
@@ -276,6 +277,7 @@ struct CBatchProblem                            # pdot_batch_problem
     warm_dual_targets::Ptr{Ptr{Float64}}
     warm_primals::Ptr{Ptr{Float64}}
     race_groups::Ptr{Int32}
+    warm_primal_weights::Ptr{Float64}
 end
 
 struct CBatchOutput                             # pdot_batch_output
@@ -343,12 +345,13 @@ function solver_options(; device::Integer = 0, precision::Symbol = :f64, cost::U
                         point_dim::Integer = 0, source_points::Ptr{Float32} = Ptr{Float32}(0),
                         target_points::Ptr{Float32} = Ptr{Float32}(0), u0::Ptr{Float64} = Ptr{Float64}(0),
                         v0::Ptr{Float64} = Ptr{Float64}(0), X0::Ptr{Float64} = Ptr{Float64}(0),
-                        recover_plan = nothing, primal_pass::Integer = 0, ctas_per_sm::Integer = 0)
+                        recover_plan = nothing, primal_pass::Integer = 0, ctas_per_sm::Integer = 0,
+                        warm_primal_weight::Real = 0.0)
     c = cost === nothing ? (precision == :f64 ? :f64 : :f32) : cost
     eps, rounds = recover_plan === nothing ? (0.0, 0) : (Float64(recover_plan[1]), Int(recover_plan[2]))
     return CSolverOptions(Int32(device), Int32(1), Int32(0), PRECISIONS[precision], COSTS[c], Int32(point_dim),
                           source_points, target_points, 0.0, u0, v0, Int32(primal_pass), Int32(ctas_per_sm), X0,
-                          eps, Int32(rounds), (Int32(0),))
+                          eps, Int32(rounds), Int32(0), Float64(warm_primal_weight))
 end
 
 # points are given one per row (m x dim); the C ABI reads them row-major
@@ -495,7 +498,7 @@ function optimize_batched(params::PdhgParameters, problems::Vector{OptimalTransp
                            warm_starts === nothing ? Ptr{Ptr{Float64}}(0) : pointer(wu),
                            warm_starts === nothing ? Ptr{Ptr{Float64}}(0) : pointer(wv),
                            warm_starts === nothing ? Ptr{Ptr{Float64}}(0) : pointer(wx),
-                           isempty(groups) ? Ptr{Int32}(0) : pointer(groups))
+                           isempty(groups) ? Ptr{Int32}(0) : pointer(groups), Ptr{Float64}(0))
         rc = ccall((:pdot_optimize_batched, libpdot), Cint,
                    (Ref{CBatchProblem}, Ref{CPdhgParameters}, Ref{CSolverOptions}, Ptr{CBatchOutput}, Ref{Float64}),
                    bp, to_c(params), opts, outs, seconds)

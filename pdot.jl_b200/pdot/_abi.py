@@ -101,6 +101,7 @@ class SolverOptionsC(ct.Structure):
         ("warm_plan_epsilon", ct.c_double),
         ("warm_plan_iterations", ct.c_int32),
         ("fail_bounded_waits", ct.c_int32),
+        ("warm_primal_weight", ct.c_double),
     ]
 
 
@@ -137,6 +138,7 @@ class BatchProblemC(ct.Structure):
         ("warm_dual_targets", ct.POINTER(ct.c_void_p)),
         ("warm_primals", ct.POINTER(ct.c_void_p)),
         ("race_groups", ct.POINTER(ct.c_int32)),
+        ("warm_primal_weights", ct.POINTER(ct.c_double)),
     ]
 
 

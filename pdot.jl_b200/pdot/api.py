@@ -371,7 +371,7 @@ _COSTS = {"f64": _abi.COST_F64, "f32": _abi.COST_F32, "bf16": _abi.COST_BF16,
 def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, precision: str = "f64",
              cost: Optional[str] = None, points=None, cost_scale: Optional[float] = None, warm_start=None,
              device_pointers: bool = False, primal_pass: str = "auto", recover_plan=None,
-             fail_bounded_waits: bool = False):
+             fail_bounded_waits: bool = False, warm_primal_weight: Optional[float] = None):
     """Build pdot_solver_options. Returns (options, objects to keep alive).
 
     precision  "f64" (the drop-in) or "f32" (mixed precision: FP32 plan)
@@ -386,6 +386,8 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
                of exp((u_i + v_j - C_ij) / eps)
     fail_bounded_waits  test hook: the staged pass's waits report a timeout at
                once (the call then fails with PDOT_ERR_CUDA)
+    warm_primal_weight  with a warm start: the initial primal weight (None:
+               primal_importance, or the scale-invariant choice)
     """
     keep = []
     opts = _abi.SolverOptionsC()
@@ -397,6 +399,7 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
         cost = "f64" if precision == "f64" else "f32"
     opts.cost_storage = _COSTS[cost]
     opts.fail_bounded_waits = 1 if fail_bounded_waits else 0
+    opts.warm_primal_weight = float(warm_primal_weight) if warm_primal_weight else 0.0
     if recover_plan is not None:
         opts.warm_plan_epsilon = float(recover_plan[0])
         opts.warm_plan_iterations = int(recover_plan[1])
@@ -443,7 +446,8 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
 def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device: int = 0,
              use_cuda_graph: bool = True, precision: str = "f64", cost: Optional[str] = None, points=None,
              cost_scale: Optional[float] = None, warm_start=None, primal_pass: str = "auto",
-             recover_plan=None, fail_bounded_waits: bool = False) -> SaddlePointOutput:
+             recover_plan=None, fail_bounded_waits: bool = False,
+             warm_primal_weight: Optional[float] = None) -> SaddlePointOutput:
     """PDOT.optimize, src/solver_gpu.jl:413-720, run by libpdot.so on the GPU.
 
     The keyword options beyond `device` select this implementation's mixed
@@ -455,7 +459,8 @@ def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device
     cp = marshal_params(params)
     opts, _keep = _options(device, use_cuda_graph, precision=precision, cost=cost, points=points,
                            cost_scale=cost_scale, warm_start=warm_start, primal_pass=primal_pass,
-                           recover_plan=recover_plan, fail_bounded_waits=fail_bounded_waits)
+                           recover_plan=recover_plan, fail_bounded_waits=fail_bounded_waits,
+                           warm_primal_weight=warm_primal_weight)
     ob = OutputBuffers(mp.m, mp.n, stats_capacity_for(params))
     rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
     _abi.check(lib, rc, "pdot_optimize")
@@ -472,7 +477,7 @@ class Solver:
                  device_problem=None, device: int = 0, use_cuda_graph: bool = True,
                  time_kernels: bool = False, precision: str = "f64", cost: Optional[str] = None,
                  points=None, cost_scale: Optional[float] = None, warm_start=None, primal_pass: str = "auto",
-                 recover_plan=None):
+                 recover_plan=None, warm_primal_weight: Optional[float] = None):
         validate(params)
         self._lib = _abi.load()
         self._params = params
@@ -480,7 +485,7 @@ class Solver:
         opts, self._keep = _options(device, use_cuda_graph, time_kernels, precision=precision, cost=cost,
                                     points=points, cost_scale=cost_scale, warm_start=warm_start,
                                     device_pointers=device_problem is not None, primal_pass=primal_pass,
-                                    recover_plan=recover_plan)
+                                    recover_plan=recover_plan, warm_primal_weight=warm_primal_weight)
         handle = ct.c_void_p()
         if device_problem is not None:
             m, n, cptr, aptr, bptr = device_problem
@@ -537,7 +542,7 @@ class Solver:
 def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", points=None, device: int = 0,
                      use_cuda_graph: bool = True, ctas_per_sm: int = 0, warm_starts=None,
                      return_primal: bool = True, recover_plan=None, race_groups=None,
-                     primal_pass: str = "auto"):
+                     primal_pass: str = "auto", warm_primal_weights=None):
     """Solve many independent instances at once (pdot_optimize_batched).
 
     problems     a list of OptimalTransportProblem (cost_matrix may be None for
@@ -550,6 +555,8 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
     race_groups  None, or a group id per instance (-1: none): once an
                  instance ends optimal, the rest of its group stop (reason OTHER)
     primal_pass  "auto" (staged for coordinate costs), "staged" or "direct"
+    warm_primal_weights  None, or per instance the initial primal weight of its
+                 warm start (<= 0: the parameters' choice)
     return_primal  False leaves every primal_solution None (no m x n copies)
     Returns (outputs, seconds): a SaddlePointOutput per instance (its
     iteration_stats holds the final evaluation record) and the device time.
@@ -635,6 +642,12 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
         bp.warm_dual_sources = wu
         bp.warm_dual_targets = wv
         bp.warm_primals = wx
+    if warm_primal_weights is not None:
+        wo = np.ascontiguousarray(warm_primal_weights, dtype=np.float64)
+        if wo.shape != (B,):
+            raise ValueError("warm_primal_weights needs one entry per instance")
+        keep.append(wo)
+        bp.warm_primal_weights = _dptr(wo)
     opts, _k = _options(device, use_cuda_graph, precision="f32", cost=cost, recover_plan=recover_plan)
     if cost != "f32":
         opts.point_dim = dim

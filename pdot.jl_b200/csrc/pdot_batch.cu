@@ -588,9 +588,17 @@ __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConf
       const long long gp = B.panel_prefix[kk] + p;
       const long long lo = bcta_of_unit(U, grid, ubase + p * I.n), hi = bcta_of_unit(U, grid, ubase + (p + 1) * I.n - 1);
       double sd = 0.0;
-      for (long long c = lo; c <= hi; ++c) {
-        if (bunit_begin(U, grid, c) == bunit_begin(U, grid, c + 1)) continue;
-        sd += B.rowpart[(c + gp) * kPanelRows + t];
+      if (U >= grid) {
+        // every CTA owns a unit: the slots c + gp, c = lo..hi, all hold partials
+        sd = sum_strided(B.rowpart + (lo + gp) * kPanelRows + t, hi - lo + 1, kPanelRows);
+      } else {
+        // fewer units than CTAs (the tail of a solve): skip the empty CTAs,
+        // whose slots hold nothing of this panel (c * U / grid fits 32 bits here)
+        const int u32 = (int)U;
+        for (long long c = lo; c <= hi; ++c) {
+          if ((int)c * u32 / grid == ((int)c + 1) * u32 / grid) continue;
+          sd += B.rowpart[(c + gp) * kPanelRows + t];
+        }
       }
       const long long o = I.row_off + i;
       dual_entry(sd, B.a[o], B.r[buf] + o, B.u[buf] + o, B.r[buf ^ 1] + o, B.u[buf ^ 1] + o, A, vals[0], vals[1]);
@@ -598,8 +606,7 @@ __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConf
   } else {
     const long long j = (lb - I.rblocks) * kVecThreads + threadIdx.x;
     if (j < I.n) {
-      double sd = 0.0;
-      for (long long p = 0; p < I.panels; ++p) sd += B.colpart[ubase + p * I.n + j];
+      const double sd = sum_strided(B.colpart + ubase + j, I.panels, I.n);
       const long long o = I.col_off + j;
       dual_entry(sd, B.b[o], B.c[buf] + o, B.v[buf] + o, B.c[buf ^ 1] + o, B.v[buf ^ 1] + o, A, vals[0], vals[1]);
     }

@@ -413,18 +413,16 @@ __global__ void __launch_bounds__(kThreads, 2) k1_primal_staged_xs(Buffers B, Ge
   k1_primal_staged_impl<TX, CK, true>(B, g);
 }
 
-// Second stage of the row sum of row i / column sum of column j.
+// Second stage of the row sum of row i / column sum of column j: the partial
+// slots added in a fixed order (sum_strided).
 __device__ __forceinline__ double finish_row_sum(const Geometry& g, const double* rowpart, int64_t i) {
   const int64_t p = i / kPanelRows, t = i - p * kPanelRows;
   const int64_t lo = cta_of_unit(g, p * g.n), hi = cta_of_unit(g, (p + 1) * g.n - 1);
-  double s = 0.0;
-  for (int64_t c = lo; c <= hi; ++c) s += rowpart[row_slot(c, p) * kPanelRows + t];
-  return s;
+  // slots row_slot(c, p) = c + p for c = lo..hi are consecutive
+  return sum_strided(rowpart + row_slot(lo, p) * kPanelRows + t, hi - lo + 1, kPanelRows);
 }
 __device__ __forceinline__ double finish_col_sum(const Geometry& g, const double* colpart, int64_t j) {
-  double s = 0.0;
-  for (int64_t p = 0; p < g.panels; ++p) s += colpart[p * g.n + j];
-  return s;
+  return sum_strided(colpart + j, g.panels, g.n);
 }
 
 // Stand-alone stage two for pdot_primal_pass_f64: delta row/column sums and

@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--no-mp", action="store_true", help="skip the mixed-precision variants")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the m=n=1000 and m=n=10000 configuration blocks (c1, c2)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--precision", choices=["f64", "f32"], default="f64",
                     help="plan precision of the primary workload (f64: the drop-in)")
     ap.add_argument("--cost", choices=["f64", "f32", "bf16", "sqeuclid"], default=None,
@@ -651,7 +652,7 @@ def run_ours(args, world, rank, local):
     c2 = run_c2(args, device, local) if not args.no_configs else None
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(full_problem_host(xs, ys, a_h, b_h), m, n, steps=5, warmup=2)
 
     value = world * iters / (ms / 1000.0)

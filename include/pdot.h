@@ -170,6 +170,11 @@ typedef struct pdot_solver_options {
   /* > 0 with warm-start duals: the initial primal weight, in place of
    * primal_importance (or the scale-invariant choice); <= 0: that choice. */
   double warm_primal_weight;
+  /* Batched solver: its matrix passes cut the units (one column of one
+   * 256-row panel) of all active instances into CTA ranges of equal cost, a
+   * unit costing its rows plus batch_unit_cost * 256 (the per-unit overhead,
+   * 0..8, in eighths). 0 balances the rows alone. */
+  double batch_unit_cost;
 } pdot_solver_options;
 
 /* ---- output -------------------------------------------------------------- */

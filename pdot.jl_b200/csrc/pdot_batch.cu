@@ -9,8 +9,12 @@
 // coordinates (squared-Euclidean or L1).
 //
 // Work decomposition: the units (one column of one 256-row panel) of all active
-// instances are concatenated into one line and cut into equal contiguous CTA
-// ranges, exactly as the single-instance pass cuts one instance's line. Row
+// instances are concatenated into one line and cut into contiguous CTA ranges
+// of equal cost, a unit costing its rows plus a fixed per-unit overhead (the
+// autotuner picks it). The units of uneven instances carry from 1 to 256 rows,
+// so ranges of equal unit count would leave some CTAs with several times the
+// bytes of others. kb_compact recomputes the ranges (cta_begin) whenever the
+// active list changes. Row
 // partials live in slot (cta + global panel), column partials at the global
 // unit index, per-instance sums of squares and evaluation partials in slot
 // (cta + active index): along the line the owning CTA, the global panel and
@@ -52,7 +56,7 @@ struct BatchInstance {
 
 struct BatchActive {
   int count;
-  int pad_;
+  int any_empty;          // some CTA range holds no unit (only in the tail of a solve)
   long long total_units;
 };
 
@@ -87,13 +91,23 @@ struct BatchBuffers {
   long long* unit_prefix;  // active prefix of units (count + 1)
   long long* panel_prefix; // active prefix of panels
   long long* vblock_prefix;// active prefix of vector blocks
+  long long* cost_prefix;  // active prefix of the units' balancing cost (count + 1)
+  long long* cta_begin;    // grid + 1: CTA c owns the active units [cta_begin[c], cta_begin[c + 1])
+  int unit_cost;           // per-unit overhead of the balancing cost, in eighths of 256 rows
 };
 
-__device__ __forceinline__ long long bunit_begin(long long units, int grid, long long cta) {
-  return cta * units / grid;
-}
-__device__ __forceinline__ long long bcta_of_unit(long long units, int grid, long long q) {
-  return ((q + 1) * (long long)grid - 1) / units;
+// The CTA that owns active unit q: the largest c with cta_begin[c] <= q (an
+// empty range c has cta_begin[c] == cta_begin[c + 1], so the search passes it).
+__device__ __forceinline__ long long bcta_of_unit(const long long* cta_begin, int grid, long long q) {
+  int lo = 0, hi = grid - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (cta_begin[mid] <= q)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
 }
 // largest k in [0, count) with prefix[k] <= q
 __device__ __forceinline__ int find_segment(const long long* prefix, int count, long long q) {
@@ -120,7 +134,7 @@ __device__ __forceinline__ bool elect_last_of(unsigned int* ticket, unsigned int
 
 // Fixed-order sum of the non-empty CTA slots [lo, hi] (+ offset) of K values.
 template <int K>
-__device__ __forceinline__ void sum_cta_slots(const double* part, long long units, int grid, long long lo,
+__device__ __forceinline__ void sum_cta_slots(const double* part, const long long* cta_begin, long long lo,
                                               long long hi, long long slot_off, unsigned maxmask,
                                               double (&out)[K]) {
   const int lane = threadIdx.x & 31;
@@ -129,7 +143,7 @@ __device__ __forceinline__ void sum_cta_slots(const double* part, long long unit
     const bool mx = (maxmask >> k) & 1u;
     double acc = 0.0;
     for (long long c = lo + lane; c <= hi; c += 32) {
-      if (bunit_begin(units, grid, c) == bunit_begin(units, grid, c + 1)) continue;  // empty CTA
+      if (cta_begin[c] == cta_begin[c + 1]) continue;  // empty CTA
       const double v = __ldcg(part + (c + slot_off) * K + k);
       acc = mx ? nanmax(acc, v) : acc + v;
     }
@@ -150,10 +164,8 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
   __shared__ double sqw[kWarps];
   const BatchActive act = *B.act;
   if (act.count == 0) return;
-  const long long U = act.total_units;
-  const int G = gridDim.x;
   const long long cta = blockIdx.x;
-  const long long q0 = bunit_begin(U, G, cta), q1 = bunit_begin(U, G, cta + 1);
+  const long long q0 = B.cta_begin[cta], q1 = B.cta_begin[cta + 1];
   if (q0 >= q1) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int kk = find_segment(B.unit_prefix, act.count, q0);
@@ -382,10 +394,8 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
   __shared__ double sqw[kWarps];
   const BatchActive act = *B.act;
   if (act.count == 0) return;
-  const long long U = act.total_units;
-  const int G = gridDim.x;
   const long long cta = blockIdx.x;
-  const long long q0 = bunit_begin(U, G, cta), q1 = bunit_begin(U, G, cta + 1);
+  const long long q0 = B.cta_begin[cta], q1 = B.cta_begin[cta + 1];
   if (q0 >= q1) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned char* ring = smem + (size_t)warp * S * L::kStageBytes;
@@ -416,6 +426,8 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
   BatchCursor prod;
   prod.init(B, act.count, q0, q1, warp);
   long long issued = 0, consumed = 0;
+  int cstage = 0;           // consumed % S, kept incrementally (no 64-bit division per unit)
+  uint32_t cphase = 0;      // (consumed / S) & 1
   for (int t = 0; t < S && prod.valid; ++t) {
     if (lane == 0) issue(prod, t);
     prod.advance(B, act.count, q0, q1, warp);
@@ -469,8 +481,8 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
       const long long jb = (ql0 > p * I.n ? ql0 : p * I.n) - p * I.n;
       const long long je = (ql1 < (p + 1) * I.n ? ql1 : (p + 1) * I.n) - p * I.n;
       for (long long j = jb + warp; !failed && j < je; j += kWarps) {
-        const int stage = (int)(consumed % S);
-        const uint32_t parity = (uint32_t)((consumed / S) & 1);
+        const int stage = cstage;
+        const uint32_t parity = cphase;
         if (!mbar_wait_bounded(bar0 + 8 * stage, parity)) {
           failed = true;
           if (lane == 0) atomicExch(&st->kernel_error, 1);
@@ -518,6 +530,10 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
         if (lane == 0) B.colpart[base_u + p * I.n + j] = cs;
         __syncwarp();
         ++consumed;
+        if (++cstage == S) {
+          cstage = 0;
+          cphase ^= 1u;
+        }
         if (prod.valid) {
           if (lane == 0) issue(prod, stage);
           prod.advance(B, act.count, q0, q1, warp);
@@ -570,7 +586,6 @@ __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConf
   const int k = B.ids[kk];
   const BatchInstance I = B.inst[k];
   DevState* st = B.st + k;
-  const long long U = act.total_units;
   const long long lb = blk - B.vblock_prefix[kk];  // block inside the instance
   const int buf = st->buf;
   const double tau = st->step_size, omega = st->primal_weight, S = st->sum_weights;
@@ -586,17 +601,16 @@ __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConf
     if (i < I.m) {
       const long long p = i / kPanelRows, t = i - p * kPanelRows;
       const long long gp = B.panel_prefix[kk] + p;
-      const long long lo = bcta_of_unit(U, grid, ubase + p * I.n), hi = bcta_of_unit(U, grid, ubase + (p + 1) * I.n - 1);
+      const long long lo = bcta_of_unit(B.cta_begin, grid, ubase + p * I.n), hi = bcta_of_unit(B.cta_begin, grid, ubase + (p + 1) * I.n - 1);
       double sd = 0.0;
-      if (U >= grid) {
+      if (!act.any_empty) {
         // every CTA owns a unit: the slots c + gp, c = lo..hi, all hold partials
         sd = sum_strided(B.rowpart + (lo + gp) * kPanelRows + t, hi - lo + 1, kPanelRows);
       } else {
-        // fewer units than CTAs (the tail of a solve): skip the empty CTAs,
-        // whose slots hold nothing of this panel (c * U / grid fits 32 bits here)
-        const int u32 = (int)U;
+        // some CTA ranges are empty (the tail of a solve): skip them, their
+        // slots hold nothing of this panel
         for (long long c = lo; c <= hi; ++c) {
-          if ((int)c * u32 / grid == ((int)c + 1) * u32 / grid) continue;
+          if (B.cta_begin[c] == B.cta_begin[c + 1]) continue;
           sd += B.rowpart[(c + gp) * kPanelRows + t];
         }
       }
@@ -617,8 +631,8 @@ __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConf
     double rs[kStepSums], cs[kStepSums], xs[1];
     warp_reduce_partials<kStepSums>(B.steppart, B.vblock_prefix[kk], I.rblocks, 0u, rs);
     warp_reduce_partials<kStepSums>(B.steppart, B.vblock_prefix[kk] + I.rblocks, I.cblocks, 0u, cs);
-    const long long lo = bcta_of_unit(U, grid, ubase), hi = bcta_of_unit(U, grid, B.unit_prefix[kk + 1] - 1);
-    sum_cta_slots<1>(B.sqpart, U, grid, lo, hi, kk, 0u, xs);
+    const long long lo = bcta_of_unit(B.cta_begin, grid, ubase), hi = bcta_of_unit(B.cta_begin, grid, B.unit_prefix[kk + 1] - 1);
+    sum_cta_slots<1>(B.sqpart, B.cta_begin, lo, hi, kk, 0u, xs);
     if (threadIdx.x == 0) {
       step_control(st, cfg, rs[0], cs[0], xs[0], rs[1] + cs[1]);
       st->ticket_step = 0;
@@ -631,10 +645,8 @@ template <int CK>
 __global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
   const BatchActive act = *B.act;
   if (act.count == 0) return;
-  const long long U = act.total_units;
-  const int G = gridDim.x;
   const long long cta = blockIdx.x;
-  const long long q0 = bunit_begin(U, G, cta), q1 = bunit_begin(U, G, cta + 1);
+  const long long q0 = B.cta_begin[cta], q1 = B.cta_begin[cta + 1];
   if (q0 >= q1) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int kk = find_segment(B.unit_prefix, act.count, q0);
@@ -643,7 +655,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
     const int k = B.ids[kk];
     const BatchInstance I = B.inst[k];
     DevState* st = B.st + k;
-    if (cta == bcta_of_unit(U, G, B.unit_prefix[kk]) && threadIdx.x == 0) st->eval_t0_ns = globaltimer_ns();
+    if (cta == bcta_of_unit(B.cta_begin, (int)gridDim.x, B.unit_prefix[kk]) && threadIdx.x == 0) st->eval_t0_ns = globaltimer_ns();
     const long long base_u = B.unit_prefix[kk];
     const long long seg_end = min(q1, (long long)B.unit_prefix[kk + 1]);
     const int buf = st->buf;
@@ -777,11 +789,10 @@ __global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, Solve
   block_reduce<kVecSums>(acc, kVecMaxMask, B.vecpart + blk * kVecSums);
   if (!elect_last_of(&st->ticket_eval, (unsigned)(I.rblocks + I.cblocks))) return;
   if (threadIdx.x < 32) {
-    const long long U = act.total_units;
-    const long long lo = bcta_of_unit(U, grid, B.unit_prefix[kk]);
-    const long long hi = bcta_of_unit(U, grid, B.unit_prefix[kk + 1] - 1);
+    const long long lo = bcta_of_unit(B.cta_begin, grid, B.unit_prefix[kk]);
+    const long long hi = bcta_of_unit(B.cta_begin, grid, B.unit_prefix[kk + 1] - 1);
     double E[kEvalSums], R[kVecSums], Cc[kVecSums];
-    sum_cta_slots<kEvalSums>(B.evpart, U, grid, lo, hi, kk, kEvalMaxMask, E);
+    sum_cta_slots<kEvalSums>(B.evpart, B.cta_begin, lo, hi, kk, kEvalMaxMask, E);
     warp_reduce_partials<kVecSums>(B.vecpart, B.vblock_prefix[kk], I.rblocks, kVecMaxMask, R);
     warp_reduce_partials<kVecSums>(B.vecpart, B.vblock_prefix[kk] + I.rblocks, I.cblocks, kVecMaxMask, Cc);
     if (threadIdx.x == 0) {
@@ -796,11 +807,22 @@ __global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, Solve
   }
 }
 
-// Rebuild the active list and its prefix sums (one CTA, instances in order).
-__global__ void kb_compact(BatchBuffers B) {
+// Rebuild the active list and its prefix sums (one CTA, instances in order),
+// then the CTA ranges: CTA c starts at the first active unit whose cumulative
+// cost reaches c / grid of the total, a unit costing 8 * rows + unit_cost * 256
+// (integers, so the split is exact and repeatable). Within an instance the
+// units run panel-major, n units of 256 rows per full panel and n units of the
+// remaining rows in the last panel, so the start of a range follows in closed
+// form after a binary search over the instances' cost prefix.
+__global__ void kb_compact(BatchBuffers B, int grid) {
   __shared__ int flags[1024];
   __shared__ int base;
-  if (threadIdx.x == 0) base = 0;
+  __shared__ long long total_cost;
+  __shared__ int empty_flag;
+  if (threadIdx.x == 0) {
+    base = 0;
+    empty_flag = 0;
+  }
   if (B.race) {
     // racing instances: once a member of a group is optimal, the others stop
     for (int k = threadIdx.x; k < B.num; k += blockDim.x) {
@@ -820,7 +842,8 @@ __global__ void kb_compact(BatchBuffers B) {
     }
   }
   __syncthreads();
-  long long units = 0, panels = 0, vblocks = 0;
+  long long units = 0, panels = 0, vblocks = 0, cost = 0;
+  const long long wu = (long long)B.unit_cost * kPanelRows;
   for (int off = 0; off < B.num; off += 1024) {
     const int k = off + threadIdx.x;
     flags[threadIdx.x] = (k < B.num && !B.st[k].done) ? 1 : 0;
@@ -835,32 +858,75 @@ __global__ void kb_compact(BatchBuffers B) {
         B.unit_prefix[c] = units;
         B.panel_prefix[c] = panels;
         B.vblock_prefix[c] = vblocks;
+        B.cost_prefix[c] = cost;
         units += I.panels * I.n;
         panels += I.panels;
         vblocks += I.rblocks + I.cblocks;
+        cost += I.n * (8 * I.m + wu * I.panels);
         ++c;
       }
       base = c;
       B.unit_prefix[c] = units;
       B.panel_prefix[c] = panels;
       B.vblock_prefix[c] = vblocks;
+      B.cost_prefix[c] = cost;
     }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
     B.act->count = base;
     B.act->total_units = units;
+    total_cost = cost;
   }
+  __syncthreads();
+  const int count = base;
+  const long long W = total_cost;
+  for (int c = threadIdx.x; c <= grid; c += blockDim.x) {
+    long long q;
+    if (count == 0 || c == 0) {
+      q = 0;
+    } else if (c == grid) {
+      q = B.unit_prefix[count];
+    } else {
+      const long long T = (long long)c * W / grid;
+      // the largest kk with cost_prefix[kk] <= T (plain loads: written above)
+      int lo = 0, hi = count - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (B.cost_prefix[mid] <= T)
+          lo = mid;
+        else
+          hi = mid - 1;
+      }
+      const BatchInstance& I = B.inst[B.ids[lo]];
+      const long long e = T - B.cost_prefix[lo];
+      const long long uf = 8 * kPanelRows + wu;                          // a unit of a full panel
+      const long long ul = 8 * (I.m - kPanelRows * (I.panels - 1)) + wu;  // a unit of the last panel
+      const long long F = I.n * uf;                                      // a full panel
+      long long local;
+      if (e < (I.panels - 1) * F) {
+        const long long p = e / F;
+        local = p * I.n + (e - p * F + uf - 1) / uf;
+      } else {
+        local = (I.panels - 1) * I.n + (e - (I.panels - 1) * F + ul - 1) / ul;
+      }
+      q = B.unit_prefix[lo] + local;
+    }
+    B.cta_begin[c] = q;
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < grid; c += blockDim.x)
+    if (B.cta_begin[c] == B.cta_begin[c + 1]) empty_flag = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) B.act->any_empty = empty_flag;
 }
 
 // Per-instance cost norms (stage one, over the full unit line).
 template <int CK>
 __global__ void __launch_bounds__(kThreads, 2) kb_norms(BatchBuffers B) {
   const BatchActive act = *B.act;
-  const long long U = act.total_units;
-  const int G = gridDim.x;
   const long long cta = blockIdx.x;
-  const long long q0 = bunit_begin(U, G, cta), q1 = bunit_begin(U, G, cta + 1);
+  const long long q0 = B.cta_begin[cta], q1 = B.cta_begin[cta + 1];
   if (q0 >= q1) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int kk = find_segment(B.unit_prefix, act.count, q0);
@@ -920,10 +986,9 @@ __global__ void kb_init_state(BatchBuffers B, SolveConfig cfg, int grid) {
   const int kk = warp_global;
   const int k = B.ids[kk];
   const BatchInstance I = B.inst[k];
-  const long long U = act.total_units;
-  const long long lo = bcta_of_unit(U, grid, B.unit_prefix[kk]), hi = bcta_of_unit(U, grid, B.unit_prefix[kk + 1] - 1);
+  const long long lo = bcta_of_unit(B.cta_begin, grid, B.unit_prefix[kk]), hi = bcta_of_unit(B.cta_begin, grid, B.unit_prefix[kk + 1] - 1);
   double nc[kNormSums];
-  sum_cta_slots<kNormSums>(B.evpart, U, grid, lo, hi, kk, 2u, nc);
+  sum_cta_slots<kNormSums>(B.evpart, B.cta_begin, lo, hi, kk, 2u, nc);
   double sqab = 0.0, mxab = 0.0;
   for (long long i = lane; i < I.m + I.n; i += 32) {
     const double x = i < I.m ? B.a[I.row_off + i] : B.b[I.col_off + i - I.m];
@@ -1097,6 +1162,10 @@ class BatchSolver {
     grid_ = (int)std::min<int64_t>((int64_t)sms * occ, std::max<int64_t>(units, 1));
     if (opt && opt->ctas_per_sm > 0)
       grid_ = (int)std::min<int64_t>((int64_t)std::min(opt->ctas_per_sm, occ) * sms, std::max<int64_t>(units, 1));
+    // per-unit overhead of the CTA split, in eighths of a full unit (0..64)
+    const double uc = opt ? opt->batch_unit_cost : 0.0;
+    if (!(uc >= 0.0 && uc <= 8.0)) bfail(PDOT_ERR_INVALID_ARGUMENT, "batch_unit_cost must be in [0, 8]");
+    D_.unit_cost = (int)std::lround(uc * 8.0);
 
     // device buffers
     D_.inst = upload(inst_.data(), B);
@@ -1270,6 +1339,8 @@ class BatchSolver {
     D_.ids = alloc<int>(B);
     D_.unit_prefix = alloc<long long>(B + 1);
     D_.panel_prefix = alloc<long long>(B + 1);
+    D_.cost_prefix = alloc<long long>(B + 1);
+    D_.cta_begin = alloc<long long>(grid_ + 1);
     D_.vblock_prefix = alloc<long long>(B + 1);
     cfg_ = pdot::SolveConfig{};
     fill_config(prm);
@@ -1385,7 +1456,7 @@ class BatchSolver {
     BCK(cudaMemsetAsync(D_.st, 0, num_ * sizeof(pdot::DevState), stream_));
     if (D_.winner) BCK(cudaMemsetAsync(D_.winner, 0x7F, num_ * sizeof(int), stream_));  // no winner yet
     BCK(cudaMemsetAsync(D_.rec, 0, num_ * sizeof(pdot_iteration_stats), stream_));
-    pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_);
+    pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_, grid_);
     BCK(cudaGetLastError());
     PDOT_BATCH_VARIANT(kind_, pdot::kb_norms, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
     BCK(cudaGetLastError());
@@ -1395,7 +1466,7 @@ class BatchSolver {
       wp_.st = D_.st;  // allocated after the recovery arguments were set up
       BCK(pdot::launch_warm_plan(wp_, plan_iters_, stream_));
     }
-    pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_);  // drops invalid problems
+    pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_, grid_);  // drops invalid problems
     BCK(cudaGetLastError());
     // warm instances start their restart information at the warm point, as
     // the reference starts it at its initial point
@@ -1411,7 +1482,7 @@ class BatchSolver {
   void launch_eval() {
     PDOT_BATCH_VARIANT(kind_, pdot::kb_eval, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
     pdot::kb_eval_vec<<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_, 0);
-    pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_);
+    pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_, grid_);
     BCK(cudaGetLastError());
   }
   static int staged_smem(int kind) {

@@ -251,7 +251,9 @@ cudaError_t launch_warm_plan(const WarmPlanArgs& A, int iterations, cudaStream_t
 
 // Large host <-> device copies (pdot_transfer.cu): one DMA for page-locked host
 // memory, a two-buffer pinned staging pipeline with parallel host copies for
-// pageable memory. Both return after the copy has completed.
+// pageable memory. copy_to_host returns after the copy has completed;
+// copy_to_device may return with a copy from page-locked memory still queued
+// on `s` (the source must stay valid until `s` is synchronised).
 constexpr size_t kTransferChunk = size_t(8) << 20;  // doubles per staged chunk (64 MiB)
 bool host_is_pinned(const void* p);
 cudaError_t copy_to_device(void* dst, const void* src, size_t bytes, cudaStream_t s);

@@ -290,6 +290,8 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
   prod.init(q0, q1, n, warp);
   cons.init(q0, q1, n, warp);
   long long issued = 0, consumed = 0;
+  int cstage = 0;           // consumed % S, kept incrementally (no 64-bit division per unit)
+  uint32_t cphase = 0;      // (consumed / S) & 1
   for (int k = 0; k < S && prod.valid; ++k) {
     if (lane == 0) issue(prod.p, prod.j, k);
     prod.advance(warp);
@@ -319,8 +321,8 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
     cost.panel(row0, lane, m, ok);
     while (!failed && cons.valid && cons.p == p) {
       const int64_t j = cons.j;
-      const int stage = (int)(consumed % S);
-      const uint32_t parity = (uint32_t)((consumed / S) & 1);
+      const int stage = cstage;
+      const uint32_t parity = cphase;
       if (!mbar_wait_bounded(bar0 + 8 * stage, parity, polls)) {
         failed = true;
         break;
@@ -362,6 +364,10 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
       if (lane == 0) B.colpart[p * n + j] = cs;
       __syncwarp();
       ++consumed;
+      if (++cstage == S) {
+        cstage = 0;
+        cphase ^= 1u;
+      }
       cons.advance(warp);
       if (prod.valid) {
         if (lane == 0) issue(prod.p, prod.j, stage);

@@ -95,7 +95,8 @@ bool host_is_pinned(const void* p) {
 }
 
 cudaError_t copy_to_device(void* dst, const void* src, size_t bytes, cudaStream_t s) {
-  if (bytes < kDirectBelow || host_is_pinned(src)) {
+  if (host_is_pinned(src)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  if (bytes < kDirectBelow) {
     PDOT_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
     return cudaStreamSynchronize(s);
   }

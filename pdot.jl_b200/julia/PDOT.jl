@@ -262,6 +262,7 @@ struct CSolverOptions                           # pdot_solver_options
     warm_plan_iterations::Int32
     fail_bounded_waits::Int32
     warm_primal_weight::Float64
+    batch_unit_cost::Float64
 end
 
 struct CBatchProblem                            # pdot_batch_problem
@@ -351,7 +352,7 @@ function solver_options(; device::Integer = 0, precision::Symbol = :f64, cost::U
     eps, rounds = recover_plan === nothing ? (0.0, 0) : (Float64(recover_plan[1]), Int(recover_plan[2]))
     return CSolverOptions(Int32(device), Int32(1), Int32(0), PRECISIONS[precision], COSTS[c], Int32(point_dim),
                           source_points, target_points, 0.0, u0, v0, Int32(primal_pass), Int32(ctas_per_sm), X0,
-                          eps, Int32(rounds), Int32(0), Float64(warm_primal_weight))
+                          eps, Int32(rounds), Int32(0), Float64(warm_primal_weight), 0.0)
 end
 
 # points are given one per row (m x dim); the C ABI reads them row-major

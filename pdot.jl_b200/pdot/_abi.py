@@ -102,6 +102,7 @@ class SolverOptionsC(ct.Structure):
         ("warm_plan_iterations", ct.c_int32),
         ("fail_bounded_waits", ct.c_int32),
         ("warm_primal_weight", ct.c_double),
+        ("batch_unit_cost", ct.c_double),
     ]
 
 

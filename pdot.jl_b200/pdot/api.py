@@ -542,7 +542,7 @@ class Solver:
 def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", points=None, device: int = 0,
                      use_cuda_graph: bool = True, ctas_per_sm: int = 0, warm_starts=None,
                      return_primal: bool = True, recover_plan=None, race_groups=None,
-                     primal_pass: str = "auto", warm_primal_weights=None):
+                     primal_pass: str = "auto", warm_primal_weights=None, unit_cost: float = 0.25):
     """Solve many independent instances at once (pdot_optimize_batched).
 
     problems     a list of OptimalTransportProblem (cost_matrix may be None for
@@ -557,6 +557,9 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
     primal_pass  "auto" (staged for coordinate costs), "staged" or "direct"
     warm_primal_weights  None, or per instance the initial primal weight of its
                  warm start (<= 0: the parameters' choice)
+    unit_cost    the matrix passes cut the active units into CTA ranges of
+                 equal cost, a unit costing its rows + unit_cost * 256 (0..8,
+                 in eighths); tune_batched picks it
     return_primal  False leaves every primal_solution None (no m x n copies)
     Returns (outputs, seconds): a SaddlePointOutput per instance (its
     iteration_stats holds the final evaluation record) and the device time.
@@ -652,6 +655,7 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
     if cost != "f32":
         opts.point_dim = dim
     opts.ctas_per_sm = int(ctas_per_sm)
+    opts.batch_unit_cost = float(unit_cost)
     opts.primal_pass = {"auto": _abi.PASS_AUTO, "staged": _abi.PASS_STAGED, "direct": _abi.PASS_DIRECT}[primal_pass]
     cp = marshal_params(params)
     sec = ct.c_double(0.0)
@@ -666,23 +670,35 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
 
 
 BATCH_TUNING_CANDIDATES = [{"primal_pass": pp, "ctas_per_sm": c} for pp in ("staged", "direct") for c in (2, 1)]
+BATCH_UNIT_COSTS = (0.0, 0.125, 0.25, 0.5, 8.0)
 
 
 def tune_batched(params: PdhgParameters, problems, *, cost: str = "f32", points=None, device: int = 0,
-                 iterations: int = 256, candidates=None):
+                 iterations: int = 256, candidates=None, unit_costs=BATCH_UNIT_COSTS):
     """The batched solver's autotuner: times the first `iterations` iterations
-    of the batch under every candidate launch configuration (the primal pass,
-    staged by bulk copies or direct, and the resident CTAs per SM of the
-    matrix passes) and returns (best configuration, [(configuration,
-    seconds)]). Pass the configuration's keys to optimize_batched."""
+    of the batch under candidate configurations and returns (best
+    configuration, [(configuration, seconds)]); pass the configuration's keys
+    to optimize_batched. First the launch configuration (the primal pass,
+    staged by bulk copies or direct, times the resident CTAs per SM of the
+    matrix passes), then, for the best of those, the tile balance: the
+    per-unit overhead that the CTA split charges beside a unit's rows (0 cuts
+    ranges of equal rows, 8 nearly equal unit counts)."""
     import copy
 
     p = copy.deepcopy(params)
     p.termination_criteria.iteration_limit = int(iterations)
     timings = []
-    for cand in candidates or BATCH_TUNING_CANDIDATES:
+
+    def run(cand):
         _, sec = optimize_batched(p, problems, cost=cost, points=points, device=device, return_primal=False,
                                   **cand)
         timings.append((dict(cand), sec))
+
+    for cand in candidates or BATCH_TUNING_CANDIDATES:
+        run({**cand, "unit_cost": 0.25})
+    best = dict(min(timings, key=lambda t: t[1])[0])
+    for uc in unit_costs:
+        if uc != best["unit_cost"]:
+            run({**best, "unit_cost": uc})
     best = min(timings, key=lambda t: t[1])[0]
     return best, timings

@@ -122,7 +122,38 @@ def test_batched_staged_and_direct_passes_agree(cuda, cost):
 def test_autotuner_times_every_candidate_and_picks_the_fastest(cuda):
     probs, pts = instances.batched_l1(count=12, lo=32, hi=400, seed=2)
     best, timings = pdot.tune_batched(pdot.default_parameters(1e-4), probs, cost="l1", points=pts, iterations=64)
-    assert len(timings) == len(pdot.api.BATCH_TUNING_CANDIDATES)
+    # the launch configurations at the default balance, then the other balances for the best of them
+    others = [c for c in pdot.api.BATCH_UNIT_COSTS if c != 0.25]
+    assert len(timings) == len(pdot.api.BATCH_TUNING_CANDIDATES) + len(others)
     assert best == min(timings, key=lambda t: t[1])[0]
     outs, _ = pdot.optimize_batched(pdot.default_parameters(1e-4), probs, cost="l1", points=pts, **best)
     assert all(o.termination_reason == OPTIMAL for o in outs)
+
+
+@pytest.mark.parametrize("unit_cost", [0.0, 0.125, 8.0])
+def test_cost_balanced_cta_split_solves_every_instance(cuda, unit_cost):
+    """The CTA ranges cut the units by cost (rows + unit_cost * 256). Every
+    split must cover each unit once: the solves end optimal with objectives in
+    the tolerance band of the default split's, whatever the order of the sums,
+    and each split is deterministic. Sizes of 3 to 700 rows and columns give
+    partial panels and short units, and a tail of few active units, where
+    ranges can hold no unit."""
+    tol = 1e-4
+    probs, pts = instances.batched_l1(count=20, lo=3, hi=700, seed=9)
+    params = pdot.default_parameters(tol)
+    ref, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts)
+    got, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts, unit_cost=unit_cost)
+    again, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts, unit_cost=unit_cost)
+    for r, g, g2 in zip(ref, got, again):
+        assert g.termination_reason == OPTIMAL
+        assert np.array_equal(g.primal_solution, g2.primal_solution)
+        ro = r.iteration_stats[-1].convergence_information[0].primal_objective
+        go = g.iteration_stats[-1].convergence_information[0].primal_objective
+        assert abs(go - ro) <= 2 * tol * (1 + abs(ro))
+
+
+def test_batch_unit_cost_is_validated(cuda):
+    probs, pts = instances.batched_l1(count=2, lo=8, hi=16, seed=1)
+    with pytest.raises(pdot.api._abi.PdotError) as ei:
+        pdot.optimize_batched(pdot.default_parameters(1e-4), probs, cost="l1", points=pts, unit_cost=9.0)
+    assert ei.value.code == pdot.api._abi.PDOT_ERR_INVALID_ARGUMENT

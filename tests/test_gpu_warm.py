@@ -39,17 +39,22 @@ def test_exact_warm_start_stops_at_the_first_evaluation(cuda):
 
 @pytest.mark.parametrize("m,n", [(64, 48), (257, 130)])
 def test_warm_start_matches_the_oracle_early(cuda, m, n):
+    """Records of iterations 1-10 and the forced one at 129: past the
+    artificial restarts of the first iterations, the adaptive restart test
+    compares against the last restart point, which a warm start sets to its
+    own start point (its residuals, gap and norms), on both sides."""
     prob = instances.uniform_sqeuclid(m, n, seed=m)
     params = pdot.default_parameters(1e-4)
     cold = oracle.optimize(params, prob)
     u0, v0, X0 = _perturbed(cold, np.random.default_rng(1), 0.05)
-    p10 = pdot.default_parameters(1e-4, iteration_limit=10)
-    g = pdot.optimize(p10, prob, warm_start=(u0, v0, X0))
-    o = oracle.optimize_warm(p10, prob, u0, v0, X0)
+    p128 = pdot.default_parameters(1e-4, iteration_limit=128)
+    g = pdot.optimize(p128, prob, warm_start=(u0, v0, X0))
+    o = oracle.optimize_warm(p128, prob, u0, v0, X0)
     assert len(g.iteration_stats) == len(o.iteration_stats)
     for a, b in zip(g.iteration_stats, o.iteration_stats):
         assert a.restart_used == b.restart_used
         assert a.step_size == pytest.approx(b.step_size, rel=1e-9)
+        assert a.primal_weight == pytest.approx(b.primal_weight, rel=1e-9)
         ca, cb = a.convergence_information[0], b.convergence_information[0]
         for f in ("primal_objective", "dual_objective", "l2_primal_residual", "l2_dual_residual"):
             assert getattr(ca, f) == pytest.approx(getattr(cb, f), rel=1e-9, abs=1e-14), f
@@ -127,3 +132,16 @@ def test_race_groups_stop_the_slower_member(cuda):
     assert out[2].termination_reason == OPTIMAL and out[2].iteration_count == cold[1].iteration_count
     with pytest.raises(pdot._abi.PdotError):
         pdot.optimize_batched(params, batch, cost="l1", points=bpts, race_groups=[0, 3, -1])
+
+
+def test_warm_primal_weight_is_the_initial_weight(cuda):
+    prob = instances.uniform_sqeuclid(60, 50, seed=6)
+    params = pdot.default_parameters(1e-4, iteration_limit=3)
+    cold = oracle.optimize(pdot.default_parameters(1e-4), prob)
+    u0, v0, X0 = _perturbed(cold, np.random.default_rng(4), 0.05)
+    g = pdot.optimize(params, prob, warm_start=(u0, v0, X0), warm_primal_weight=7.5)
+    o = oracle.optimize_warm(params, prob, u0, v0, X0, omega0=7.5)
+    assert g.iteration_stats[0].primal_weight == 7.5
+    for a, b in zip(g.iteration_stats, o.iteration_stats):
+        assert a.primal_weight == pytest.approx(b.primal_weight, rel=1e-9)
+        assert a.step_size == pytest.approx(b.step_size, rel=1e-9)

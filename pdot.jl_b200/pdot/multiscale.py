@@ -76,6 +76,34 @@ def c_transform(points: np.ndarray, centres: np.ndarray, dual: np.ndarray, scale
     return out
 
 
+def learned_to_fine_duals(xs, ys, a, b, starter, *, scale: float | None = None, floor: float = 1e-6):
+    """Warm-start duals (u, v) for the fine problem from the learned network
+    instead of a coarse solve: both point sets are binned on the network's
+    32 x 32 grid over their common bounding square, the network predicts the
+    grid problem's duals (its cost is the squared grid distance divided by its
+    maximum, 2 * 31^2), they are rescaled to the fine cost between cell centres,
+    scale * (side / 32)^2 * |g_I - g_J|^2, and extended to every point by the
+    c-transform over the non-empty cells. `starter` is a learned.WarmStarter;
+    empty cells get `floor` mass before the histograms are renormalised, as the
+    training histograms carry a small floor."""
+    from .learned import SIDE
+
+    G = SIDE
+    s = scale if scale is not None else 1.0 / max_sq_distance(xs, ys)
+    lo, side = bounding_square(xs, ys)
+    A, _ = bin_masses(xs, a, lo, side, G)
+    B, _ = bin_masses(ys, b, lo, side, G)
+    ha = (A + floor) / (A + floor).sum()
+    hb = (B + floor) / (B + floor).sum()
+    U, V = starter.predict(ha[None, :], hb[None, :])
+    kappa = s * (side / G) ** 2 * 2.0 * (G - 1) ** 2
+    cent = cell_centres(lo, side, G)
+    ia, ib = np.nonzero(A > 0)[0], np.nonzero(B > 0)[0]
+    u = c_transform(xs, cent[ib], kappa * V[0][ib], s)
+    v = c_transform(ys, cent[ia], kappa * U[0][ia], s)
+    return u, v, {"cells": [int(ia.size), int(ib.size)]}
+
+
 def coarse_to_fine_duals(xs, ys, a, b, *, G: int = 32, tol: float = 1e-4, iteration_limit: int = 100_000,
                          scale: float | None = None, device: int = 0):
     """Warm-start duals (u, v) for the fine problem, and facts about the coarse solve."""

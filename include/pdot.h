@@ -167,6 +167,11 @@ typedef struct pdot_solver_options {
    * copies it has in flight, sets its error word and returns, and the call
    * fails with PDOT_ERR_CUDA. It exercises the timeout path without a fault. */
   int32_t fail_bounded_waits;
+  /* With a warm start: 0 (default) starts the restart information (the last
+   * restart point of the adaptive restart test and of the primal-weight
+   * update) at the warm point, as the reference starts it at its initial
+   * point; 1 starts it at the zero point, as a cold start's. */
+  int32_t warm_restart_at_zero;
   /* > 0 with warm-start duals: the initial primal weight, in place of
    * primal_importance (or the scale-invariant choice); <= 0: that choice. */
   double warm_primal_weight;

@@ -45,7 +45,7 @@ def load():
     lib.pdot_oracle_optimize_warm.restype = ct.c_int
     lib.pdot_oracle_optimize_warm.argtypes = [
         ct.POINTER(_abi.ProblemC), ct.POINTER(_abi.PdhgParametersC), ct.c_void_p, ct.c_void_p, ct.c_void_p,
-        ct.c_double, ct.POINTER(_abi.SaddlePointOutputC), ct.c_int,
+        ct.c_double, ct.c_int, ct.POINTER(_abi.SaddlePointOutputC), ct.c_int,
     ]
     lib.pdot_oracle_primal_pass.restype = None
     lib.pdot_oracle_primal_pass.argtypes = [
@@ -78,9 +78,11 @@ def optimize(params, problem, num_threads: int = 0):
     return ob.to_output()
 
 
-def optimize_warm(params, problem, u0, v0, X0=None, omega0=0.0, num_threads: int = 0):
+def optimize_warm(params, problem, u0, v0, X0=None, omega0=0.0, num_threads: int = 0,
+                  restart_at_zero: bool = False):
     """The oracle's solve from a warm start (initial duals, optional plan and
-    primal weight)."""
+    primal weight; the restart information starts at the warm point, or at
+    the zero point with `restart_at_zero`)."""
     from pdot import api, _abi
 
     api.validate(params)
@@ -95,7 +97,8 @@ def optimize_warm(params, problem, u0, v0, X0=None, omega0=0.0, num_threads: int
         X0 = np.asfortranarray(X0, dtype=np.float64)
         X0p = X0.ctypes.data
     rc = lib.pdot_oracle_optimize_warm(ct.byref(mp.c), ct.byref(cp), u0.ctypes.data, v0.ctypes.data, X0p,
-                                       float(omega0), ct.byref(ob.c), int(num_threads))
+                                       float(omega0), int(bool(restart_at_zero)), ct.byref(ob.c),
+                                       int(num_threads))
     if rc != 0:
         raise _abi.PdotError(rc, f"oracle optimize failed ({rc})")
     return ob.to_output()

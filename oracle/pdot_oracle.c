@@ -614,12 +614,12 @@ static int ostate_init(ostate* S, const pdot_problem* P) {
 
 /* ---- src/solver_gpu.jl:413-720  optimize ----------------------------- */
 int pdot_oracle_optimize_warm(const pdot_problem* P, const pdot_pdhg_parameters* prm, const double* u0,
-                              const double* v0, const double* X0, double omega0,
+                              const double* v0, const double* X0, double omega0, int restart_at_zero,
                               pdot_saddle_point_output* out, int num_threads);
 
 int pdot_oracle_optimize(const pdot_problem* P, const pdot_pdhg_parameters* prm,
                          pdot_saddle_point_output* out, int num_threads) {
-  return pdot_oracle_optimize_warm(P, prm, NULL, NULL, NULL, 0.0, out, num_threads);
+  return pdot_oracle_optimize_warm(P, prm, NULL, NULL, NULL, 0.0, 0, out, num_threads);
 }
 
 /* Warm start (an addition; the reference always starts at zero,
@@ -627,9 +627,10 @@ int pdot_oracle_optimize(const pdot_problem* P, const pdot_pdhg_parameters* prm,
  * (its row and column sums become r and c) and optional initial primal weight
  * (omega0 > 0). The stored gradient is C - u0 - v0 from the start. The last
  * restart information starts at this initial point, as the reference's does
- * at its own (create_last_restart_info, src/saddle_point_gpu.jl:371-393). */
+ * at its own (create_last_restart_info, src/saddle_point_gpu.jl:371-393), or
+ * at the zero point when restart_at_zero is set. */
 int pdot_oracle_optimize_warm(const pdot_problem* P, const pdot_pdhg_parameters* prm, const double* u0,
-                              const double* v0, const double* X0, double omega0,
+                              const double* v0, const double* X0, double omega0, int restart_at_zero,
                               pdot_saddle_point_output* out, int num_threads) {
   int rc = pdot_oracle_validate(P, prm);
   if (rc != PDOT_OK) return rc;
@@ -673,13 +674,16 @@ int pdot_oracle_optimize_warm(const pdot_problem* P, const pdot_pdhg_parameters*
     }
     for (i64 j = 0; j < n; ++j)
       for (i64 i = 0; i < m; ++i) S->G[i + j * m] = (S->C[i + j * m] - S->u[i]) - S->v[j];
-    /* create_last_restart_info at the initial point */
+    /* create_last_restart_info at the initial point (the copies stay zero
+     * when the restart information starts at the zero point) */
+    if (!restart_at_zero) {
     memcpy(S->Xl, S->X, sizeof(double) * N);
     memcpy(S->Gl, S->G, sizeof(double) * N);
     memcpy(S->ul, S->u, sizeof(double) * m);
     memcpy(S->rl, S->r, sizeof(double) * m);
     memcpy(S->vl, S->v, sizeof(double) * n);
     memcpy(S->cl, S->c, sizeof(double) * n);
+    }
   }
   const double smoothing = prm->restart_params.primal_weight_update_smoothing;
   const double start_time = now_sec();

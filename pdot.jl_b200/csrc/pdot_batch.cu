@@ -1163,6 +1163,9 @@ class BatchSolver {
     if (opt && opt->ctas_per_sm > 0)
       grid_ = (int)std::min<int64_t>((int64_t)std::min(opt->ctas_per_sm, occ) * sms, std::max<int64_t>(units, 1));
     // per-unit overhead of the CTA split, in eighths of a full unit (0..64)
+    if (opt && opt->warm_restart_at_zero != 0 && opt->warm_restart_at_zero != 1)
+      bfail(PDOT_ERR_INVALID_ARGUMENT, "warm_restart_at_zero must be 0 or 1");
+    warm_zero_ = opt && opt->warm_restart_at_zero == 1;
     const double uc = opt ? opt->batch_unit_cost : 0.0;
     if (!(uc >= 0.0 && uc <= 8.0)) bfail(PDOT_ERR_INVALID_ARGUMENT, "batch_unit_cost must be in [0, 8]");
     D_.unit_cost = (int)std::lround(uc * 8.0);
@@ -1469,8 +1472,9 @@ class BatchSolver {
     pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_, grid_);  // drops invalid problems
     BCK(cudaGetLastError());
     // warm instances start their restart information at the warm point, as
-    // the reference starts it at its initial point
-    if (any_warm_) {
+    // the reference starts it at its initial point (unless asked to start at
+    // zero, kb_init_state's record)
+    if (any_warm_ && !warm_zero_) {
       PDOT_BATCH_VARIANT(kind_, pdot::kb_eval, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
       pdot::kb_eval_vec<<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_, 1);
       BCK(cudaGetLastError());
@@ -1573,6 +1577,7 @@ class BatchSolver {
   }
 
   int device_ = 0, num_ = 0, dim_ = 0, kind_ = 0, grid_ = 1;
+  bool warm_zero_ = false;
   bool use_graph_ = true, any_warm_ = false, recover_plans_ = false, staged_ = false;
   int plan_iters_ = 0;
   pdot::WarmPlanArgs wp_{};

@@ -190,8 +190,9 @@ inline size_t pass_scratch_doubles(const Geometry& g) {
 }
 
 cudaError_t launch_init(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
-// xsums = 1: the next loop body evaluates; the pass also leaves that
-// evaluation's plan sums (k1_primal_xs), so the evaluation reads only the cost.
+// xsums = 1: the next loop body evaluates; the direct pass also leaves that
+// evaluation's plan sums (k1_primal_xs), so the evaluation reads only the cost
+// (the staged pass ignores it and the evaluation reads the plans).
 cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s, int xsums = 0);
 cudaError_t launch_dual(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
 cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s,

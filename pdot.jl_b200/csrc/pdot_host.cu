@@ -134,6 +134,7 @@ struct Variant {
   int staged = 2;  // 0 direct, 1 staged, 2 automatic
   int fail_waits = 0;  // test hook: the staged pass's waits report timeouts
   double warm_omega = 0.0;  // > 0: initial primal weight of a warm start
+  bool warm_zero = false;   // a warm start's restart information starts at the zero point
 };
 
 Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
@@ -192,6 +193,9 @@ Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
   if (o->warm_primal_weight > 0.0 && !o->warm_dual_source)
     fail(PDOT_ERR_INVALID_ARGUMENT, "warm_primal_weight needs the warm-start duals");
   v.warm_omega = o->warm_primal_weight > 0.0 ? o->warm_primal_weight : 0.0;
+  if (o->warm_restart_at_zero != 0 && o->warm_restart_at_zero != 1)
+    fail(PDOT_ERR_INVALID_ARGUMENT, "warm_restart_at_zero must be 0 or 1");
+  v.warm_zero = o->warm_restart_at_zero == 1;
   return v;
 }
 
@@ -456,6 +460,7 @@ class Solver {
     cfg_.cost_scale = var.cost_scale;
     cfg_.warm_start = warm_u_ != nullptr;
     cfg_.warm_primal_weight = var.warm_omega;
+    warm_zero_ = var.warm_zero;
     freq_ = prm.termination_evaluation_frequency;
     limit_ = prm.termination_criteria.iteration_limit;
     if (use_graph_ && !time_kernels_) capture_regular_chunk();
@@ -517,8 +522,9 @@ class Solver {
       CK(pdot::launch_warm_plan(wp_, plan_iters_, stream_));
     }
     // a warm start's restart information starts at the warm point, as the
-    // reference's starts at its initial point
-    if (cfg_.warm_start) CK(pdot::launch_eval(B_, g_, cfg_, stream_, 1));
+    // reference's starts at its initial point (unless asked to start at zero,
+    // k0_init's record)
+    if (cfg_.warm_start && !warm_zero_) CK(pdot::launch_eval(B_, g_, cfg_, stream_, 1));
     CK(cudaStreamSynchronize(stream_));
     CK(cudaMemcpy(&status_, st_, sizeof(status_), cudaMemcpyDeviceToHost));
     host_it_ = 1;
@@ -818,6 +824,7 @@ class Solver {
   double* warm_c_ = nullptr;
   double plan_eps_ = 0.0;
   int plan_iters_ = 0;
+  bool warm_zero_ = false;
   pdot::WarmPlanArgs wp_{};
   void* X_[2] = {};
   size_t xbytes_ = sizeof(double);

@@ -233,7 +233,7 @@ struct StagedLayout {
   static constexpr int kSmem = kRingBytes + kWarps * S * 8;  // plus the mbarriers
 };
 
-template <typename TX, int CK, bool XS>
+template <typename TX, int CK>
 __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Geometry& g) {
   using L = StagedLayout<TX, CK>;
   constexpr int R = 16 / sizeof(TX);
@@ -302,7 +302,6 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
   // hook); the drain after a failure always polls up to kSpinLimit times
   const int polls = g.fail_waits ? 0 : kSpinLimit;
   double sq = 0.0;
-  double xa[kXSums] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   for (int64_t p = q0 / n; p * n < q1; ++p) {
     const int64_t row0 = p * kPanelRows;
     double acc[RPL][R];
@@ -354,7 +353,6 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
             acc[k][e] += d;
             cs += d;
             add_sq<TX>(sq, d);
-            if constexpr (XS) xsums_add(xa, widen(cv[e]), widen(xv[e]), widen(av[e]));
           }
           vst<TX, R>(X + base + k * 32 * R, xv);
           vst<TX, R>(Xa + base + k * 32 * R, av);
@@ -403,20 +401,15 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
     for (int w = 1; w < kWarps; ++w) s2 += sqw[w];
     B.sqpart[cta] = s2;
   }
-  if constexpr (XS) {
-    xsums_store(xa, B.evpart + cta * kEvalSums);
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->xsums_iter = st->iteration;
-  }
 }
 
+// The staged pass never carries the evaluation's plan sums: their six FP64
+// accumulators push it past the registers of two CTAs per SM, and the spilling
+// variant measured 1.8x slower on B200 than the plain pass, more than the plan
+// reads it would save the evaluation (8 B per entry with an FP32 plan).
 template <typename TX, int CK>
 __global__ void __launch_bounds__(kThreads, 2) k1_primal_staged(Buffers B, Geometry g) {
-  k1_primal_staged_impl<TX, CK, false>(B, g);
-}
-// the same pass before an evaluation: it also leaves the evaluation's plan sums
-template <typename TX, int CK>
-__global__ void __launch_bounds__(kThreads, 2) k1_primal_staged_xs(Buffers B, Geometry g) {
-  k1_primal_staged_impl<TX, CK, true>(B, g);
+  k1_primal_staged_impl<TX, CK>(B, g);
 }
 
 // Second stage of the row sum of row i / column sum of column j: the partial
@@ -901,19 +894,6 @@ Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device, int plan_f3
         occ = 1;
       }
     });
-    // the variant before an evaluation runs on the same grid
-    if (g.tma) {
-      int occ_xs = 0;
-      PDOT_STAGED_VARIANT(g, k1_primal_staged_xs, {
-        if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_xs, kfn, kThreads, smem) != cudaSuccess)
-          cudaGetLastError();
-      });
-      if (occ_xs < 1) {
-        g.tma = 0;
-        occ = 1;
-      }
-    }
   }
   if (!g.tma) PDOT_VARIANT(g, k1_primal, occ = blocks_per_sm(kfn));
   int64_t grid = (int64_t)sms * occ;
@@ -940,9 +920,7 @@ cudaError_t launch_init(const Buffers& B, const Geometry& g, const SolveConfig& 
 }
 
 cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s, int xsums) {
-  if (g.tma && xsums)
-    PDOT_STAGED_VARIANT(g, k1_primal_staged_xs, (kfn<<<g.grid, kThreads, smem, s>>>(B, g)));
-  else if (g.tma)
+  if (g.tma)
     PDOT_STAGED_VARIANT(g, k1_primal_staged, (kfn<<<g.grid, kThreads, smem, s>>>(B, g)));
   else if (xsums)
     PDOT_VARIANT(g, k1_primal_xs, (kfn<<<g.grid, kThreads, 0, s>>>(B, g)));

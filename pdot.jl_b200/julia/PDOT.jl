@@ -261,6 +261,7 @@ struct CSolverOptions                           # pdot_solver_options
     warm_plan_epsilon::Float64
     warm_plan_iterations::Int32
     fail_bounded_waits::Int32
+    warm_restart_at_zero::Int32
     warm_primal_weight::Float64
     batch_unit_cost::Float64
 end
@@ -347,12 +348,12 @@ function solver_options(; device::Integer = 0, precision::Symbol = :f64, cost::U
                         target_points::Ptr{Float32} = Ptr{Float32}(0), u0::Ptr{Float64} = Ptr{Float64}(0),
                         v0::Ptr{Float64} = Ptr{Float64}(0), X0::Ptr{Float64} = Ptr{Float64}(0),
                         recover_plan = nothing, primal_pass::Integer = 0, ctas_per_sm::Integer = 0,
-                        warm_primal_weight::Real = 0.0)
+                        warm_primal_weight::Real = 0.0, warm_restart_at_zero::Bool = false)
     c = cost === nothing ? (precision == :f64 ? :f64 : :f32) : cost
     eps, rounds = recover_plan === nothing ? (0.0, 0) : (Float64(recover_plan[1]), Int(recover_plan[2]))
     return CSolverOptions(Int32(device), Int32(1), Int32(0), PRECISIONS[precision], COSTS[c], Int32(point_dim),
                           source_points, target_points, 0.0, u0, v0, Int32(primal_pass), Int32(ctas_per_sm), X0,
-                          eps, Int32(rounds), Int32(0), Float64(warm_primal_weight), 0.0)
+                          eps, Int32(rounds), Int32(0), Int32(warm_restart_at_zero), Float64(warm_primal_weight), 0.0)
 end
 
 # points are given one per row (m x dim); the C ABI reads them row-major

@@ -101,6 +101,7 @@ class SolverOptionsC(ct.Structure):
         ("warm_plan_epsilon", ct.c_double),
         ("warm_plan_iterations", ct.c_int32),
         ("fail_bounded_waits", ct.c_int32),
+        ("warm_restart_at_zero", ct.c_int32),
         ("warm_primal_weight", ct.c_double),
         ("batch_unit_cost", ct.c_double),
     ]

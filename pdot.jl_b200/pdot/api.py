@@ -371,7 +371,8 @@ _COSTS = {"f64": _abi.COST_F64, "f32": _abi.COST_F32, "bf16": _abi.COST_BF16,
 def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, precision: str = "f64",
              cost: Optional[str] = None, points=None, cost_scale: Optional[float] = None, warm_start=None,
              device_pointers: bool = False, primal_pass: str = "auto", recover_plan=None,
-             fail_bounded_waits: bool = False, warm_primal_weight: Optional[float] = None):
+             fail_bounded_waits: bool = False, warm_primal_weight: Optional[float] = None,
+             warm_restart: str = "warm"):
     """Build pdot_solver_options. Returns (options, objects to keep alive).
 
     precision  "f64" (the drop-in) or "f32" (mixed precision: FP32 plan)
@@ -388,6 +389,9 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
                once (the call then fails with PDOT_ERR_CUDA)
     warm_primal_weight  with a warm start: the initial primal weight (None:
                primal_importance, or the scale-invariant choice)
+    warm_restart  with a warm start, where the restart information starts:
+               "warm" (the warm point, as the reference's starts at its initial
+               point) or "zero" (the zero point, as a cold start's)
     """
     keep = []
     opts = _abi.SolverOptionsC()
@@ -400,6 +404,7 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
     opts.cost_storage = _COSTS[cost]
     opts.fail_bounded_waits = 1 if fail_bounded_waits else 0
     opts.warm_primal_weight = float(warm_primal_weight) if warm_primal_weight else 0.0
+    opts.warm_restart_at_zero = {"warm": 0, "zero": 1}[warm_restart]
     if recover_plan is not None:
         opts.warm_plan_epsilon = float(recover_plan[0])
         opts.warm_plan_iterations = int(recover_plan[1])
@@ -447,7 +452,7 @@ def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device
              use_cuda_graph: bool = True, precision: str = "f64", cost: Optional[str] = None, points=None,
              cost_scale: Optional[float] = None, warm_start=None, primal_pass: str = "auto",
              recover_plan=None, fail_bounded_waits: bool = False,
-             warm_primal_weight: Optional[float] = None) -> SaddlePointOutput:
+             warm_primal_weight: Optional[float] = None, warm_restart: str = "warm") -> SaddlePointOutput:
     """PDOT.optimize, src/solver_gpu.jl:413-720, run by libpdot.so on the GPU.
 
     The keyword options beyond `device` select this implementation's mixed
@@ -460,7 +465,7 @@ def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device
     opts, _keep = _options(device, use_cuda_graph, precision=precision, cost=cost, points=points,
                            cost_scale=cost_scale, warm_start=warm_start, primal_pass=primal_pass,
                            recover_plan=recover_plan, fail_bounded_waits=fail_bounded_waits,
-                           warm_primal_weight=warm_primal_weight)
+                           warm_primal_weight=warm_primal_weight, warm_restart=warm_restart)
     ob = OutputBuffers(mp.m, mp.n, stats_capacity_for(params))
     rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
     _abi.check(lib, rc, "pdot_optimize")
@@ -477,7 +482,7 @@ class Solver:
                  device_problem=None, device: int = 0, use_cuda_graph: bool = True,
                  time_kernels: bool = False, precision: str = "f64", cost: Optional[str] = None,
                  points=None, cost_scale: Optional[float] = None, warm_start=None, primal_pass: str = "auto",
-                 recover_plan=None, warm_primal_weight: Optional[float] = None):
+                 recover_plan=None, warm_primal_weight: Optional[float] = None, warm_restart: str = "warm"):
         validate(params)
         self._lib = _abi.load()
         self._params = params
@@ -485,7 +490,8 @@ class Solver:
         opts, self._keep = _options(device, use_cuda_graph, time_kernels, precision=precision, cost=cost,
                                     points=points, cost_scale=cost_scale, warm_start=warm_start,
                                     device_pointers=device_problem is not None, primal_pass=primal_pass,
-                                    recover_plan=recover_plan, warm_primal_weight=warm_primal_weight)
+                                    recover_plan=recover_plan, warm_primal_weight=warm_primal_weight,
+                                    warm_restart=warm_restart)
         handle = ct.c_void_p()
         if device_problem is not None:
             m, n, cptr, aptr, bptr = device_problem
@@ -542,7 +548,8 @@ class Solver:
 def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", points=None, device: int = 0,
                      use_cuda_graph: bool = True, ctas_per_sm: int = 0, warm_starts=None,
                      return_primal: bool = True, recover_plan=None, race_groups=None,
-                     primal_pass: str = "auto", warm_primal_weights=None, unit_cost: float = 0.25):
+                     primal_pass: str = "auto", warm_primal_weights=None, unit_cost: float = 0.25,
+                     warm_restart: str = "warm"):
     """Solve many independent instances at once (pdot_optimize_batched).
 
     problems     a list of OptimalTransportProblem (cost_matrix may be None for
@@ -557,6 +564,8 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
     primal_pass  "auto" (staged for coordinate costs), "staged" or "direct"
     warm_primal_weights  None, or per instance the initial primal weight of its
                  warm start (<= 0: the parameters' choice)
+    warm_restart "warm" or "zero": where warm instances start their restart
+                 information (see _options)
     unit_cost    the matrix passes cut the active units into CTA ranges of
                  equal cost, a unit costing its rows + unit_cost * 256 (0..8,
                  in eighths); tune_batched picks it
@@ -651,7 +660,8 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
             raise ValueError("warm_primal_weights needs one entry per instance")
         keep.append(wo)
         bp.warm_primal_weights = _dptr(wo)
-    opts, _k = _options(device, use_cuda_graph, precision="f32", cost=cost, recover_plan=recover_plan)
+    opts, _k = _options(device, use_cuda_graph, precision="f32", cost=cost, recover_plan=recover_plan,
+                        warm_restart=warm_restart)
     if cost != "f32":
         opts.point_dim = dim
     opts.ctas_per_sm = int(ctas_per_sm)

@@ -73,3 +73,19 @@ def test_timeout_hook_is_validated_before_device_work(built):
     rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
     assert rc == _abi.PDOT_ERR_INVALID_ARGUMENT
     assert "fail_bounded_waits" in _abi.last_error(lib)
+
+
+def test_warm_restart_flag_is_validated_before_device_work(built):
+    prob = instances.uniform_sqeuclid(4, 3, seed=0)
+    lib = _abi.load()
+    mp = api.MarshalledProblem(prob)
+    cp = api.marshal_params(pdot.default_parameters(1e-4))
+    opts = _abi.SolverOptionsC()
+    opts.use_cuda_graph = 1
+    opts.warm_restart_at_zero = 3
+    ob = api.OutputBuffers(4, 3, 16)
+    rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
+    assert rc == _abi.PDOT_ERR_INVALID_ARGUMENT
+    assert "warm_restart_at_zero" in _abi.last_error(lib)
+    with pytest.raises(KeyError):
+        api._options(0, True, warm_restart="later")

@@ -145,3 +145,25 @@ def test_warm_primal_weight_is_the_initial_weight(cuda):
     for a, b in zip(g.iteration_stats, o.iteration_stats):
         assert a.primal_weight == pytest.approx(b.primal_weight, rel=1e-9)
         assert a.step_size == pytest.approx(b.step_size, rel=1e-9)
+
+
+@pytest.mark.parametrize("m,n", [(64, 48)])
+def test_warm_restart_at_zero_matches_the_oracle(cuda, m, n):
+    """With warm_restart="zero" the restart information starts at the zero
+    point, as a cold start's, on both sides."""
+    prob = instances.uniform_sqeuclid(m, n, seed=m + 1)
+    cold = oracle.optimize(pdot.default_parameters(1e-4), prob)
+    u0, v0, X0 = _perturbed(cold, np.random.default_rng(3), 0.05)
+    p128 = pdot.default_parameters(1e-4, iteration_limit=128)
+    g = pdot.optimize(p128, prob, warm_start=(u0, v0, X0), warm_restart="zero")
+    o = oracle.optimize_warm(p128, prob, u0, v0, X0, restart_at_zero=True)
+    w = oracle.optimize_warm(p128, prob, u0, v0, X0)
+    assert len(g.iteration_stats) == len(o.iteration_stats)
+    for a, b in zip(g.iteration_stats, o.iteration_stats):
+        assert a.restart_used == b.restart_used
+        assert a.step_size == pytest.approx(b.step_size, rel=1e-9)
+        assert a.primal_weight == pytest.approx(b.primal_weight, rel=1e-9)
+        ca, cb = a.convergence_information[0], b.convergence_information[0]
+        assert ca.primal_objective == pytest.approx(cb.primal_objective, rel=1e-9, abs=1e-14)
+    # the two records differ: the first primal-weight update measures from a different point
+    assert [s.primal_weight for s in o.iteration_stats] != [s.primal_weight for s in w.iteration_stats]

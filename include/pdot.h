@@ -397,6 +397,21 @@ int pdot_rounding_host(int64_t m, int64_t n, const double* source, const double*
 int pdot_sqeuclid_cost_f64(int64_t m, int64_t n, int32_t dim, const double* source_points,
                            const double* target_points, int32_t normalise, double* cost, void* stream);
 
+/* ---- the coarse-to-fine warm start for point clouds -----------------------
+ * Device passes of pdot/multiscale.py (no counterpart in the reference, which
+ * always starts at zero, src/solver_gpu.jl:428-441). Points are FP32, row-major
+ * (one point per row, dim 1..3), in device memory; work is ordered on `stream`. */
+/* out[0] = max_ij ||x_i - y_j||^2 (FP64), the normaliser of the squared-Euclidean
+ * cost (`out` is device memory). */
+int pdot_points_max_sqdist(int64_t m, int64_t n, int32_t dim, const float* source_points,
+                           const float* target_points, double* out, void* stream);
+/* The semi-discrete c-transform out_i = min_J (scale * ||p_i - c_J||^2 - dual_J):
+ * duals known on num_centres points (FP64 centres, num_centres x dim, row-major)
+ * extended to every point p_i. */
+int pdot_points_c_transform(int64_t num_points, int64_t num_centres, int32_t dim, const float* points,
+                            const double* centres, const double* duals, double scale, double* out,
+                            void* stream);
+
 /* The same fused primal pass for callers that cannot allocate device memory
  * (a host framework that hands out its whole memory budget from its own pool,
  * or a latency-critical loop that cannot afford cudaMalloc's implicit device

@@ -253,6 +253,8 @@ SIGNATURES = {
     "pdot_rounding_f64": (ct.c_int, [_I64, _I64, _P, _P, _P, _P]),
     "pdot_rounding_host": (ct.c_int, [_I64, _I64, _P, _P, _P, _I32]),
     "pdot_sqeuclid_cost_f64": (ct.c_int, [_I64, _I64, _I32, _P, _P, _I32, _P, _P]),
+    "pdot_points_max_sqdist": (ct.c_int, [_I64, _I64, _I32, _P, _P, _P, _P]),
+    "pdot_points_c_transform": (ct.c_int, [_I64, _I64, _I32, _P, _P, _P, _D, _P, _P]),
     "pdot_primal_pass_workspace_bytes": (_I64, [_I64, _I64]),
     "pdot_primal_pass_f64_noalloc": (
         ct.c_int,

@@ -16,12 +16,9 @@ fine solve; `python -m pdot.multiscale` measures it against the cold start.
 """
 from __future__ import annotations
 
-import json
-import time
-
 import numpy as np
 
-from . import api, instances
+from . import _abi, api
 
 
 def bounding_square(xs: np.ndarray, ys: np.ndarray):
@@ -45,12 +42,26 @@ def cell_centres(lo, side: float, G: int) -> np.ndarray:
     return lo + (np.stack([gx.ravel(), gy.ravel()], axis=1) + 0.5) * (side / G)
 
 
-def max_sq_distance(xs: np.ndarray, ys: np.ndarray, chunk: int = 4096) -> float:
-    mx = 0.0
-    for k in range(0, xs.shape[0], chunk):
-        d = ((xs[k:k + chunk, None, :] - ys[None, :, :]) ** 2).sum(-1)
-        mx = max(mx, float(d.max()))
-    return mx
+def _device_points(p, device: int):
+    import torch
+
+    t = p if isinstance(p, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(p, dtype=np.float32))
+    return t.to(device=torch.device("cuda", device), dtype=torch.float32).contiguous()
+
+
+def max_sq_distance(xs, ys, *, device: int = 0) -> float:
+    """max_ij ||x_i - y_j||^2 over the two point sets, on the GPU
+    (pdot_points_max_sqdist; coordinates rounded to FP32 as the solver reads
+    them, distances in FP64)."""
+    import torch
+
+    lib = _abi.load()
+    x, y = _device_points(xs, device), _device_points(ys, device)
+    out = torch.zeros(1, dtype=torch.float64, device=x.device)
+    stream = torch.cuda.current_stream(x.device).cuda_stream
+    _abi.check(lib, lib.pdot_points_max_sqdist(x.shape[0], y.shape[0], x.shape[1], x.data_ptr(), y.data_ptr(),
+                                               out.data_ptr(), stream), "pdot_points_max_sqdist")
+    return float(out.item())
 
 
 def coarse_problem(xs, ys, a, b, G: int, scale: float):
@@ -66,14 +77,21 @@ def coarse_problem(xs, ys, a, b, G: int, scale: float):
     return np.asfortranarray(Cc), A[ia], B[ib], ca, cb
 
 
-def c_transform(points: np.ndarray, centres: np.ndarray, dual: np.ndarray, scale: float,
-                chunk: int = 4096) -> np.ndarray:
-    """min_J (scale * ||p - c_J||^2 - dual_J) for every point p."""
-    out = np.empty(points.shape[0])
-    for k in range(0, points.shape[0], chunk):
-        d = scale * ((points[k:k + chunk, None, :] - centres[None, :, :]) ** 2).sum(-1) - dual[None, :]
-        out[k:k + chunk] = d.min(axis=1)
-    return out
+def c_transform(points, centres: np.ndarray, dual: np.ndarray, scale: float, *, device: int = 0) -> np.ndarray:
+    """min_J (scale * ||p - c_J||^2 - dual_J) for every point p, on the GPU
+    (pdot_points_c_transform)."""
+    import torch
+
+    lib = _abi.load()
+    p = _device_points(points, device)
+    c = torch.from_numpy(np.ascontiguousarray(centres, dtype=np.float64)).to(p.device)
+    d = torch.from_numpy(np.ascontiguousarray(dual, dtype=np.float64)).to(p.device)
+    out = torch.empty(p.shape[0], dtype=torch.float64, device=p.device)
+    stream = torch.cuda.current_stream(p.device).cuda_stream
+    _abi.check(lib, lib.pdot_points_c_transform(p.shape[0], c.shape[0], p.shape[1], p.data_ptr(), c.data_ptr(),
+                                                d.data_ptr(), float(scale), out.data_ptr(), stream),
+               "pdot_points_c_transform")
+    return out.cpu().numpy()
 
 
 def learned_to_fine_duals(xs, ys, a, b, starter, *, scale: float | None = None, floor: float = 1e-6):
@@ -89,7 +107,8 @@ def learned_to_fine_duals(xs, ys, a, b, starter, *, scale: float | None = None, 
     from .learned import SIDE
 
     G = SIDE
-    s = scale if scale is not None else 1.0 / max_sq_distance(xs, ys)
+    xs, ys = np.asarray(xs, dtype=np.float64), np.asarray(ys, dtype=np.float64)
+    s = scale if scale is not None else 1.0 / max_sq_distance(xs, ys, device=starter.device)
     lo, side = bounding_square(xs, ys)
     A, _ = bin_masses(xs, a, lo, side, G)
     B, _ = bin_masses(ys, b, lo, side, G)
@@ -99,68 +118,26 @@ def learned_to_fine_duals(xs, ys, a, b, starter, *, scale: float | None = None, 
     kappa = s * (side / G) ** 2 * 2.0 * (G - 1) ** 2
     cent = cell_centres(lo, side, G)
     ia, ib = np.nonzero(A > 0)[0], np.nonzero(B > 0)[0]
-    u = c_transform(xs, cent[ib], kappa * V[0][ib], s)
-    v = c_transform(ys, cent[ia], kappa * U[0][ia], s)
+    u = c_transform(xs, cent[ib], kappa * V[0][ib], s, device=starter.device)
+    v = c_transform(ys, cent[ia], kappa * U[0][ia], s, device=starter.device)
     return u, v, {"cells": [int(ia.size), int(ib.size)]}
 
 
-def coarse_to_fine_duals(xs, ys, a, b, *, G: int = 32, tol: float = 1e-4, iteration_limit: int = 100_000,
+def coarse_to_fine_duals(xs, ys, a, b, *, G: int = 64, tol: float = 1e-4, iteration_limit: int = 200_000,
                          scale: float | None = None, device: int = 0):
-    """Warm-start duals (u, v) for the fine problem, and facts about the coarse solve."""
-    s = scale if scale is not None else 1.0 / max_sq_distance(xs, ys)
+    """Warm-start duals (u, v) for the fine problem, and facts about the coarse
+    solve. The binning and the coarse cost are host work on at most G^2 cells;
+    the normaliser, the coarse solve and the c-transforms run on the GPU."""
+    xs, ys = np.asarray(xs, dtype=np.float64), np.asarray(ys, dtype=np.float64)
+    s = scale if scale is not None else 1.0 / max_sq_distance(xs, ys, device=device)
     Cc, A, B, ca, cb = coarse_problem(xs, ys, a, b, G, s)
     from .solve import default_parameters
 
     params = default_parameters(tol, iteration_limit=iteration_limit)
     out = api.optimize(params, api.OptimalTransportProblem(Cc, A, B), device=device)
-    u = c_transform(xs, cb, out.dual_target_solution, s)
-    v = c_transform(ys, ca, out.dual_source_solution, s)
+    u = c_transform(xs, cb, out.dual_target_solution, s, device=device)
+    v = c_transform(ys, ca, out.dual_source_solution, s, device=device)
     info = {"cells": [int(A.size), int(B.size)], "coarse_iterations": out.iteration_count,
             "coarse_termination": out.termination_string,
             "coarse_seconds": out.iteration_stats[-1].cumulative_time_sec}
     return u, v, info
-
-
-def main(argv=None):
-    import argparse
-
-    from .solve import default_parameters
-
-    ap = argparse.ArgumentParser(prog="python -m pdot.multiscale")
-    ap.add_argument("--m", type=int, default=20000)
-    ap.add_argument("--n", type=int, default=15000)
-    ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--grids", type=int, nargs="+", default=[32, 64])
-    ap.add_argument("--eps", type=float, nargs="+", default=[1e-4, 3e-4, 1e-3])
-    ap.add_argument("--rounds", type=int, nargs="+", default=[30, 100])
-    ap.add_argument("--iteration-limit", type=int, default=40_000)
-    ap.add_argument("--out")
-    args = ap.parse_args(argv)
-    xs, ys, a, b = instances.gauss_mixture_instance(args.m, args.n, args.seed)
-    xs32, ys32 = xs.astype(np.float32), ys.astype(np.float32)
-    prob = api.OptimalTransportProblem(None, a, b)
-    params = default_parameters(1e-4, iteration_limit=args.iteration_limit)
-    kw = {"precision": "f32", "cost": "sqeuclid", "points": (xs32, ys32)}
-    cold = api.optimize(params, prob, **kw)
-    rows = [{"start": "cold", "iterations": cold.iteration_count,
-             "seconds": cold.iteration_stats[-1].cumulative_time_sec}]
-    print(json.dumps(rows[-1]), flush=True)
-    scale = 1.0 / max_sq_distance(xs32.astype(np.float64), ys32.astype(np.float64))
-    for G in args.grids:
-        t0 = time.perf_counter()
-        u, v, info = coarse_to_fine_duals(xs32.astype(np.float64), ys32.astype(np.float64), a, b, G=G, scale=scale)
-        prep = time.perf_counter() - t0
-        for eps in args.eps:
-            for rounds in args.rounds:
-                w = api.optimize(params, prob, warm_start=(u, v), recover_plan=(eps, rounds), **kw)
-                rows.append({"start": f"coarse-to-fine G={G}", "eps": eps, "rounds": rounds,
-                             "iterations": w.iteration_count, "termination": w.termination_string,
-                             "seconds": w.iteration_stats[-1].cumulative_time_sec, "prep_seconds": prep, **info})
-                print(json.dumps(rows[-1]), flush=True)
-    if args.out:
-        with open(args.out, "w") as f:
-            json.dump(rows, f, indent=1)
-
-
-if __name__ == "__main__":
-    main()

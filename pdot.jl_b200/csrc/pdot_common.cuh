@@ -51,8 +51,12 @@ struct Geometry {
   int32_t tma;         // 1: the fused pass stages its operands with bulk copies
   int32_t tma_smem;    // dynamic shared memory of the staged pass (bytes)
   int32_t fail_waits;  // test hook: the staged pass's consumer waits report a timeout at once
-  int32_t pad_;
+  // CTAs of the dual step covering the rows: row_blocks (a thread per row) or,
+  // when a panel's row partials lie in many CTA slots (small problems, kDualWarpSlots
+  // or more), ceil(m / kWarps) (a warp per row)
+  int32_t dual_row_blocks;
 };
+constexpr int kDualWarpSlots = 16;
 
 // Where the cost entries come from.
 struct CostSource {

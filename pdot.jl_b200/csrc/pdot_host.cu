@@ -427,7 +427,7 @@ class Solver {
       B_.c[k] = c_[k];
     }
     const pdot::Geometry& g = g_;
-    const size_t vb = (size_t)g.row_blocks + g.col_blocks;
+    const size_t db = (size_t)g.dual_row_blocks + g.col_blocks;
     double* w = work_;
     B_.rowpart = w;
     w += ((size_t)g.grid + g.panels) * pdot::kPanelRows;
@@ -436,7 +436,7 @@ class Solver {
     B_.sqpart = w;
     w += g.grid;
     B_.steppart = w;
-    w += vb * pdot::kStepSums;
+    w += db * pdot::kStepSums;
     B_.evpart = w;
     w += (size_t)g.grid * pdot::kEvalSums;
     B_.vecpart = w;

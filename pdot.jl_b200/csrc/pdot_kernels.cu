@@ -455,13 +455,30 @@ __global__ void __launch_bounds__(kVecThreads) k2_dual(Buffers B, Geometry g, So
   A.aw = A.first ? 1.0 : __ddiv_rn(S, __dadd_rn(S, tau));
   double vals[kStepSums] = {0.0, 0.0};
   const int bid = blockIdx.x;
-  if (bid < g.row_blocks) {
+  const int rb = g.dual_row_blocks;
+  if (bid < rb && rb == g.row_blocks) {
     const int64_t i = (int64_t)bid * kVecThreads + threadIdx.x;
     if (i < g.m)
       dual_entry(finish_row_sum(g, B.rowpart, i), B.a[i], B.r[buf] + i, B.u[buf] + i, B.r[buf ^ 1] + i,
                  B.u[buf ^ 1] + i, A, vals[0], vals[1]);
+  } else if (bid < rb) {
+    // a warp per row: lane l adds slots l, l + 32, ... in order, then a fixed
+    // shuffle tree; the row's many slots are read in parallel, not in a chain
+    const int64_t i = (int64_t)bid * kWarps + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i < g.m) {
+      const int64_t p = i / kPanelRows, t = i - p * kPanelRows;
+      const int64_t lo = cta_of_unit(g, p * g.n), hi = cta_of_unit(g, (p + 1) * g.n - 1);
+      const double* q = B.rowpart + row_slot(lo, p) * kPanelRows + t;
+      double sd = 0.0;
+      for (int64_t c = lane; c <= hi - lo; c += 32) sd += q[c * kPanelRows];
+      sd = warp_sum(sd);
+      if (lane == 0)
+        dual_entry(sd, B.a[i], B.r[buf] + i, B.u[buf] + i, B.r[buf ^ 1] + i, B.u[buf ^ 1] + i, A, vals[0],
+                   vals[1]);
+    }
   } else {
-    const int64_t j = (int64_t)(bid - g.row_blocks) * kVecThreads + threadIdx.x;
+    const int64_t j = (int64_t)(bid - rb) * kVecThreads + threadIdx.x;
     if (j < g.n)
       dual_entry(finish_col_sum(g, B.colpart, j), B.b[j], B.c[buf] + j, B.v[buf] + j, B.c[buf ^ 1] + j,
                  B.v[buf ^ 1] + j, A, vals[0], vals[1]);
@@ -470,8 +487,8 @@ __global__ void __launch_bounds__(kVecThreads) k2_dual(Buffers B, Geometry g, So
   if (!elect_last_cta(&st->ticket_step)) return;
   if (threadIdx.x < 32) {
     double rs[kStepSums], cs[kStepSums], xs[1];
-    warp_reduce_partials<kStepSums>(B.steppart, 0, g.row_blocks, 0u, rs);
-    warp_reduce_partials<kStepSums>(B.steppart, g.row_blocks, g.col_blocks, 0u, cs);
+    warp_reduce_partials<kStepSums>(B.steppart, 0, rb, 0u, rs);
+    warp_reduce_partials<kStepSums>(B.steppart, rb, g.col_blocks, 0u, cs);
     warp_reduce_partials<1>(B.sqpart, 0, g.grid, 0u, xs);
     if (threadIdx.x == 0) {
       // interaction = dot(dr, du) + dot(dc, dv); ||[du; dv]||^2
@@ -882,7 +899,6 @@ Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device, int plan_f3
   g.tma = (want && g.vec > 1 && !(cost_kind == PDOT_COST_BF16 && m % 8 != 0)) ? 1 : 0;
   g.tma_smem = 0;
   g.fail_waits = 0;
-  g.pad_ = 0;
   int occ = 1;
   if (g.tma) {
     PDOT_STAGED_VARIANT(g, k1_primal_staged, {
@@ -901,15 +917,19 @@ Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device, int plan_f3
   g.grid = (int32_t)grid;
   g.row_blocks = (int32_t)((m + kVecThreads - 1) / kVecThreads);
   g.col_blocks = (int32_t)((n + kVecThreads - 1) / kVecThreads);
+  // the most CTA slots one panel's row partials can lie in
+  const int64_t slots = (g.grid + g.panels - 1) / g.panels + 1;
+  g.dual_row_blocks = slots >= kDualWarpSlots ? (int32_t)((m + kWarps - 1) / kWarps) : g.row_blocks;
   return g;
 }
 
 size_t workspace_doubles(const Geometry& g) {
   const size_t vb = (size_t)g.row_blocks + g.col_blocks;
+  const size_t db = (size_t)g.dual_row_blocks + g.col_blocks;
   return ((size_t)g.grid + g.panels) * kPanelRows  // rowpart
          + (size_t)g.panels * g.n                   // colpart
          + (size_t)g.grid                           // sqpart
-         + vb * kStepSums                           // steppart
+         + db * kStepSums                           // steppart
          + (size_t)g.grid * kEvalSums               // evpart
          + vb * kVecSums;                           // vecpart
 }
@@ -930,7 +950,7 @@ cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s, i
 }
 
 cudaError_t launch_dual(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s) {
-  k2_dual<<<g.row_blocks + g.col_blocks, kVecThreads, 0, s>>>(B, g, cfg);
+  k2_dual<<<g.dual_row_blocks + g.col_blocks, kVecThreads, 0, s>>>(B, g, cfg);
   return cudaGetLastError();
 }
 

@@ -449,12 +449,12 @@ def run_c2(args, device, local):
     return res
 
 
-WARM_GRID, WARM_EPS, WARM_ROUNDS = 64, 3e-4, 100  # coarse-to-fine warm start of the 20000 x 15000 solve
+WARM_GRID, WARM_EPS, WARM_ROUNDS = 96, 3e-4, 100  # coarse-to-fine warm start of the 20000 x 15000 solve
 
 
 def run_warm_mixed(args, params, m, n, xs, ys, a_h, b_h, Ct, a, b, xs_d, ys_d, device, local, fp64_ttk):
     """The mixed-precision solve (FP32 plan, cost from FP32 coordinates) from
-    the coarse-to-fine warm start: points binned on a 64 x 64 grid, the binned
+    the coarse-to-fine warm start: points binned on a 96 x 96 grid, the binned
     problem solved, its duals extended to every point by the c-transform, a
     plan recovered from them by 100 balancing rounds (eps 3e-4), then PDHG to
     relative KKT 1e-4. One wall-clock region covers all of it, from the host
@@ -665,22 +665,27 @@ def run_ours(args, world, rank, local):
         eparams = pdot.default_parameters(TOL, iteration_limit=args.steps)
         # one untimed call first, as the warm-up steps of the primary region
         pdot.optimize(pdot.default_parameters(TOL, iteration_limit=max(args.warmup, 1)), prob, device=local, **ekw)
-        torch.cuda.synchronize()
-        barrier(world)
-        w0 = time.perf_counter()
-        out = pdot.optimize(eparams, prob, device=local, **ekw)
-        torch.cuda.synchronize()
-        w1 = time.perf_counter()
-        e_sec = max_over_ranks(w1 - w0, world, device)
+        # three timed calls, the median reported (each allocates, copies in, solves, copies out, frees)
+        calls = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            barrier(world)
+            w0 = time.perf_counter()
+            out = pdot.optimize(eparams, prob, device=local, **ekw)
+            torch.cuda.synchronize()
+            w1 = time.perf_counter()
+            calls.append(max_over_ranks(w1 - w0, world, device))
+        e_sec = statistics.median(calls)
         vec_bytes = 8 * (m + n)
         h2d = (8 * (m + n) * xs.shape[1] // 2 if cost == "sqeuclid" else 8 * N) + vec_bytes
         e2e = {"value": world * out.iteration_count / e_sec, "unit": UNIT,
                "h2d_bytes_per_step": h2d / max(out.iteration_count, 1),
                "d2h_bytes_per_step": (8 * N + vec_bytes) / max(out.iteration_count, 1),
                "iterations_per_call": out.iteration_count, "seconds_per_call": e_sec,
-               "note": "one pdot.optimize call after one untimed call: H2D of C, a, b from pinned memory, "
-                       "the solve, D2H of the returned plan and duals into fresh host arrays; bytes "
-                       "amortised per iteration"}
+               "seconds_of_the_three_calls": calls,
+               "note": "the median of three pdot.optimize calls after one untimed call: H2D of C, a, b "
+                       "from pinned memory, the solve, D2H of the returned plan and duals into fresh host "
+                       "arrays; bytes amortised per iteration"}
         del C_host
 
     mixed = None

@@ -138,21 +138,29 @@ __device__ __forceinline__ void sum_cta_slots(const double* part, const long lon
                                               long long hi, long long slot_off, unsigned maxmask,
                                               double (&out)[K]) {
   const int lane = threadIdx.x & 31;
+  // all K values of a slot at once (independent loads); each value's
+  // additions keep their order
+  double acc[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = 0.0;
+  for (long long c = lo + lane; c <= hi; c += 32) {
+    if (cta_begin[c] == cta_begin[c + 1]) continue;  // empty CTA
+    double v[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = __ldcg(part + (c + slot_off) * K + k);
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = ((maxmask >> k) & 1u) ? nanmax(acc[k], v[k]) : acc[k] + v[k];
+  }
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const bool mx = (maxmask >> k) & 1u;
-    double acc = 0.0;
-    for (long long c = lo + lane; c <= hi; c += 32) {
-      if (cta_begin[c] == cta_begin[c + 1]) continue;  // empty CTA
-      const double v = __ldcg(part + (c + slot_off) * K + k);
-      acc = mx ? nanmax(acc, v) : acc + v;
-    }
+    double a = acc[k];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      const double y = __shfl_xor_sync(0xffffffffu, acc, o);
-      acc = mx ? nanmax(acc, y) : acc + y;
+      const double y = __shfl_xor_sync(0xffffffffu, a, o);
+      a = mx ? nanmax(a, y) : a + y;
     }
-    out[k] = acc;
+    out[k] = a;
   }
 }
 

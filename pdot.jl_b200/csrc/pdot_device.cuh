@@ -78,24 +78,33 @@ __device__ __forceinline__ void block_reduce(double (&vals)[K], unsigned maxmask
 
 // One warp reduces `count` records of K partials in a fixed order; lane 0 holds
 // the result. Reads go through L2 (the partials were written by other CTAs).
+// Lane l visits records l, l + 32, ... and takes all K values of a record at
+// once, so the loads of a record are independent; each value's additions keep
+// their order (record by record, then the shuffle tree).
 template <int K>
 __device__ __forceinline__ void warp_reduce_partials(const double* part, int64_t first, int64_t count,
                                                      unsigned maxmask, double (&out)[K]) {
   const int lane = threadIdx.x & 31;
+  double acc[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = 0.0;
+  for (int64_t c = lane; c < count; c += 32) {
+    double v[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = __ldcg(part + (first + c) * K + k);
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = ((maxmask >> k) & 1u) ? nanmax(acc[k], v[k]) : acc[k] + v[k];
+  }
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const bool mx = (maxmask >> k) & 1u;
-    double acc = 0.0;
-    for (int64_t c = lane; c < count; c += 32) {
-      const double v = __ldcg(part + (first + c) * K + k);
-      acc = mx ? nanmax(acc, v) : acc + v;
-    }
+    double a = acc[k];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      double y = __shfl_xor_sync(0xffffffffu, acc, o);
-      acc = mx ? nanmax(acc, y) : acc + y;
+      double y = __shfl_xor_sync(0xffffffffu, a, o);
+      a = mx ? nanmax(a, y) : a + y;
     }
-    out[k] = acc;
+    out[k] = a;
   }
 }
 

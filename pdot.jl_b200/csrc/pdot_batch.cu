@@ -488,6 +488,12 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
       cost.panel(row0, lane, I.m, ok);
       const long long jb = (ql0 > p * I.n ? ql0 : p * I.n) - p * I.n;
       const long long je = (ql1 < (p + 1) * I.n ? ql1 : (p + 1) * I.n) - p * I.n;
+      // the column's dual and coordinates are loaded one unit ahead
+      double vnext = 0.0;
+      if (jb + warp < je) {
+        if (!zero_g) vnext = __ldg(v + jb + warp);
+        cost.prefetch(jb + warp);
+      }
       for (long long j = jb + warp; !failed && j < je; j += kWarps) {
         const int stage = cstage;
         const uint32_t parity = cphase;
@@ -500,8 +506,12 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
         const float* sC = reinterpret_cast<const float*>(stg);
         const float* sX = reinterpret_cast<const float*>(stg + L::kCBytes);
         const float* sXa = reinterpret_cast<const float*>(stg + L::kCBytes + L::kXBytes);
-        const float vj = zero_g ? 0.0f : (float)__ldg(v + j);
-        cost.column(j);
+        const float vj = (float)vnext;
+        cost.take();
+        if (j + kWarps < je) {
+          if (!zero_g) vnext = __ldg(v + j + kWarps);
+          cost.prefetch(j + kWarps);
+        }
         const long long col = j * I.ld + row0 + lane * kBR;
         double cs = 0.0;
 #pragma unroll

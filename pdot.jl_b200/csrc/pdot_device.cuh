@@ -256,6 +256,7 @@ struct CostReader {
   float scale;
   float xr[RPL][R][DIM];
   float yr[DIM];
+  float yn[DIM];  // the next column's coordinates, loaded one unit ahead
   __device__ __forceinline__ CostReader(const CostSource& s, float scl) : xs(s.xs), ys(s.ys), scale(scl) {}
   __device__ __forceinline__ void panel(int64_t row0, int lane, int64_t m, const bool (&ok)[RPL]) {
 #pragma unroll
@@ -270,6 +271,17 @@ struct CostReader {
   __device__ __forceinline__ void column(int64_t j) {
 #pragma unroll
     for (int d = 0; d < DIM; ++d) yr[d] = __ldg(ys + j * DIM + d);
+  }
+  // prefetch(j) starts the loads of column j's coordinates; take() makes them
+  // the current column. A staged pass prefetches its next unit's column while
+  // it computes the current one, so the loads' latency is off the unit's path.
+  __device__ __forceinline__ void prefetch(int64_t j) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) yn[d] = __ldg(ys + j * DIM + d);
+  }
+  __device__ __forceinline__ void take() {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) yr[d] = yn[d];
   }
   __device__ __forceinline__ void get(int64_t, int k, float (&c)[R]) const {
 #pragma unroll
@@ -292,6 +304,8 @@ struct StoredCost {
   __device__ __forceinline__ StoredCost(const CostSource& s, float) : C(static_cast<const T*>(s.C)) {}
   __device__ __forceinline__ void panel(int64_t, int, int64_t, const bool (&)[RPL]) {}
   __device__ __forceinline__ void column(int64_t) {}
+  __device__ __forceinline__ void prefetch(int64_t) {}
+  __device__ __forceinline__ void take() {}
   __device__ __forceinline__ void get(int64_t idx, int, T (&c)[R]) const { vldg<T, R>(C + idx, c); }
 };
 template <int R, int RPL>

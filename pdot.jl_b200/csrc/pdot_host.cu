@@ -586,7 +586,7 @@ class Solver {
     Prefault(double* p, size_t count) {
       if (!p || count < (size_t(1) << 22) || pdot::host_is_pinned(p)) return;  // small plans: not worth a thread
       const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-      const size_t parts = std::min<size_t>(16, hw);
+      const size_t parts = std::min<size_t>(8, std::max<size_t>(1, hw / 2));
       const size_t per = (count + parts - 1) / parts;
       for (size_t k = 0; k < parts; ++k) {
         const size_t lo = k * per, hi = std::min(count, lo + per);

@@ -30,7 +30,7 @@ void* g_stage[2] = {nullptr, nullptr};
 
 int copy_workers() {
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  return (int)std::min(16u, hw);
+  return (int)std::min(8u, std::max(1u, hw / 2));
 }
 
 // memcpy of `bytes` split over `workers` threads (the caller is one of them),

@@ -324,28 +324,9 @@ def stats_from_c(s: _abi.IterationStatsC) -> IterationStats:
     )
 
 
-def host_plan(m: int, n: int) -> np.ndarray:
-    """A zeroed m x n FP64 column-major array for a returned plan. Large ones
-    are anonymous mappings advised for transparent huge pages: the solver's
-    copy back writes every page of a fresh array, and first-touch faults on
-    2 MiB pages are 512 times fewer than on 4 KiB ones (the advice is a hint;
-    where the kernel does not take it, the array is an ordinary one)."""
-    nbytes = m * n * 8
-    if nbytes < (1 << 26):
-        return np.zeros((m, n), dtype=np.float64, order="F")
-    import mmap
-
-    mm = mmap.mmap(-1, nbytes)
-    try:
-        mm.madvise(mmap.MADV_HUGEPAGE)
-    except (AttributeError, OSError, ValueError):
-        pass
-    return np.frombuffer(mm, dtype=np.float64).reshape((m, n), order="F")
-
-
 class OutputBuffers:
     def __init__(self, m: int, n: int, stats_capacity: int):
-        self.X = host_plan(m, n)
+        self.X = np.zeros((m, n), dtype=np.float64, order="F")
         self.u = np.zeros(m, dtype=np.float64)
         self.v = np.zeros(n, dtype=np.float64)
         self.stats = (_abi.IterationStatsC * max(stats_capacity, 1))()

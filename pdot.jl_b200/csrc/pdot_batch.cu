@@ -645,16 +645,31 @@ __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConf
   }
   block_reduce<kStepSums>(vals, 0u, B.steppart + blk * kStepSums);
   if (!elect_last_of(&st->ticket_step, (unsigned)(I.rblocks + I.cblocks))) return;
-  if (threadIdx.x < 32) {
-    double rs[kStepSums], cs[kStepSums], xs[1];
+  // warps 0-2 reduce the three partial sets side by side, warp 3 computes the
+  // step rule's powers; thread 0 then runs the step control
+  __shared__ double fin[2 * kStepSums + 1];
+  __shared__ StepPowers pw;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w == 0) {
+    double rs[kStepSums];
     warp_reduce_partials<kStepSums>(B.steppart, B.vblock_prefix[kk], I.rblocks, 0u, rs);
+    if (lane == 0) fin[0] = rs[0], fin[1] = rs[1];
+  } else if (w == 1) {
+    double cs[kStepSums];
     warp_reduce_partials<kStepSums>(B.steppart, B.vblock_prefix[kk] + I.rblocks, I.cblocks, 0u, cs);
+    if (lane == 0) fin[2] = cs[0], fin[3] = cs[1];
+  } else if (w == 2) {
+    double xs[1];
     const long long lo = bcta_of_unit(B.cta_begin, grid, ubase), hi = bcta_of_unit(B.cta_begin, grid, B.unit_prefix[kk + 1] - 1);
     sum_cta_slots<1>(B.sqpart, B.cta_begin, lo, hi, kk, 0u, xs);
-    if (threadIdx.x == 0) {
-      step_control(st, cfg, rs[0], cs[0], xs[0], rs[1] + cs[1]);
-      st->ticket_step = 0;
-    }
+    if (lane == 0) fin[4] = xs[0];
+  } else if (w == 3 && lane == 0) {
+    pw = step_powers(st, cfg);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    step_control(st, cfg, fin[0], fin[2], fin[4], fin[1] + fin[3], pw);
+    st->ticket_step = 0;
   }
 }
 
@@ -806,22 +821,39 @@ __global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, Solve
   }
   block_reduce<kVecSums>(acc, kVecMaxMask, B.vecpart + blk * kVecSums);
   if (!elect_last_of(&st->ticket_eval, (unsigned)(I.rblocks + I.cblocks))) return;
-  if (threadIdx.x < 32) {
+  // warps 0-2 reduce the three partial sets side by side
+  __shared__ double fin[kEvalSums + 2 * kVecSums];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w == 0) {
     const long long lo = bcta_of_unit(B.cta_begin, grid, B.unit_prefix[kk]);
     const long long hi = bcta_of_unit(B.cta_begin, grid, B.unit_prefix[kk + 1] - 1);
-    double E[kEvalSums], R[kVecSums], Cc[kVecSums];
+    double E[kEvalSums];
     sum_cta_slots<kEvalSums>(B.evpart, B.cta_begin, lo, hi, kk, kEvalMaxMask, E);
+    if (lane == 0)
+      for (int q = 0; q < kEvalSums; ++q) fin[q] = E[q];
+  } else if (w == 1) {
+    double R[kVecSums];
     warp_reduce_partials<kVecSums>(B.vecpart, B.vblock_prefix[kk], I.rblocks, kVecMaxMask, R);
+    if (lane == 0)
+      for (int q = 0; q < kVecSums; ++q) fin[kEvalSums + q] = R[q];
+  } else if (w == 2) {
+    double Cc[kVecSums];
     warp_reduce_partials<kVecSums>(B.vecpart, B.vblock_prefix[kk] + I.rblocks, I.cblocks, kVecMaxMask, Cc);
-    if (threadIdx.x == 0) {
-      const PointSums cur = point_sums(E, R, Cc, 0);
-      const PointSums avg = point_sums(E, R, Cc, E_AVG);
-      if (!start_only)
-        eval_control(st, cfg, cur, avg, B.rec + k, 1);
-      else if (B.warm[k])
-        record_start_point(st, cur);
-      st->ticket_eval = 0;
-    }
+    if (lane == 0)
+      for (int q = 0; q < kVecSums; ++q) fin[kEvalSums + kVecSums + q] = Cc[q];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double* E = fin;
+    const double* R = fin + kEvalSums;
+    const double* Cc = fin + kEvalSums + kVecSums;
+    const PointSums cur = point_sums(E, R, Cc, 0);
+    const PointSums avg = point_sums(E, R, Cc, E_AVG);
+    if (!start_only)
+      eval_control(st, cfg, cur, avg, B.rec + k, 1);
+    else if (B.warm[k])
+      record_start_point(st, cur);
+    st->ticket_eval = 0;
   }
 }
 

@@ -436,8 +436,22 @@ struct UnitCursor {
 // (the kernels use solver_state.step_size, not the shrunk local step), so the
 // candidate computed once is the accepted one; a rejection only adds an
 // attempt to the counters and one more application of the shrink rule.
+// First-attempt powers of the step-size rule, computed by a spare warp while
+// the finishing CTA's other warps reduce the partial sums: (k + 1)^e for the
+// iteration count k that the first attempt sees.
+struct StepPowers {
+  double k1 = -1.0, reduction = 0.0, growth = 0.0;
+};
+__device__ __forceinline__ StepPowers step_powers(const DevState* st, const SolveConfig& cfg) {
+  StepPowers p;
+  p.k1 = (double)(st->total_iters + 2);
+  p.reduction = powd(p.k1, cfg.reduction_exponent);
+  p.growth = powd(p.k1, cfg.growth_exponent);
+  return p;
+}
+
 __device__ void step_control(DevState* st, const SolveConfig& cfg, double dot_r, double dot_c, double dx2,
-                             double dy2) {
+                             double dy2, const StepPowers& pre = StepPowers()) {
   const double omega = st->primal_weight;
   const double weight = st->step_size;
   const bool fresh = !(st->sum_weights > 0.0);
@@ -464,8 +478,11 @@ __device__ void step_control(DevState* st, const SolveConfig& cfg, double dot_r,
       }
       if (tau <= limit) accepted = true;
       const double k1 = (double)(st->total_iters + 1);
-      const double first_term = __dmul_rn(__dsub_rn(1.0, __ddiv_rn(1.0, powd(k1, cfg.reduction_exponent))), limit);
-      const double second_term = __dmul_rn(__dadd_rn(1.0, __ddiv_rn(1.0, powd(k1, cfg.growth_exponent))), tau);
+      const bool have = k1 == pre.k1;
+      const double pr = have ? pre.reduction : powd(k1, cfg.reduction_exponent);
+      const double pg = have ? pre.growth : powd(k1, cfg.growth_exponent);
+      const double first_term = __dmul_rn(__dsub_rn(1.0, __ddiv_rn(1.0, pr)), limit);
+      const double second_term = __dmul_rn(__dadd_rn(1.0, __ddiv_rn(1.0, pg)), tau);
       tau = jl_min(first_term, second_term);
       if (accepted) break;
       // the reference loops forever on a NaN limit; stop with a numerical error

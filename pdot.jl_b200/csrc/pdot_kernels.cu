@@ -495,16 +495,31 @@ __global__ void __launch_bounds__(kVecThreads) k2_dual(Buffers B, Geometry g, So
   }
   block_reduce<kStepSums>(vals, 0u, B.steppart + (int64_t)bid * kStepSums);
   if (!elect_last_cta(&st->ticket_step)) return;
-  if (threadIdx.x < 32) {
-    double rs[kStepSums], cs[kStepSums], xs[1];
+  // warps 0-2 reduce the three partial sets side by side, warp 3 computes the
+  // step rule's powers; thread 0 then runs the step control
+  __shared__ double fin[2 * kStepSums + 1];
+  __shared__ StepPowers pw;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w == 0) {
+    double rs[kStepSums];
     warp_reduce_partials<kStepSums>(B.steppart, 0, rb, 0u, rs);
+    if (lane == 0) fin[0] = rs[0], fin[1] = rs[1];
+  } else if (w == 1) {
+    double cs[kStepSums];
     warp_reduce_partials<kStepSums>(B.steppart, rb, g.col_blocks, 0u, cs);
+    if (lane == 0) fin[2] = cs[0], fin[3] = cs[1];
+  } else if (w == 2) {
+    double xs[1];
     warp_reduce_partials<1>(B.sqpart, 0, g.grid, 0u, xs);
-    if (threadIdx.x == 0) {
-      // interaction = dot(dr, du) + dot(dc, dv); ||[du; dv]||^2
-      step_control(st, cfg, rs[0], cs[0], xs[0], rs[1] + cs[1]);
-      st->ticket_step = 0;
-    }
+    if (lane == 0) fin[4] = xs[0];
+  } else if (w == 3 && lane == 0) {
+    pw = step_powers(st, cfg);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // interaction = dot(dr, du) + dot(dc, dv); ||[du; dv]||^2
+    step_control(st, cfg, fin[0], fin[2], fin[4], fin[1] + fin[3], pw);
+    st->ticket_step = 0;
   }
 }
 
@@ -666,20 +681,37 @@ __global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, So
   }
   block_reduce<kVecSums>(acc, kVecMaxMask, B.vecpart + (int64_t)bid * kVecSums);
   if (!elect_last_cta(&st->ticket_eval)) return;
-  if (threadIdx.x < 32) {
-    double E[kEvalSums], R[kVecSums], Cc[kVecSums];
+  // warps 0-2 reduce the three partial sets side by side
+  __shared__ double fin[kEvalSums + 2 * kVecSums];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w == 0) {
+    double E[kEvalSums];
     warp_reduce_partials<kEvalSums>(B.evpart, 0, g.grid, kEvalMaxMask, E);
+    if (lane == 0)
+      for (int k = 0; k < kEvalSums; ++k) fin[k] = E[k];
+  } else if (w == 1) {
+    double R[kVecSums];
     warp_reduce_partials<kVecSums>(B.vecpart, 0, g.row_blocks, kVecMaxMask, R);
+    if (lane == 0)
+      for (int k = 0; k < kVecSums; ++k) fin[kEvalSums + k] = R[k];
+  } else if (w == 2) {
+    double Cc[kVecSums];
     warp_reduce_partials<kVecSums>(B.vecpart, g.row_blocks, g.col_blocks, kVecMaxMask, Cc);
-    if (threadIdx.x == 0) {
-      const PointSums cur = point_sums(E, R, Cc, 0);
-      const PointSums avg = point_sums(E, R, Cc, E_AVG);
-      if (start_only)
-        record_start_point(st, cur);
-      else
-        eval_control(st, cfg, cur, avg, B.ring, B.ring_cap);
-      st->ticket_eval = 0;
-    }
+    if (lane == 0)
+      for (int k = 0; k < kVecSums; ++k) fin[kEvalSums + kVecSums + k] = Cc[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double* E = fin;
+    const double* R = fin + kEvalSums;
+    const double* Cc = fin + kEvalSums + kVecSums;
+    const PointSums cur = point_sums(E, R, Cc, 0);
+    const PointSums avg = point_sums(E, R, Cc, E_AVG);
+    if (start_only)
+      record_start_point(st, cur);
+    else
+      eval_control(st, cfg, cur, avg, B.ring, B.ring_cap);
+    st->ticket_eval = 0;
   }
 }
 

@@ -180,6 +180,12 @@ typedef struct pdot_solver_options {
    * unit costing its rows plus batch_unit_cost * 256 (the per-unit overhead,
    * 0..8, in eighths). 0 balances the rows alone. */
   double batch_unit_cost;
+  /* Regular chunks of loop bodies (the evaluation and the steps up to the next
+   * one) as one persistent cooperative launch with grid barriers between the
+   * phases, instead of a CUDA graph of separate launches; the results are
+   * bit-identical. 0: automatic (small problems, when CUDA graphs are on),
+   * 1: whenever the direct 16-byte pass runs, -1: never. */
+  int32_t persistent_chunks;
 } pdot_solver_options;
 
 /* ---- output -------------------------------------------------------------- */

@@ -122,15 +122,6 @@ __device__ __forceinline__ int find_segment(const long long* prefix, int count, 
   return lo;
 }
 
-__device__ __forceinline__ bool elect_last_of(unsigned int* ticket, unsigned int count) {
-  __shared__ bool last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = (atomicAdd(ticket, 1u) == count - 1);
-  __syncthreads();
-  if (last) __threadfence();
-  return last;
-}
 
 // Fixed-order sum of the non-empty CTA slots [lo, hi] (+ offset) of K values.
 template <int K>

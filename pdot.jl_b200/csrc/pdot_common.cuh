@@ -55,6 +55,9 @@ struct Geometry {
   // when a panel's row partials lie in many CTA slots (small problems, kDualWarpSlots
   // or more), ceil(m / kWarps) (a warp per row)
   int32_t dual_row_blocks;
+  // CTAs of the persistent chunk kernel (all co-resident; each runs the CTA
+  // ranges grid / chunk_ctas of the matrix passes in turn), 0: not available
+  int32_t chunk_ctas;
 };
 constexpr int kDualWarpSlots = 16;
 
@@ -136,6 +139,8 @@ struct DevState {
   unsigned int ticket_step;  // last-CTA tickets
   unsigned int ticket_eval;
   unsigned int ticket_init;
+  unsigned int bar_count;    // grid barrier of the persistent chunk kernel: arrivals
+  unsigned int bar_gen;      // and generation
   int pad_[1];
 };
 
@@ -201,6 +206,10 @@ cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s, i
 cudaError_t launch_dual(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s);
 cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s,
                         int xsums = 0);
+// One regular chunk (evaluation, then `steps` steps, the last with xsums) as
+// one persistent cooperative launch (needs g.chunk_ctas > 0); bit-identical to
+// launch_eval followed by the steps.
+cudaError_t launch_chunk(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s, int steps);
 // start_only = 1: a warm start's initial point becomes the last restart
 // point; nothing else of the evaluation block runs.
 cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s,

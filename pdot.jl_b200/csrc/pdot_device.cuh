@@ -126,15 +126,27 @@ __device__ __forceinline__ double sum_strided(const double* q, int64_t count, in
   return s;
 }
 
-// Last-CTA election for a grid-wide finish step.
-__device__ __forceinline__ bool elect_last_cta(unsigned int* ticket) {
+// Last-of-`count` election for a finish step: every CTA (or virtual block of
+// a persistent launch) takes a ticket once; the one that takes the last sees
+// the others' writes.
+__device__ __forceinline__ bool elect_last_of(unsigned int* ticket, unsigned int count) {
   __shared__ bool last;
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  if (threadIdx.x == 0) last = (atomicAdd(ticket, 1u) == count - 1);
   __syncthreads();
   if (last) __threadfence();
   return last;
+}
+__device__ __forceinline__ bool elect_last_cta(unsigned int* ticket) { return elect_last_of(ticket, gridDim.x); }
+
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned int* p, unsigned int v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 // ---- vector loads and stores of R consecutive rows (R*sizeof(T) bytes) -------
@@ -201,6 +213,37 @@ __device__ __forceinline__ void vldg(const T* p, T (&v)[R]) {
   } else {
     using W = typename VecWord<sizeof(T) * R>::type;
     const W w = __ldg(reinterpret_cast<const W*>(p));
+    memcpy(v, &w, sizeof(W));
+  }
+}
+// The same through L2 only (ld.global.cg): for data that other CTAs of the
+// same launch wrote (the persistent chunk kernel), where the read-only path
+// of vldg is not coherent.
+template <typename T, int R>
+__device__ __forceinline__ void vldcg(const T* p, T (&v)[R]) {
+  if constexpr (R == 1) {
+    if constexpr (sizeof(T) == 2) {
+      const unsigned short w = __ldcg(reinterpret_cast<const unsigned short*>(p));
+      memcpy(v, &w, 2);
+    } else {
+      v[0] = __ldcg(p);
+    }
+  } else if constexpr (sizeof(T) == 8) {
+#pragma unroll
+    for (int h = 0; h < R / 2; ++h) {
+      const double2 t = __ldcg(reinterpret_cast<const double2*>(p) + h);
+      v[2 * h] = t.x;
+      v[2 * h + 1] = t.y;
+    }
+  } else if constexpr (sizeof(T) == 4 && R == 4) {
+    const float4 t = __ldcg(reinterpret_cast<const float4*>(p));
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+  } else {
+    using W = typename VecWord<sizeof(T) * R>::type;
+    const W w = __ldcg(reinterpret_cast<const W*>(p));
     memcpy(v, &w, sizeof(W));
   }
 }
@@ -395,6 +438,41 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity,
   for (int it = 0; it < polls; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
+}
+
+// Grid-wide barrier of a persistent launch whose CTAs are all co-resident (a
+// cooperative launch). Thread 0 of each CTA reads the generation, publishes
+// its CTA's writes (fence) and arrives; the last arrival resets the count and
+// releases the next generation, the others poll it with acquire loads, at most
+// `polls` times, and stop early once `abort_flag` is non-zero (another CTA's
+// poll ran out). Returns false to every thread of the CTA when its poll ran
+// out or was aborted (the caller records the error and leaves), so after one
+// timeout every CTA leaves within one more barrier.
+__device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int* gen, unsigned int ctas,
+                                             const int* abort_flag, int polls = kSpinLimit) {
+  __shared__ int bar_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned int g0 = ld_acquire_gpu(gen);
+    __threadfence();
+    if (atomicAdd(count, 1u) == ctas - 1) {
+      atomicExch(count, 0u);
+      st_release_gpu(gen, g0 + 1u);
+    } else {
+      int it = 0;
+      while (ld_acquire_gpu(gen) == g0) {
+        if (++it >= polls || ld_acquire_gpu(reinterpret_cast<const unsigned int*>(abort_flag)) != 0u) {
+          ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+    bar_ok = ok;
+  }
+  __syncthreads();
+  return bar_ok != 0;
 }
 
 // The units of warp w inside [q0, q1): column w, w+8, ... of each panel segment.

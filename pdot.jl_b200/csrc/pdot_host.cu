@@ -135,6 +135,7 @@ struct Variant {
   int fail_waits = 0;  // test hook: the staged pass's waits report timeouts
   double warm_omega = 0.0;  // > 0: initial primal weight of a warm start
   bool warm_zero = false;   // a warm start's restart information starts at the zero point
+  int persistent = 0;       // persistent chunk kernel: 0 automatic, 1 on, -1 off
 };
 
 Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
@@ -196,6 +197,9 @@ Variant read_options(const pdot_problem& P, const pdot_solver_options* o) {
   if (o->warm_restart_at_zero != 0 && o->warm_restart_at_zero != 1)
     fail(PDOT_ERR_INVALID_ARGUMENT, "warm_restart_at_zero must be 0 or 1");
   v.warm_zero = o->warm_restart_at_zero == 1;
+  if (o->persistent_chunks < -1 || o->persistent_chunks > 1)
+    fail(PDOT_ERR_INVALID_ARGUMENT, "persistent_chunks must be -1, 0 or 1");
+  v.persistent = o->persistent_chunks;
   return v;
 }
 
@@ -248,6 +252,9 @@ int64_t pass_workspace_bytes(const pdot::Geometry& g) {
 
 constexpr int kRingCap = 4096;
 constexpr int kInFlight = 2;
+// Automatic persistent chunks up to this many plan entries: below it the
+// launches and the dual step's latency, not the bytes, set an iteration's time.
+constexpr int64_t kChunkAutoEntries = int64_t(1) << 24;
 
 enum TimedKind { kTimedPrimal = 0, kTimedDual = 1, kTimedEval = 2 };
 
@@ -463,7 +470,10 @@ class Solver {
     warm_zero_ = var.warm_zero;
     freq_ = prm.termination_evaluation_frequency;
     limit_ = prm.termination_criteria.iteration_limit;
-    if (use_graph_ && !time_kernels_) capture_regular_chunk();
+    const bool small = (int64_t)g_.m * g_.n <= kChunkAutoEntries;
+    persistent_ = g_.chunk_ctas > 0 && !time_kernels_ &&
+                  (var.persistent == 1 || (var.persistent == 0 && use_graph_ && small));
+    if (use_graph_ && !time_kernels_ && !persistent_) capture_regular_chunk();
     reset();
   }
 
@@ -554,7 +564,8 @@ class Solver {
       drain();
       if (status_.kernel_error) {
         sync_all(issued, completed);
-        fail(PDOT_ERR_CUDA, "a bounded wait in the fused primal pass timed out (kernel_error %d)",
+        fail(PDOT_ERR_CUDA,
+             "a bounded wait timed out (staged primal pass or persistent chunk barrier; kernel_error %d)",
              status_.kernel_error);
       }
       if (status_.done) break;
@@ -685,10 +696,11 @@ class Solver {
 
   bool is_eval(long long it) const { return (it - 1) % freq_ == 0 || it == limit_ + 1 || it <= 10; }
 
-  // A chunk starting here may be the captured graph: evaluation at its first
-  // iteration only, and no forced evaluation (iteration_limit + 1) inside.
+  // A chunk starting here may be the captured graph or the persistent chunk
+  // kernel: evaluation at its first iteration only, and no forced evaluation
+  // (iteration_limit + 1) inside.
   bool regular_start(long long it) const {
-    if (!graph_exec_ || it <= 10 || (it - 1) % freq_ != 0) return false;
+    if (!(graph_exec_ || persistent_) || it <= 10 || (it - 1) % freq_ != 0) return false;
     for (long long k = it + 1; k < it + freq_; ++k)
       if (is_eval(k)) return false;
     return true;
@@ -730,7 +742,10 @@ class Solver {
   // Enqueues up to `budget` loop bodies starting at host_it_; returns how many.
   int64_t enqueue_chunk(int64_t budget, int slot) {
     if (regular_start(host_it_) && budget >= freq_) {
-      CK(cudaGraphLaunch(graph_exec_, stream_));
+      if (persistent_)
+        CK(pdot::launch_chunk(B_, g_, cfg_, stream_, (int)freq_));
+      else
+        CK(cudaGraphLaunch(graph_exec_, stream_));
       host_it_ += freq_;
       return freq_;
     }
@@ -801,6 +816,7 @@ class Solver {
 
   int device_ = 0;
   bool use_graph_ = true, time_kernels_ = false;
+  bool persistent_ = false;  // regular chunks run as one persistent launch
   pdot_pdhg_parameters params_;
   pdot::Geometry g_{};
   pdot::SolveConfig cfg_{};

@@ -77,13 +77,13 @@ __device__ __forceinline__ void primal_pass_body(const CostSource& csrc, float s
                                                  const double nw, const double aw, const bool zero_g,
                                                  const bool first, double* __restrict__ colpart,
                                                  double* __restrict__ rowpart, double* __restrict__ sqpart,
-                                                 const Geometry g, double* __restrict__ evpart = nullptr) {
+                                                 const Geometry g, const int64_t cta,
+                                                 double* __restrict__ evpart = nullptr) {
   constexpr int RPL = kPanelRows / (32 * R);
   __shared__ double red[kWarps][kPanelRows];
   __shared__ double sqw[kWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t m = g.m, n = g.n;
-  const int64_t cta = blockIdx.x;
   const int64_t q0 = unit_begin(g, cta), q1 = unit_begin(g, cta + 1);
   CostReader<CK, R, RPL> cost(csrc, scale);
   double sq = 0.0;
@@ -102,12 +102,12 @@ __device__ __forceinline__ void primal_pass_body(const CostSource& csrc, float s
 #pragma unroll
       for (int e = 0; e < R; ++e) {
         acc[k][e] = 0.0;
-        ur[k][e] = (ok[k] && !zero_g) ? __ldg(u + i + e) : 0.0;
+        ur[k][e] = (ok[k] && !zero_g) ? __ldcg(u + i + e) : 0.0;
       }
     }
     cost.panel(row0, lane, m, ok);
     for (int64_t j = jb + warp; j < je; j += kWarps) {
-      const double vj = zero_g ? 0.0 : __ldg(v + j);
+      const double vj = zero_g ? 0.0 : __ldcg(v + j);
       cost.column(j);
       const int64_t base = j * m + row0 + lane * R;
       typename CostReader<CK, R, RPL>::value_t cv[RPL][R];
@@ -168,8 +168,10 @@ __device__ __forceinline__ void primal_pass_body(const CostSource& csrc, float s
   if constexpr (XS) xsums_store(xa, evpart + cta * kEvalSums);
 }
 
+// The duals are read through L2 (__ldcg): in the persistent chunk kernel the
+// dual step of the same launch wrote them.
 template <typename TX, int CK, int R, bool XS>
-__device__ __forceinline__ void k1_primal_impl(const Buffers& B, const Geometry& g) {
+__device__ __forceinline__ void k1_primal_impl(const Buffers& B, const Geometry& g, const int64_t cta) {
   DevState* st = B.st;
   if (st->done | st->numerical_error) return;
   const int buf = st->buf;
@@ -183,18 +185,18 @@ __device__ __forceinline__ void k1_primal_impl(const Buffers& B, const Geometry&
   const double aw = first ? 1.0 : __ddiv_rn(S, __dadd_rn(S, tau));
   primal_pass_body<TX, CK, R, XS>(B.cost, (float)st->cost_scale, static_cast<TX*>(B.X[buf]),
                                   static_cast<TX*>(B.X[buf ^ 1]), B.u[buf], B.v[buf], s, nw, aw, zero_g, first,
-                                  B.colpart, B.rowpart, B.sqpart, g, B.evpart);
-  if (XS && blockIdx.x == 0 && threadIdx.x == 0) st->xsums_iter = st->iteration;
+                                  B.colpart, B.rowpart, B.sqpart, g, cta, B.evpart);
+  if (XS && cta == 0 && threadIdx.x == 0) st->xsums_iter = st->iteration;
 }
 
 template <typename TX, int CK, int R>
 __global__ void __launch_bounds__(kThreads, 2) k1_primal(Buffers B, Geometry g) {
-  k1_primal_impl<TX, CK, R, false>(B, g);
+  k1_primal_impl<TX, CK, R, false>(B, g, blockIdx.x);
 }
 // the same pass before an evaluation: it also leaves the evaluation's plan sums
 template <typename TX, int CK, int R>
 __global__ void __launch_bounds__(kThreads, 2) k1_primal_xs(Buffers B, Geometry g) {
-  k1_primal_impl<TX, CK, R, true>(B, g);
+  k1_primal_impl<TX, CK, R, true>(B, g, blockIdx.x);
 }
 
 template <int R>
@@ -208,7 +210,8 @@ __global__ void __launch_bounds__(kThreads, 2)
   cs.dim = 0;
   primal_pass_body<double, PDOT_COST_F64, R>(cs, 1.0f, X, Xa, u, v, s, nw, aw,
                                              (flags & PDOT_PASS_ZERO_GRADIENT) != 0,
-                                             (flags & PDOT_PASS_FIRST_AVERAGE) != 0, colpart, rowpart, sqpart, g);
+                                             (flags & PDOT_PASS_FIRST_AVERAGE) != 0, colpart, rowpart, sqpart, g,
+                                             blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -453,7 +456,10 @@ __global__ void __launch_bounds__(kVecThreads) k_pass_sums(Geometry g, const dou
   }
 }
 
-__global__ void __launch_bounds__(kVecThreads) k2_dual(Buffers B, Geometry g, SolveConfig cfg) {
+// Block `bid` of the `nblocks` = dual_row_blocks + col_blocks blocks of the
+// dual step; the last to finish runs the step control.
+__device__ __forceinline__ void k2_dual_body(const Buffers& B, const Geometry& g, const SolveConfig& cfg,
+                                             const int bid, const unsigned nblocks) {
   DevState* st = B.st;
   if (st->done | st->numerical_error) return;
   const int buf = st->buf;
@@ -464,7 +470,6 @@ __global__ void __launch_bounds__(kVecThreads) k2_dual(Buffers B, Geometry g, So
   A.nw = A.first ? 1.0 : __ddiv_rn(tau, S);
   A.aw = A.first ? 1.0 : __ddiv_rn(S, __dadd_rn(S, tau));
   double vals[kStepSums] = {0.0, 0.0};
-  const int bid = blockIdx.x;
   const int rb = g.dual_row_blocks;
   if (bid < rb && rb == g.row_blocks) {
     const int64_t i = (int64_t)bid * kVecThreads + threadIdx.x;
@@ -494,7 +499,7 @@ __global__ void __launch_bounds__(kVecThreads) k2_dual(Buffers B, Geometry g, So
                  B.v[buf ^ 1] + j, A, vals[0], vals[1]);
   }
   block_reduce<kStepSums>(vals, 0u, B.steppart + (int64_t)bid * kStepSums);
-  if (!elect_last_cta(&st->ticket_step)) return;
+  if (!elect_last_of(&st->ticket_step, nblocks)) return;
   // warps 0-2 reduce the three partial sets side by side, warp 3 computes the
   // step rule's powers; thread 0 then runs the step control
   __shared__ double fin[2 * kStepSums + 1];
@@ -523,6 +528,10 @@ __global__ void __launch_bounds__(kVecThreads) k2_dual(Buffers B, Geometry g, So
   }
 }
 
+__global__ void __launch_bounds__(kVecThreads) k2_dual(Buffers B, Geometry g, SolveConfig cfg) {
+  k2_dual_body(B, g, cfg, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------------------
 // Evaluation, matrix part: for the current point (X, G = C - u - v^T, or G = 0
 // before the first accepted step) and, when an average exists, the average
@@ -534,11 +543,14 @@ __global__ void __launch_bounds__(kVecThreads) k2_dual(Buffers B, Geometry g, So
 // and only the reduced-cost sums are written; otherwise every sum is computed
 // here (the first evaluation, a warm start's initial point, an evaluation
 // after a numerical error stopped the step kernels).
+//
+// The plan and the duals are read through L2 (vldcg, __ldcg): in the
+// persistent chunk kernel other CTAs of the same launch wrote them.
 template <typename TX, int CK, int R>
-__global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
+__device__ __forceinline__ void k3_eval_body(const Buffers& B, const Geometry& g, const int64_t cta) {
   DevState* st = B.st;
   if (st->done) return;
-  if (blockIdx.x == 0 && threadIdx.x == 0) st->eval_t0_ns = globaltimer_ns();
+  if (cta == 0 && threadIdx.x == 0) st->eval_t0_ns = globaltimer_ns();
   constexpr int RPL = kPanelRows / (32 * R);
   const int buf = st->buf;
   const bool have_avg = st->avg_count > 0;
@@ -553,7 +565,6 @@ __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
   const double* __restrict__ va = B.v[buf ^ 1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t m = g.m, n = g.n;
-  const int64_t cta = blockIdx.x;
   const int64_t q0 = unit_begin(g, cta), q1 = unit_begin(g, cta + 1);
   double acc[kEvalSums];
 #pragma unroll
@@ -570,14 +581,14 @@ __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
       ok[k] = i < m;
 #pragma unroll
       for (int e = 0; e < R; ++e) {
-        ur[k][e] = ok[k] ? __ldg(u + i + e) : 0.0;
-        uar[k][e] = (ok[k] && have_avg) ? __ldg(ua + i + e) : 0.0;
+        ur[k][e] = ok[k] ? __ldcg(u + i + e) : 0.0;
+        uar[k][e] = (ok[k] && have_avg) ? __ldcg(ua + i + e) : 0.0;
       }
     }
     cost.panel(row0, lane, m, ok);
     for (int64_t j = jb + warp; j < je; j += kWarps) {
-      const double vj = __ldg(v + j);
-      const double vaj = have_avg ? __ldg(va + j) : 0.0;
+      const double vj = __ldcg(v + j);
+      const double vaj = have_avg ? __ldcg(va + j) : 0.0;
       cost.column(j);
       const int64_t base = j * m + row0 + lane * R;
       typename CostReader<CK, R, RPL>::value_t cv[RPL][R];
@@ -588,8 +599,8 @@ __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
           const int64_t idx = base + k * 32 * R;
           cost.get(idx, k, cv[k]);
           if (need_x) {
-            vldg<TX, R>(X + idx, xv[k]);
-            if (have_avg) vldg<TX, R>(Xa + idx, av[k]);
+            vldcg<TX, R>(X + idx, xv[k]);
+            if (have_avg) vldcg<TX, R>(Xa + idx, av[k]);
           }
         }
       }
@@ -643,10 +654,17 @@ __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
   }
 }
 
+template <typename TX, int CK, int R>
+__global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
+  k3_eval_body<TX, CK, R>(B, g, blockIdx.x);
+}
+
 // start_only: the evaluation of a warm start's initial point, run once after
 // k0_init; its last CTA records the point as the last restart point
 // (record_start_point) and takes no other step of the evaluation block.
-__global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, SolveConfig cfg, int start_only) {
+// Block `bid` of the `nblocks` = row_blocks + col_blocks blocks.
+__device__ __forceinline__ void k4_eval_body(const Buffers& B, const Geometry& g, const SolveConfig& cfg,
+                                             const int start_only, const int bid, const unsigned nblocks) {
   DevState* st = B.st;
   if (st->done) return;
   const int buf = st->buf;
@@ -654,7 +672,6 @@ __global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, So
   double acc[kVecSums];
 #pragma unroll
   for (int k = 0; k < kVecSums; ++k) acc[k] = 0.0;
-  const int bid = blockIdx.x;
   const bool is_row = bid < g.row_blocks;
   const int64_t idx = (int64_t)(is_row ? bid : bid - g.row_blocks) * kVecThreads + threadIdx.x;
   const int64_t len = is_row ? g.m : g.n;
@@ -680,7 +697,7 @@ __global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, So
     }
   }
   block_reduce<kVecSums>(acc, kVecMaxMask, B.vecpart + (int64_t)bid * kVecSums);
-  if (!elect_last_cta(&st->ticket_eval)) return;
+  if (!elect_last_of(&st->ticket_eval, nblocks)) return;
   // warps 0-2 reduce the three partial sets side by side
   __shared__ double fin[kEvalSums + 2 * kVecSums];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -712,6 +729,85 @@ __global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, So
     else
       eval_control(st, cfg, cur, avg, B.ring, B.ring_cap);
     st->ticket_eval = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, SolveConfig cfg, int start_only) {
+  k4_eval_body(B, g, cfg, start_only, blockIdx.x, gridDim.x);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent chunk: one cooperative launch runs a regular chunk of loop bodies
+// (the evaluation, then `steps` iterations of primal pass and dual step) with
+// grid barriers between the phases instead of kernel boundaries: for small
+// problems the launches, the kernel tails and the dual step's chains of L2
+// round trips, not the bytes, set the time of an iteration.
+//
+// Every phase runs the body of its own kernel over the same CTA ranges of the
+// matrix passes (physical CTA b takes ranges b, b + gridDim.x, ...) and the same
+// blocks of the vector passes, with the same last-block elections, so the
+// results are bit-identical to the launches the chunk replaces. Each CTA reads
+// the solver state after the same barrier, so all of them leave together once
+// the solve is done. A barrier whose poll runs out records kernel_error and the
+// CTA leaves; the others' polls see the error and leave too.
+//
+// Each phase is a call of its own (not inlined into the loop), so that its
+// registers are allocated as in its own kernel.
+static_assert(kThreads == kVecThreads, "the chunk kernel runs the vector passes' blocks on its CTAs");
+template <typename TX, int CK, int R, bool XS>
+__device__ __noinline__ void chunk_primal(const Buffers& B, const Geometry& g, int64_t cta) {
+  k1_primal_impl<TX, CK, R, XS>(B, g, cta);
+}
+template <typename TX, int CK, int R>
+__device__ __noinline__ void chunk_eval_matrix(const Buffers& B, const Geometry& g, int64_t cta) {
+  k3_eval_body<TX, CK, R>(B, g, cta);
+}
+__device__ __noinline__ void chunk_eval_vector(const Buffers& B, const Geometry& g, const SolveConfig& cfg, int bid,
+                                               unsigned nblocks) {
+  k4_eval_body(B, g, cfg, 0, bid, nblocks);
+}
+__device__ __noinline__ void chunk_dual(const Buffers& B, const Geometry& g, const SolveConfig& cfg, int bid,
+                                        unsigned nblocks) {
+  k2_dual_body(B, g, cfg, bid, nblocks);
+}
+
+template <typename TX, int CK, int R>
+__global__ void __launch_bounds__(kThreads, 2) k_chunk(Buffers B, Geometry g, SolveConfig cfg, int steps) {
+  DevState* st = B.st;
+  const unsigned P = gridDim.x;
+  auto sync = [&]() -> bool {
+    if (grid_barrier(&st->bar_count, &st->bar_gen, P, &st->kernel_error)) return true;
+    if (threadIdx.x == 0) atomicExch(&st->kernel_error, 1);
+    return false;
+  };
+  const unsigned vb = (unsigned)(g.row_blocks + g.col_blocks);
+  const unsigned db = (unsigned)(g.dual_row_blocks + g.col_blocks);
+  for (int64_t c = blockIdx.x; c < g.grid; c += P) {
+    chunk_eval_matrix<TX, CK, R>(B, g, c);
+    __syncthreads();
+  }
+  if (!sync()) return;
+  for (unsigned b = blockIdx.x; b < vb; b += P) {
+    chunk_eval_vector(B, g, cfg, (int)b, vb);
+    __syncthreads();
+  }
+  if (!sync()) return;
+  for (int k = 0; k < steps; ++k) {
+    if (st->done | st->numerical_error) return;  // the same value in every CTA
+    const bool xs = k == steps - 1;               // the next chunk starts with an evaluation
+    for (int64_t c = blockIdx.x; c < g.grid; c += P) {
+      if (xs)
+        chunk_primal<TX, CK, R, true>(B, g, c);
+      else
+        chunk_primal<TX, CK, R, false>(B, g, c);
+      __syncthreads();
+    }
+    if (!sync()) return;
+    for (unsigned b = blockIdx.x; b < db; b += P) {
+      chunk_dual(B, g, cfg, (int)b, db);
+      __syncthreads();
+    }
+    if (!sync()) return;
   }
 }
 
@@ -893,6 +989,22 @@ __global__ void k_widen(const float* __restrict__ src, double* __restrict__ dst,
     }                                                                                      \
   } while (0)
 
+// The 16-byte variants only (g.vec > 1): the persistent chunk kernel.
+#define PDOT_VEC_VARIANT(g, KERNEL, LAUNCH)  \
+  do {  \
+    if (!(g).plan_f32) { auto kfn = KERNEL<double, PDOT_COST_F64, 2>; LAUNCH; }  \
+    else if ((g).cost_kind == PDOT_COST_F32) { auto kfn = KERNEL<float, PDOT_COST_F32, 4>; LAUNCH; }  \
+    else if ((g).cost_kind == PDOT_COST_BF16) { auto kfn = KERNEL<float, PDOT_COST_BF16, 4>; LAUNCH; }  \
+    else if ((g).cost_kind == kCostSqBase + 1) { auto kfn = KERNEL<float, kCostSqBase + 1, 4>; LAUNCH; }  \
+    else if ((g).cost_kind == kCostSqBase + 2) { auto kfn = KERNEL<float, kCostSqBase + 2, 4>; LAUNCH; }  \
+    else if ((g).cost_kind == kCostSqBase + 3) { auto kfn = KERNEL<float, kCostSqBase + 3, 4>; LAUNCH; }  \
+    else if ((g).cost_kind == kCostSqBase + 4) { auto kfn = KERNEL<float, kCostSqBase + 4, 4>; LAUNCH; }  \
+    else if ((g).cost_kind == kCostL1Base + 1) { auto kfn = KERNEL<float, kCostL1Base + 1, 4>; LAUNCH; }  \
+    else if ((g).cost_kind == kCostL1Base + 2) { auto kfn = KERNEL<float, kCostL1Base + 2, 4>; LAUNCH; }  \
+    else if ((g).cost_kind == kCostL1Base + 3) { auto kfn = KERNEL<float, kCostL1Base + 3, 4>; LAUNCH; }  \
+    else { auto kfn = KERNEL<float, kCostL1Base + 4, 4>; LAUNCH; }  \
+  } while (0)
+
 // The staged fused pass exists for the 16-byte path of every variant
 // (KERNEL: k1_primal_staged or k1_primal_staged_xs).
 #define PDOT_STAGED_VARIANT(g, KERNEL, LAUNCH)                                                      \
@@ -957,6 +1069,20 @@ Geometry make_geometry(int64_t m, int64_t n, int vec_ok, int device, int plan_f3
   int64_t grid = (int64_t)sms * occ;
   if (grid > g.units) grid = g.units;
   g.grid = (int32_t)grid;
+  // the persistent chunk kernel: the direct 16-byte passes only, as many CTAs
+  // as stay co-resident (at most one per CTA range)
+  g.chunk_ctas = 0;
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+  if (!g.tma && g.vec > 1 && coop) {
+    int cocc = 0;
+    PDOT_VEC_VARIANT(g, k_chunk, {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cocc, kfn, kThreads, 0) != cudaSuccess) cocc = 0;
+    });
+    cudaGetLastError();
+    const int64_t c = (int64_t)sms * cocc;
+    g.chunk_ctas = (int32_t)(c < g.grid ? c : g.grid);
+  }
   g.row_blocks = (int32_t)((m + kVecThreads - 1) / kVecThreads);
   g.col_blocks = (int32_t)((n + kVecThreads - 1) / kVecThreads);
   // the most CTA slots one panel's row partials can lie in
@@ -1000,6 +1126,19 @@ cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& 
   cudaError_t e = launch_primal(B, g, s, xsums);
   if (e != cudaSuccess) return e;
   return launch_dual(B, g, cfg, s);
+}
+
+cudaError_t launch_chunk(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s,
+                         int steps) {
+  if (g.chunk_ctas < 1) return cudaErrorNotSupported;
+  Buffers b = B;
+  Geometry gg = g;
+  SolveConfig c = cfg;
+  void* args[] = {&b, &gg, &c, &steps};
+  cudaError_t e = cudaSuccess;
+  PDOT_VEC_VARIANT(g, k_chunk,
+                   (e = cudaLaunchCooperativeKernel((const void*)kfn, dim3(g.chunk_ctas), dim3(kThreads), args, 0, s)));
+  return e;
 }
 
 cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s,

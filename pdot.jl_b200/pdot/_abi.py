@@ -104,6 +104,7 @@ class SolverOptionsC(ct.Structure):
         ("warm_restart_at_zero", ct.c_int32),
         ("warm_primal_weight", ct.c_double),
         ("batch_unit_cost", ct.c_double),
+        ("persistent_chunks", ct.c_int32),
     ]
 
 

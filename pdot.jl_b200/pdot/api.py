@@ -372,7 +372,7 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
              cost: Optional[str] = None, points=None, cost_scale: Optional[float] = None, warm_start=None,
              device_pointers: bool = False, primal_pass: str = "auto", recover_plan=None,
              fail_bounded_waits: bool = False, warm_primal_weight: Optional[float] = None,
-             warm_restart: str = "warm"):
+             warm_restart: str = "warm", persistent: Optional[bool] = None):
     """Build pdot_solver_options. Returns (options, objects to keep alive).
 
     precision  "f64" (the drop-in) or "f32" (mixed precision: FP32 plan)
@@ -392,6 +392,8 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
     warm_restart  with a warm start, where the restart information starts:
                "warm" (the warm point, as the reference's starts at its initial
                point) or "zero" (the zero point, as a cold start's)
+    persistent  regular chunks as one persistent cooperative launch: None
+               automatic (small problems), True whenever available, False never
     """
     keep = []
     opts = _abi.SolverOptionsC()
@@ -405,6 +407,7 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
     opts.fail_bounded_waits = 1 if fail_bounded_waits else 0
     opts.warm_primal_weight = float(warm_primal_weight) if warm_primal_weight else 0.0
     opts.warm_restart_at_zero = {"warm": 0, "zero": 1}[warm_restart]
+    opts.persistent_chunks = {None: 0, True: 1, False: -1}[persistent]
     if recover_plan is not None:
         opts.warm_plan_epsilon = float(recover_plan[0])
         opts.warm_plan_iterations = int(recover_plan[1])
@@ -452,12 +455,14 @@ def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device
              use_cuda_graph: bool = True, precision: str = "f64", cost: Optional[str] = None, points=None,
              cost_scale: Optional[float] = None, warm_start=None, primal_pass: str = "auto",
              recover_plan=None, fail_bounded_waits: bool = False,
-             warm_primal_weight: Optional[float] = None, warm_restart: str = "warm") -> SaddlePointOutput:
+             warm_primal_weight: Optional[float] = None, warm_restart: str = "warm",
+             persistent: Optional[bool] = None) -> SaddlePointOutput:
     """PDOT.optimize, src/solver_gpu.jl:413-720, run by libpdot.so on the GPU.
 
     The keyword options beyond `device` select this implementation's mixed
-    precision (FP32 plan; FP32/BF16/coordinate cost) and a warm start from
-    given duals (and plan); the defaults are the FP64 drop-in."""
+    precision (FP32 plan; FP32/BF16/coordinate cost), a warm start from
+    given duals (and plan) and how regular chunks launch (`persistent`, see
+    _options); the defaults are the FP64 drop-in."""
     validate(params)
     lib = _abi.load()
     mp = MarshalledProblem(problem)
@@ -465,7 +470,8 @@ def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device
     opts, _keep = _options(device, use_cuda_graph, precision=precision, cost=cost, points=points,
                            cost_scale=cost_scale, warm_start=warm_start, primal_pass=primal_pass,
                            recover_plan=recover_plan, fail_bounded_waits=fail_bounded_waits,
-                           warm_primal_weight=warm_primal_weight, warm_restart=warm_restart)
+                           warm_primal_weight=warm_primal_weight, warm_restart=warm_restart,
+                           persistent=persistent)
     ob = OutputBuffers(mp.m, mp.n, stats_capacity_for(params))
     rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
     _abi.check(lib, rc, "pdot_optimize")
@@ -482,7 +488,8 @@ class Solver:
                  device_problem=None, device: int = 0, use_cuda_graph: bool = True,
                  time_kernels: bool = False, precision: str = "f64", cost: Optional[str] = None,
                  points=None, cost_scale: Optional[float] = None, warm_start=None, primal_pass: str = "auto",
-                 recover_plan=None, warm_primal_weight: Optional[float] = None, warm_restart: str = "warm"):
+                 recover_plan=None, warm_primal_weight: Optional[float] = None, warm_restart: str = "warm",
+                 persistent: Optional[bool] = None):
         validate(params)
         self._lib = _abi.load()
         self._params = params
@@ -491,7 +498,7 @@ class Solver:
                                     points=points, cost_scale=cost_scale, warm_start=warm_start,
                                     device_pointers=device_problem is not None, primal_pass=primal_pass,
                                     recover_plan=recover_plan, warm_primal_weight=warm_primal_weight,
-                                    warm_restart=warm_restart)
+                                    warm_restart=warm_restart, persistent=persistent)
         handle = ct.c_void_p()
         if device_problem is not None:
             m, n, cptr, aptr, bptr = device_problem

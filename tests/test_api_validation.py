@@ -89,3 +89,20 @@ def test_warm_restart_flag_is_validated_before_device_work(built):
     assert "warm_restart_at_zero" in _abi.last_error(lib)
     with pytest.raises(KeyError):
         api._options(0, True, warm_restart="later")
+
+
+def test_persistent_chunks_flag_is_validated_before_device_work(built):
+    prob = instances.uniform_sqeuclid(4, 3, seed=0)
+    lib = _abi.load()
+    mp = api.MarshalledProblem(prob)
+    cp = api.marshal_params(pdot.default_parameters(1e-4))
+    opts = _abi.SolverOptionsC()
+    opts.use_cuda_graph = 1
+    opts.persistent_chunks = 2
+    ob = api.OutputBuffers(4, 3, 16)
+    rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
+    assert rc == _abi.PDOT_ERR_INVALID_ARGUMENT
+    assert "persistent_chunks" in _abi.last_error(lib)
+    assert api._options(0, True)[0].persistent_chunks == 0
+    assert api._options(0, True, persistent=True)[0].persistent_chunks == 1
+    assert api._options(0, True, persistent=False)[0].persistent_chunks == -1

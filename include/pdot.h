@@ -183,8 +183,8 @@ typedef struct pdot_solver_options {
   /* Regular chunks of loop bodies (the evaluation and the steps up to the next
    * one) as one persistent cooperative launch with grid barriers between the
    * phases, instead of a CUDA graph of separate launches; the results are
-   * bit-identical. 0: automatic (small problems, when CUDA graphs are on),
-   * 1: whenever the direct 16-byte pass runs, -1: never. */
+   * bit-identical. 0: automatic (the CUDA graph, which measured faster on
+   * B200), 1: whenever the direct 16-byte pass runs, -1: never. */
   int32_t persistent_chunks;
 } pdot_solver_options;
 

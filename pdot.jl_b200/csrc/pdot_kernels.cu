@@ -321,12 +321,6 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
       }
     }
     cost.panel(row0, lane, m, ok);
-    // the column's dual and coordinates are loaded one unit ahead
-    double vnext = 0.0;
-    if (cons.valid && cons.p == p) {
-      if (!zero_g) vnext = __ldg(v + cons.j);
-      cost.prefetch(cons.j);
-    }
     while (!failed && cons.valid && cons.p == p) {
       const int64_t j = cons.j;
       const int stage = cstage;
@@ -339,12 +333,8 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
       const TC* sC = reinterpret_cast<const TC*>(stg);
       const TX* sX = reinterpret_cast<const TX*>(stg + L::kCBytes);
       const TX* sXa = reinterpret_cast<const TX*>(stg + L::kCBytes + L::kXBytes);
-      const double vj = vnext;
-      cost.take();
-      if (j + kWarps < cons.je) {
-        if (!zero_g) vnext = __ldg(v + j + kWarps);
-        cost.prefetch(j + kWarps);
-      }
+      const double vj = zero_g ? 0.0 : __ldg(v + j);
+      cost.column(j);
       const int64_t base = j * m + row0 + lane * R;
       double cs = 0.0;
 #pragma unroll

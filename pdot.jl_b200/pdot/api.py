@@ -393,7 +393,8 @@ def _options(device: int, use_cuda_graph: bool, time_kernels: bool = False, *, p
                "warm" (the warm point, as the reference's starts at its initial
                point) or "zero" (the zero point, as a cold start's)
     persistent  regular chunks as one persistent cooperative launch: None
-               automatic (small problems), True whenever available, False never
+               automatic (the CUDA graph, faster on B200), True whenever
+               available, False never
     """
     keep = []
     opts = _abi.SolverOptionsC()

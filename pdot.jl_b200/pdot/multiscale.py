@@ -124,17 +124,19 @@ def learned_to_fine_duals(xs, ys, a, b, starter, *, scale: float | None = None, 
 
 
 def coarse_to_fine_duals(xs, ys, a, b, *, G: int = 64, tol: float = 1e-4, iteration_limit: int = 200_000,
-                         scale: float | None = None, device: int = 0):
+                         scale: float | None = None, device: int = 0, precision: str = "f64"):
     """Warm-start duals (u, v) for the fine problem, and facts about the coarse
     solve. The binning and the coarse cost are host work on at most G^2 cells;
-    the normaliser, the coarse solve and the c-transforms run on the GPU."""
+    the normaliser, the coarse solve and the c-transforms run on the GPU.
+    `precision` is the coarse solve's plan precision ("f64", or "f32" with an
+    FP32 copy of the coarse cost)."""
     xs, ys = np.asarray(xs, dtype=np.float64), np.asarray(ys, dtype=np.float64)
     s = scale if scale is not None else 1.0 / max_sq_distance(xs, ys, device=device)
     Cc, A, B, ca, cb = coarse_problem(xs, ys, a, b, G, s)
     from .solve import default_parameters
 
     params = default_parameters(tol, iteration_limit=iteration_limit)
-    out = api.optimize(params, api.OptimalTransportProblem(Cc, A, B), device=device)
+    out = api.optimize(params, api.OptimalTransportProblem(Cc, A, B), device=device, precision=precision)
     u = c_transform(xs, cb, out.dual_target_solution, s, device=device)
     v = c_transform(ys, ca, out.dual_source_solution, s, device=device)
     info = {"cells": [int(A.size), int(B.size)], "coarse_iterations": out.iteration_count,

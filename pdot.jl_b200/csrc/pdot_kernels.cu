@@ -744,25 +744,36 @@ __global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, So
 // Each phase is a call of its own (not inlined into the loop), so that its
 // registers are allocated as in its own kernel.
 static_assert(kThreads == kVecThreads, "the chunk kernel runs the vector passes' blocks on its CTAs");
+// Build knobs of the chunk kernel: resident CTAs per SM it is compiled for, and
+// whether the phases are calls (0) or inlined (1).
+#ifndef PDOT_CHUNK_MIN_BLOCKS
+#define PDOT_CHUNK_MIN_BLOCKS 2
+#endif
+#if defined(PDOT_CHUNK_INLINE) && PDOT_CHUNK_INLINE
+#define PDOT_CHUNK_PHASE __device__ __forceinline__
+#else
+#define PDOT_CHUNK_PHASE __device__ __noinline__
+#endif
 template <typename TX, int CK, int R, bool XS>
-__device__ __noinline__ void chunk_primal(const Buffers& B, const Geometry& g, int64_t cta) {
+PDOT_CHUNK_PHASE void chunk_primal(const Buffers& B, const Geometry& g, int64_t cta) {
   k1_primal_impl<TX, CK, R, XS>(B, g, cta);
 }
 template <typename TX, int CK, int R>
-__device__ __noinline__ void chunk_eval_matrix(const Buffers& B, const Geometry& g, int64_t cta) {
+PDOT_CHUNK_PHASE void chunk_eval_matrix(const Buffers& B, const Geometry& g, int64_t cta) {
   k3_eval_body<TX, CK, R>(B, g, cta);
 }
-__device__ __noinline__ void chunk_eval_vector(const Buffers& B, const Geometry& g, const SolveConfig& cfg, int bid,
+PDOT_CHUNK_PHASE void chunk_eval_vector(const Buffers& B, const Geometry& g, const SolveConfig& cfg, int bid,
                                                unsigned nblocks) {
   k4_eval_body(B, g, cfg, 0, bid, nblocks);
 }
-__device__ __noinline__ void chunk_dual(const Buffers& B, const Geometry& g, const SolveConfig& cfg, int bid,
+PDOT_CHUNK_PHASE void chunk_dual(const Buffers& B, const Geometry& g, const SolveConfig& cfg, int bid,
                                         unsigned nblocks) {
   k2_dual_body(B, g, cfg, bid, nblocks);
 }
 
 template <typename TX, int CK, int R>
-__global__ void __launch_bounds__(kThreads, 2) k_chunk(Buffers B, Geometry g, SolveConfig cfg, int steps) {
+__global__ void __launch_bounds__(kThreads, PDOT_CHUNK_MIN_BLOCKS)
+    k_chunk(Buffers B, Geometry g, SolveConfig cfg, int steps) {
   DevState* st = B.st;
   const unsigned P = gridDim.x;
   auto sync = [&]() -> bool {

@@ -449,12 +449,12 @@ def run_c2(args, device, local):
     return res
 
 
-WARM_GRID, WARM_EPS, WARM_ROUNDS = 96, 3e-4, 100  # coarse-to-fine warm start of the 20000 x 15000 solve
+WARM_GRID, WARM_EPS, WARM_ROUNDS = 128, 3e-4, 100  # coarse-to-fine warm start of the 20000 x 15000 solve
 
 
 def run_warm_mixed(args, params, m, n, xs, ys, a_h, b_h, Ct, a, b, xs_d, ys_d, device, local, fp64_ttk):
     """The mixed-precision solve (FP32 plan, cost from FP32 coordinates) from
-    the coarse-to-fine warm start: points binned on a 96 x 96 grid, the binned
+    the coarse-to-fine warm start: points binned on a 128 x 128 grid, the binned
     problem solved, its duals extended to every point by the c-transform, a
     plan recovered from them by 100 balancing rounds (eps 3e-4), then PDHG to
     relative KKT 1e-4. One wall-clock region covers all of it, from the host

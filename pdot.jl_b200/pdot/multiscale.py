@@ -123,7 +123,7 @@ def learned_to_fine_duals(xs, ys, a, b, starter, *, scale: float | None = None, 
     return u, v, {"cells": [int(ia.size), int(ib.size)]}
 
 
-def coarse_to_fine_duals(xs, ys, a, b, *, G: int = 64, tol: float = 1e-4, iteration_limit: int = 200_000,
+def coarse_to_fine_duals(xs, ys, a, b, *, G: int = 128, tol: float = 1e-4, iteration_limit: int = 200_000,
                          scale: float | None = None, device: int = 0, precision: str = "f64"):
     """Warm-start duals (u, v) for the fine problem, and facts about the coarse
     solve. The binning and the coarse cost are host work on at most G^2 cells;

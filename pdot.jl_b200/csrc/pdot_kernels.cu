@@ -740,16 +740,18 @@ __global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, So
 // the solver state after the same barrier, so all of them leave together once
 // the solve is done. A barrier whose poll runs out records kernel_error and the
 // CTA leaves; the others' polls see the error and leave too.
-//
-// Each phase is a call of its own (not inlined into the loop), so that its
-// registers are allocated as in its own kernel.
 static_assert(kThreads == kVecThreads, "the chunk kernel runs the vector passes' blocks on its CTAs");
 // Build knobs of the chunk kernel: resident CTAs per SM it is compiled for, and
-// whether the phases are calls (0) or inlined (1).
+// whether the phases are inlined (1) or calls (0). The default, 1 CTA per SM
+// with inlined phases, measured fastest of the four on B200 (no spills; each
+// CTA runs two of the matrix passes' CTA ranges).
 #ifndef PDOT_CHUNK_MIN_BLOCKS
-#define PDOT_CHUNK_MIN_BLOCKS 2
+#define PDOT_CHUNK_MIN_BLOCKS 1
 #endif
-#if defined(PDOT_CHUNK_INLINE) && PDOT_CHUNK_INLINE
+#ifndef PDOT_CHUNK_INLINE
+#define PDOT_CHUNK_INLINE 1
+#endif
+#if PDOT_CHUNK_INLINE
 #define PDOT_CHUNK_PHASE __device__ __forceinline__
 #else
 #define PDOT_CHUNK_PHASE __device__ __noinline__

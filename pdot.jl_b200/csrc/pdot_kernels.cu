@@ -93,7 +93,7 @@ __device__ __forceinline__ void primal_pass_body(const CostSource& csrc, float s
     const int64_t je = (q1 < (p + 1) * n ? q1 : (p + 1) * n) - p * n;
     const int64_t row0 = p * kPanelRows;
     double acc[RPL][R];
-    double ur[RPL][R];
+    TX ur[RPL][R];  // an FP32 plan's entry arithmetic takes u_i in FP32: rounded once per panel
     bool ok[RPL];
 #pragma unroll
     for (int k = 0; k < RPL; ++k) {
@@ -102,7 +102,7 @@ __device__ __forceinline__ void primal_pass_body(const CostSource& csrc, float s
 #pragma unroll
       for (int e = 0; e < R; ++e) {
         acc[k][e] = 0.0;
-        ur[k][e] = (ok[k] && !zero_g) ? __ldcg(u + i + e) : 0.0;
+        ur[k][e] = (ok[k] && !zero_g) ? (TX)__ldcg(u + i + e) : (TX)0;
       }
     }
     cost.panel(row0, lane, m, ok);
@@ -308,7 +308,7 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
   for (int64_t p = q0 / n; p * n < q1; ++p) {
     const int64_t row0 = p * kPanelRows;
     double acc[RPL][R];
-    double ur[RPL][R];
+    TX ur[RPL][R];  // an FP32 plan's entry arithmetic takes u_i in FP32: rounded once per panel
     bool ok[RPL];
 #pragma unroll
     for (int k = 0; k < RPL; ++k) {
@@ -317,7 +317,7 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
 #pragma unroll
       for (int e = 0; e < R; ++e) {
         acc[k][e] = 0.0;
-        ur[k][e] = (ok[k] && !zero_g) ? __ldg(u + i + e) : 0.0;
+        ur[k][e] = (ok[k] && !zero_g) ? (TX)__ldg(u + i + e) : (TX)0;
       }
     }
     cost.panel(row0, lane, m, ok);

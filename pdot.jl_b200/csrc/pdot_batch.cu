@@ -123,6 +123,14 @@ __device__ __forceinline__ int find_segment(const long long* prefix, int count, 
 }
 
 
+// A lane's per-load partial sums added in load order.
+__device__ __forceinline__ double lane_sum(const double (&x)[kBRPL]) {
+  double t = x[0];
+#pragma unroll
+  for (int kq = 1; kq < kBRPL; ++kq) t += x[kq];
+  return t;
+}
+
 // Fixed-order sum of the non-empty CTA slots [lo, hi] (+ offset) of K values.
 template <int K>
 __device__ __forceinline__ void sum_cta_slots(const double* part, const long long* cta_begin, long long lo,
@@ -192,7 +200,11 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
     csrc.ys = B.ys ? B.ys + I.tpts_off * B.dim : nullptr;
     csrc.dim = B.dim;
     CostReader<CK, kBR, kBRPL> cost(csrc, (float)st->cost_scale);
-    double sq = 0.0;
+    // the sums of a lane's two row loads are kept apart (two shorter dependency
+    // chains) and added at the end of the unit / segment
+    double sqk[kBRPL];
+#pragma unroll
+    for (int kq = 0; kq < kBRPL; ++kq) sqk[kq] = 0.0;
     const long long ql0 = q - base_u, ql1 = seg_end - base_u;  // local unit range
     for (long long p = ql0 / I.n; p * I.n < ql1; ++p) {
       const long long jb = (ql0 > p * I.n ? ql0 : p * I.n) - p * I.n;
@@ -241,7 +253,9 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
           const long long jj = j + ju * kWarps;
           if (jj >= je) continue;
           const long long col = jj * I.ld + row0 + lane * kBR;
-          double cs = 0.0;
+          double csk[kBRPL];
+#pragma unroll
+          for (int kq = 0; kq < kBRPL; ++kq) csk[kq] = 0.0;
 #pragma unroll
           for (int kq = 0; kq < kBRPL; ++kq) {
             if (ok[kq]) {
@@ -253,8 +267,8 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
                   primal_entry<float>(widen(cv[ju][kq][e]), ur[kq][e], vj[ju], s, nw, aw, zero_g, first,
                                       xv[ju][kq][e], av[ju][kq][e], d);
                   acc[kq][e] += d;
-                  cs += d;
-                  sq = __fma_rn(d, d, sq);
+                  csk[kq] += d;
+                  sqk[kq] = __fma_rn(d, d, sqk[kq]);
                 } else {  // padded row
                   xv[ju][kq][e] = 0.0f;
                   av[ju][kq][e] = 0.0f;
@@ -265,7 +279,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
               vst<float, kBR>(Xa + idx, av[ju][kq]);
             }
           }
-          cs = warp_sum(cs);
+          const double cs = warp_sum(lane_sum(csk));
           if (lane == 0) B.colpart[base_u + p * I.n + jj] = cs;
         }
       }
@@ -283,7 +297,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
       }
       __syncthreads();
     }
-    sq = warp_sum(sq);
+    const double sq = warp_sum(lane_sum(sqk));
     if (lane == 0) sqw[warp] = sq;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -407,13 +421,13 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
 
   // lane 0 fills stage t with the producer cursor's unit
   auto issue = [&](const BatchCursor& c, int t) {
-    const long long row0 = (long long)c.p * kPanelRows;
-    const long long rows = ((long long)c.ld - row0) < kPanelRows ? ((long long)c.ld - row0) : kPanelRows;
+    const int row0 = c.p * kPanelRows;
+    const int rows = (c.ld - row0) < kPanelRows ? (c.ld - row0) : kPanelRows;
     const uint32_t xb = (uint32_t)(rows * 4);
     const uint32_t cb = L::kPts ? 0u : xb;
     const uint32_t bar = bar0 + 8 * t;
     unsigned char* stg = ring + (size_t)t * L::kStageBytes;
-    const long long off = (long long)c.j * c.ld + row0;
+    const int off = c.j * c.ld + row0;  // inside the instance: fewer than 2^31 entries
     mbar_expect_tx(bar, cb + xb + (c.first ? 0u : xb));
     if (!L::kPts) bulk_g2s(smem_u32(stg), B.C + c.x_off + off, cb, bar);
     bulk_g2s(smem_u32(stg + L::kCBytes), B.X[c.buf] + c.x_off + off, xb, bar);
@@ -459,33 +473,44 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
     csrc.ys = B.ys ? B.ys + I.tpts_off * B.dim : nullptr;
     csrc.dim = B.dim;
     CostReader<CK, kBR, kBRPL> cost(csrc, (float)st->cost_scale);
-    double sq = 0.0;
-    const long long ql0 = q - base_u, ql1 = seg_end - base_u;
-    for (long long p = ql0 / I.n; p * I.n < ql1; ++p) {
-      const long long row0 = p * kPanelRows;
+    // the sums of a lane's two row loads are kept apart (two shorter dependency
+    // chains) and added at the end of the unit / segment
+    double sqk[kBRPL];
+#pragma unroll
+    for (int kq = 0; kq < kBRPL; ++kq) sqk[kq] = 0.0;
+    // offsets inside an instance fit 32 bits (fewer than 2^31 plan entries)
+    const int m32 = (int)I.m, n32 = (int)I.n, ld32 = (int)I.ld;
+    const int ql0 = (int)(q - base_u), ql1 = (int)(seg_end - base_u);
+    for (int p = ql0 / n32; p * n32 < ql1; ++p) {
+      const int row0 = p * kPanelRows;
       double acc[kBRPL][kBR];
       float ur[kBRPL][kBR];
       bool ok[kBRPL];
+      int nv[kBRPL];  // rows of this lane's load that exist (the rest are padding)
 #pragma unroll
       for (int kq = 0; kq < kBRPL; ++kq) {
-        const long long i = row0 + kq * 32 * kBR + lane * kBR;
-        ok[kq] = i < I.m;
+        const int i = row0 + kq * 32 * kBR + lane * kBR;
+        nv[kq] = min(max(m32 - i, 0), kBR);
+        ok[kq] = nv[kq] > 0;
 #pragma unroll
         for (int e = 0; e < kBR; ++e) {
           acc[kq][e] = 0.0;
-          ur[kq][e] = (ok[kq] && i + e < I.m && !zero_g) ? (float)__ldg(u + i + e) : 0.0f;
+          ur[kq][e] = (e < nv[kq] && !zero_g) ? (float)__ldg(u + i + e) : 0.0f;
         }
       }
       cost.panel(row0, lane, I.m, ok);
-      const long long jb = (ql0 > p * I.n ? ql0 : p * I.n) - p * I.n;
-      const long long je = (ql1 < (p + 1) * I.n ? ql1 : (p + 1) * I.n) - p * I.n;
+      const int jb = (ql0 > p * n32 ? ql0 : p * n32) - p * n32;
+      const int je = (ql1 < (p + 1) * n32 ? ql1 : (p + 1) * n32) - p * n32;
+      double* __restrict__ cpart = B.colpart + base_u + (long long)p * n32;
+      float* __restrict__ Xp = X + row0 + lane * kBR;
+      float* __restrict__ Xap = Xa + row0 + lane * kBR;
       // the column's dual and coordinates are loaded one unit ahead
       double vnext = 0.0;
       if (jb + warp < je) {
         if (!zero_g) vnext = __ldg(v + jb + warp);
         cost.prefetch(jb + warp);
       }
-      for (long long j = jb + warp; !failed && j < je; j += kWarps) {
+      for (int j = jb + warp; !failed && j < je; j += kWarps) {
         const int stage = cstage;
         const uint32_t parity = cphase;
         if (!mbar_wait_bounded(bar0 + 8 * stage, parity)) {
@@ -503,8 +528,10 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
           if (!zero_g) vnext = __ldg(v + j + kWarps);
           cost.prefetch(j + kWarps);
         }
-        const long long col = j * I.ld + row0 + lane * kBR;
-        double cs = 0.0;
+        const int col = j * ld32;
+        double csk[kBRPL];
+#pragma unroll
+        for (int kq = 0; kq < kBRPL; ++kq) csk[kq] = 0.0;
 #pragma unroll
         for (int kq = 0; kq < kBRPL; ++kq) {
           if (ok[kq]) {
@@ -517,26 +544,25 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
             float xv[kBR], av[kBR];
             vld<float, kBR>(sX + r, xv);
             if (!first) vld<float, kBR>(sXa + r, av);
-            const long long i = row0 + r;
 #pragma unroll
             for (int e = 0; e < kBR; ++e) {
-              if (i + e < I.m) {
+              if (e < nv[kq]) {
                 double d;
                 primal_entry<float>(widen(cv[e]), ur[kq][e], vj, s, nw, aw, zero_g, first, xv[e], av[e], d);
                 acc[kq][e] += d;
-                cs += d;
-                sq = __fma_rn(d, d, sq);
+                csk[kq] += d;
+                sqk[kq] = __fma_rn(d, d, sqk[kq]);
               } else {  // padded row
                 xv[e] = 0.0f;
                 av[e] = 0.0f;
               }
             }
-            vst<float, kBR>(X + col + kq * 32 * kBR, xv);
-            vst<float, kBR>(Xa + col + kq * 32 * kBR, av);
+            vst<float, kBR>(Xp + col + kq * 32 * kBR, xv);
+            vst<float, kBR>(Xap + col + kq * 32 * kBR, av);
           }
         }
-        cs = warp_sum(cs);
-        if (lane == 0) B.colpart[base_u + p * I.n + j] = cs;
+        const double cs = warp_sum(lane_sum(csk));
+        if (lane == 0) cpart[j] = cs;
         __syncwarp();
         ++consumed;
         if (++cstage == S) {
@@ -563,7 +589,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
       }
       __syncthreads();
     }
-    sq = warp_sum(sq);
+    const double sq = warp_sum(lane_sum(sqk));
     if (lane == 0) sqw[warp] = sq;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1661,8 +1687,13 @@ extern "C" int pdot_optimize_batched(const pdot_batch_problem* problem, const pd
     if (!points && !problem->cost_matrices) bfail(PDOT_ERR_INVALID_ARGUMENT, "null cost matrices");
     if (params->termination_evaluation_frequency < 1 || !(params->primal_importance > 0))
       bfail(PDOT_ERR_INVALID_ARGUMENT, "invalid parameters");
-    for (int64_t k = 0; k < problem->num_instances; ++k)
+    for (int64_t k = 0; k < problem->num_instances; ++k) {
       if (problem->num_rows[k] < 1 || problem->num_cols[k] < 1) bfail(PDOT_ERR_INVALID_ARGUMENT, "empty instance %lld", (long long)k);
+      // the matrix passes index inside an instance with 32-bit offsets
+      if ((problem->num_rows[k] + 3) / 4 * 4 * problem->num_cols[k] >= (int64_t(1) << 31))
+        bfail(PDOT_ERR_INVALID_ARGUMENT, "instance %lld: a batched instance holds fewer than 2^31 plan entries",
+              (long long)k);
+    }
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count < 1) {
       cudaGetLastError();

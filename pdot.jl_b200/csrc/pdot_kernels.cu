@@ -304,7 +304,11 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
   // consumer waits poll up to kSpinLimit times (none under the fail_waits test
   // hook); the drain after a failure always polls up to kSpinLimit times
   const int polls = g.fail_waits ? 0 : kSpinLimit;
-  double sq = 0.0;
+  // a lane's two row loads keep their column and square sums apart (two
+  // shorter dependency chains), added in load order
+  double sqk[RPL];
+#pragma unroll
+  for (int k = 0; k < RPL; ++k) sqk[k] = 0.0;
   for (int64_t p = q0 / n; p * n < q1; ++p) {
     const int64_t row0 = p * kPanelRows;
     double acc[RPL][R];
@@ -336,7 +340,9 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
       const double vj = zero_g ? 0.0 : __ldg(v + j);
       cost.column(j);
       const int64_t base = j * m + row0 + lane * R;
-      double cs = 0.0;
+      double csk[RPL];
+#pragma unroll
+      for (int k = 0; k < RPL; ++k) csk[k] = 0.0;
 #pragma unroll
       for (int k = 0; k < RPL; ++k) {
         if (ok[k]) {
@@ -354,13 +360,16 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
             double d;
             primal_entry<TX>(widen(cv[e]), ur[k][e], vj, s, nw, aw, zero_g, first, xv[e], av[e], d);
             acc[k][e] += d;
-            cs += d;
-            add_sq<TX>(sq, d);
+            csk[k] += d;
+            add_sq<TX>(sqk[k], d);
           }
           vst<TX, R>(X + base + k * 32 * R, xv);
           vst<TX, R>(Xa + base + k * 32 * R, av);
         }
       }
+      double cs = csk[0];
+#pragma unroll
+      for (int k = 1; k < RPL; ++k) cs += csk[k];
       cs = warp_sum(cs);
       if (lane == 0) B.colpart[p * n + j] = cs;
       __syncwarp();
@@ -395,6 +404,9 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
     for (long long c = consumed; c < issued; ++c)
       mbar_wait_bounded(bar0 + 8 * (int)(c % S), (uint32_t)((c / S) & 1));
   }
+  double sq = sqk[0];
+#pragma unroll
+  for (int k = 1; k < RPL; ++k) sq += sqk[k];
   sq = warp_sum(sq);
   if (lane == 0) sqw[warp] = sq;
   __syncthreads();

@@ -60,6 +60,8 @@ struct BatchActive {
   int count;
   int any_empty;          // some CTA range holds no unit (only in the tail of a solve)
   long long total_units;
+  int error;              // a bounded wait gave up: every later launch returns at once
+  int pad_;
 };
 
 struct BatchBuffers {
@@ -172,7 +174,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
   __shared__ double red[kWarps][kPanelRows];
   __shared__ double sqw[kWarps];
   const BatchActive act = *B.act;
-  if (act.count == 0) return;
+  if (act.count == 0 || act.error) return;
   const long long cta = blockIdx.x;
   const long long q0 = B.cta_begin[cta], q1 = B.cta_begin[cta + 1];
   if (q0 >= q1) return;
@@ -408,7 +410,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
   __shared__ double red[kWarps][kPanelRows];
   __shared__ double sqw[kWarps];
   const BatchActive act = *B.act;
-  if (act.count == 0) return;
+  if (act.count == 0 || act.error) return;
   const long long cta = blockIdx.x;
   const long long q0 = B.cta_begin[cta], q1 = B.cta_begin[cta + 1];
   if (q0 >= q1) return;
@@ -517,7 +519,10 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
         const uint32_t parity = cphase;
         if (!mbar_wait_bounded(bar0 + 8 * stage, parity)) {
           failed = true;
-          if (lane == 0) atomicExch(&st->kernel_error, 1);
+          if (lane == 0) {
+            atomicExch(&st->kernel_error, 1);
+            atomicExch(&B.act->error, 1);
+          }
           break;
         }
         const unsigned char* stg = ring + (size_t)stage * L::kStageBytes;
@@ -607,7 +612,10 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
   if (consumed < issued) {
     // only after a timeout: drain the copies still in flight (bounded) before
     // the shared memory goes away, and report
-    if (!failed && lane == 0) atomicExch(&B.st[B.ids[find_segment(B.unit_prefix, act.count, q0)]].kernel_error, 1);
+    if (!failed && lane == 0) {
+      atomicExch(&B.st[B.ids[find_segment(B.unit_prefix, act.count, q0)]].kernel_error, 1);
+      atomicExch(&B.act->error, 1);
+    }
     for (long long c = consumed; c < issued; ++c)
       mbar_wait_bounded(bar0 + 8 * (int)(c % S), (uint32_t)((c / S) & 1));
   }
@@ -616,7 +624,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
 // Batched dual step + per-instance step control (last CTA of each instance).
 __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConfig cfg, int grid) {
   const BatchActive act = *B.act;
-  if (act.count == 0) return;
+  if (act.count == 0 || act.error) return;
   const long long blk = blockIdx.x;
   if (blk >= B.vblock_prefix[act.count]) return;
   const int kk = find_segment(B.vblock_prefix, act.count, blk);
@@ -696,7 +704,7 @@ __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConf
 template <int CK>
 __global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
   const BatchActive act = *B.act;
-  if (act.count == 0) return;
+  if (act.count == 0 || act.error) return;
   const long long cta = blockIdx.x;
   const long long q0 = B.cta_begin[cta], q1 = B.cta_begin[cta + 1];
   if (q0 >= q1) return;
@@ -801,7 +809,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
 __global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, SolveConfig cfg, int grid,
                                                             int start_only) {
   const BatchActive act = *B.act;
-  if (act.count == 0) return;
+  if (act.count == 0 || act.error) return;
   const long long blk = blockIdx.x;
   if (blk >= B.vblock_prefix[act.count]) return;
   const int kk = find_segment(B.vblock_prefix, act.count, blk);
@@ -1408,6 +1416,7 @@ class BatchSolver {
     D_.st = alloc<pdot::DevState>(B);
     D_.rec = alloc<pdot_iteration_stats>(B);
     D_.act = alloc<pdot::BatchActive>(1);
+    BCK(cudaMemset(D_.act, 0, sizeof(pdot::BatchActive)));
     D_.ids = alloc<int>(B);
     D_.unit_prefix = alloc<long long>(B + 1);
     D_.panel_prefix = alloc<long long>(B + 1);
@@ -1453,6 +1462,10 @@ class BatchSolver {
       BCK(cudaEventSynchronize(ev_[completed % 2]));
       const pdot::BatchActive a = host_act_[completed % 2];
       ++completed;
+      if (a.error) {
+        BCK(cudaStreamSynchronize(stream_));
+        bfail(PDOT_ERR_CUDA, "the staged primal pass gave up waiting for its copies");
+      }
       if (a.count == 0) break;
       if (it > (long long)limit_ + 2 * freq_ + 16)
         bfail(PDOT_ERR_CUDA, "batched solve did not finish by the iteration limit");

@@ -436,9 +436,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// Waits for the phase `parity` of an mbarrier: at most `polls` polls and at
+// most about kWaitLimitNs of device time (each try_wait may suspend the
+// thread for a while, so the poll count alone does not bound the time).
+constexpr unsigned long long kWaitLimitNs = 1000000000ull;
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, int polls = kSpinLimit) {
-  for (int it = 0; it < polls; ++it)
+  unsigned long long t0 = 0;
+  for (int it = 0; it < polls; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 1023) == 1023) {
+      const unsigned long long t = globaltimer_ns();
+      if (t0 == 0)
+        t0 = t;
+      else if (t - t0 > kWaitLimitNs)
+        return false;
+    }
+  }
   return false;
 }
 

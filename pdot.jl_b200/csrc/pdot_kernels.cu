@@ -173,7 +173,7 @@ __device__ __forceinline__ void primal_pass_body(const CostSource& csrc, float s
 template <typename TX, int CK, int R, bool XS>
 __device__ __forceinline__ void k1_primal_impl(const Buffers& B, const Geometry& g, const int64_t cta) {
   DevState* st = B.st;
-  if (st->done | st->numerical_error) return;
+  if (st->done | st->numerical_error | st->kernel_error) return;
   const int buf = st->buf;
   const double tau = st->step_size, omega = st->primal_weight, S = st->sum_weights;
   const bool zero_g = st->g_is_zero != 0;
@@ -247,7 +247,7 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
   __shared__ double red[kWarps][kPanelRows];
   __shared__ double sqw[kWarps];
   DevState* st = B.st;
-  if (st->done | st->numerical_error) return;
+  if (st->done | st->numerical_error | st->kernel_error) return;
   const int buf = st->buf;
   const double tau = st->step_size, omega = st->primal_weight, Ssum = st->sum_weights;
   const bool zero_g = st->g_is_zero != 0;
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(kVecThreads) k_pass_sums(Geometry g, const dou
 __device__ __forceinline__ void k2_dual_body(const Buffers& B, const Geometry& g, const SolveConfig& cfg,
                                              const int bid, const unsigned nblocks) {
   DevState* st = B.st;
-  if (st->done | st->numerical_error) return;
+  if (st->done | st->numerical_error | st->kernel_error) return;
   const int buf = st->buf;
   const double tau = st->step_size, omega = st->primal_weight, S = st->sum_weights;
   DualArgs A;
@@ -551,7 +551,7 @@ __global__ void __launch_bounds__(kVecThreads) k2_dual(Buffers B, Geometry g, So
 template <typename TX, int CK, int R>
 __device__ __forceinline__ void k3_eval_body(const Buffers& B, const Geometry& g, const int64_t cta) {
   DevState* st = B.st;
-  if (st->done) return;
+  if (st->done | st->kernel_error) return;
   if (cta == 0 && threadIdx.x == 0) st->eval_t0_ns = globaltimer_ns();
   constexpr int RPL = kPanelRows / (32 * R);
   const int buf = st->buf;
@@ -668,7 +668,7 @@ __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
 __device__ __forceinline__ void k4_eval_body(const Buffers& B, const Geometry& g, const SolveConfig& cfg,
                                              const int start_only, const int bid, const unsigned nblocks) {
   DevState* st = B.st;
-  if (st->done) return;
+  if (st->done | st->kernel_error) return;
   const int buf = st->buf;
   const bool have_avg = st->avg_count > 0;
   double acc[kVecSums];

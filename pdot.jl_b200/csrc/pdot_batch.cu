@@ -425,13 +425,13 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
 
   // lane 0 fills stage t with the producer cursor's unit
   auto issue = [&](const BatchCursor& c, int t) {
-    const int row0 = c.p * kPanelRows;
-    const int rows = (c.ld - row0) < kPanelRows ? (c.ld - row0) : kPanelRows;
+    const long long row0 = (long long)c.p * kPanelRows;
+    const long long rows = ((long long)c.ld - row0) < kPanelRows ? ((long long)c.ld - row0) : kPanelRows;
     const uint32_t xb = (uint32_t)(rows * 4);
     const uint32_t cb = L::kPts ? 0u : xb;
     const uint32_t bar = bar0 + 8 * t;
     unsigned char* stg = ring + (size_t)t * L::kStageBytes;
-    const int off = c.j * c.ld + row0;  // inside the instance: fewer than 2^31 entries
+    const long long off = (long long)c.j * c.ld + row0;
     mbar_expect_tx(bar, cb + xb + (c.first ? 0u : xb));
     if (!L::kPts) bulk_g2s(smem_u32(stg), B.C + c.x_off + off, cb, bar);
     bulk_g2s(smem_u32(stg + L::kCBytes), B.X[c.buf] + c.x_off + off, xb, bar);
@@ -482,19 +482,17 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
     double sqk[kBRPL];
 #pragma unroll
     for (int kq = 0; kq < kBRPL; ++kq) sqk[kq] = 0.0;
-    // offsets inside an instance fit 32 bits (fewer than 2^31 plan entries)
-    const int m32 = (int)I.m, n32 = (int)I.n, ld32 = (int)I.ld;
-    const int ql0 = (int)(q - base_u), ql1 = (int)(seg_end - base_u);
-    for (int p = ql0 / n32; p * n32 < ql1; ++p) {
-      const int row0 = p * kPanelRows;
+    const long long ql0 = q - base_u, ql1 = seg_end - base_u;
+    for (long long p = ql0 / I.n; p * I.n < ql1; ++p) {
+      const long long row0 = p * kPanelRows;
       double acc[kBRPL][kBR];
       float ur[kBRPL][kBR];
       bool ok[kBRPL];
       int nv[kBRPL];  // rows of this lane's load that exist (the rest are padding)
 #pragma unroll
       for (int kq = 0; kq < kBRPL; ++kq) {
-        const int i = row0 + kq * 32 * kBR + lane * kBR;
-        nv[kq] = min(max(m32 - i, 0), kBR);
+        const long long i = row0 + kq * 32 * kBR + lane * kBR;
+        nv[kq] = (int)min(max(I.m - i, 0ll), (long long)kBR);
         ok[kq] = nv[kq] > 0;
 #pragma unroll
         for (int e = 0; e < kBR; ++e) {
@@ -503,18 +501,15 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
         }
       }
       cost.panel(row0, lane, I.m, ok);
-      const int jb = (ql0 > p * n32 ? ql0 : p * n32) - p * n32;
-      const int je = (ql1 < (p + 1) * n32 ? ql1 : (p + 1) * n32) - p * n32;
-      double* __restrict__ cpart = B.colpart + base_u + (long long)p * n32;
-      float* __restrict__ Xp = X + row0 + lane * kBR;
-      float* __restrict__ Xap = Xa + row0 + lane * kBR;
+      const long long jb = (ql0 > p * I.n ? ql0 : p * I.n) - p * I.n;
+      const long long je = (ql1 < (p + 1) * I.n ? ql1 : (p + 1) * I.n) - p * I.n;
       // the column's dual and coordinates are loaded one unit ahead
       double vnext = 0.0;
       if (jb + warp < je) {
         if (!zero_g) vnext = __ldg(v + jb + warp);
         cost.prefetch(jb + warp);
       }
-      for (int j = jb + warp; !failed && j < je; j += kWarps) {
+      for (long long j = jb + warp; !failed && j < je; j += kWarps) {
         const int stage = cstage;
         const uint32_t parity = cphase;
         if (!mbar_wait_bounded(bar0 + 8 * stage, parity)) {
@@ -535,7 +530,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
           if (!zero_g) vnext = __ldg(v + j + kWarps);
           cost.prefetch(j + kWarps);
         }
-        const int col = j * ld32;
+        const long long col = j * I.ld + row0 + lane * kBR;
         double csk[kBRPL];
 #pragma unroll
         for (int kq = 0; kq < kBRPL; ++kq) csk[kq] = 0.0;
@@ -564,12 +559,12 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
                 av[e] = 0.0f;
               }
             }
-            vst<float, kBR>(Xp + col + kq * 32 * kBR, xv);
-            vst<float, kBR>(Xap + col + kq * 32 * kBR, av);
+            vst<float, kBR>(X + col + kq * 32 * kBR, xv);
+            vst<float, kBR>(Xa + col + kq * 32 * kBR, av);
           }
         }
         const double cs = warp_sum(lane_sum(csk));
-        if (lane == 0) cpart[j] = cs;
+        if (lane == 0) B.colpart[base_u + p * I.n + j] = cs;
         __syncwarp();
         ++consumed;
         if (++cstage == S) {
@@ -1704,7 +1699,7 @@ extern "C" int pdot_optimize_batched(const pdot_batch_problem* problem, const pd
       bfail(PDOT_ERR_INVALID_ARGUMENT, "invalid parameters");
     for (int64_t k = 0; k < problem->num_instances; ++k) {
       if (problem->num_rows[k] < 1 || problem->num_cols[k] < 1) bfail(PDOT_ERR_INVALID_ARGUMENT, "empty instance %lld", (long long)k);
-      // the matrix passes index inside an instance with 32-bit offsets
+      // the staged pass's producer cursor keeps positions inside an instance in 32 bits
       if ((problem->num_rows[k] + 7) / 8 * 8 * problem->num_cols[k] >= (int64_t(1) << 31))
         bfail(PDOT_ERR_INVALID_ARGUMENT, "instance %lld: a batched instance holds fewer than 2^31 plan entries",
               (long long)k);

@@ -119,6 +119,28 @@ def test_batched_staged_and_direct_passes_agree(cuda, cost):
         assert np.array_equal(x.dual_source_solution, y.dual_source_solution)
 
 
+@pytest.mark.parametrize("sizes", [[(65, 40), (3, 5), (300, 200)], [(257, 70), (700, 650), (128, 3)],
+                                   [(3, 40), (300, 200)], [(65, 40), (300, 5)]])
+def test_batched_small_instances_both_pass_forms(cuda, sizes):
+    """Batches with a few rows or a few columns (fewer columns than warps, a
+    single 8-row padded panel) beside larger instances, with point costs: the
+    staged pass's copies and waits cover every unit (no bounded wait gives up)
+    and it agrees bit for bit with the direct pass."""
+    rng = np.random.default_rng(1)
+    probs, pts = [], []
+    for m, n in sizes:
+        xs, ys = rng.uniform(0, 1, (m, 2)).astype(np.float32), rng.uniform(0, 1, (n, 2)).astype(np.float32)
+        probs.append(pdot.OptimalTransportProblem(None, rng.dirichlet(np.ones(m)), rng.dirichlet(np.ones(n))))
+        pts.append((xs, ys))
+    params = pdot.default_parameters(1e-4, iteration_limit=3000)
+    st, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts, primal_pass="staged")
+    di, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts, primal_pass="direct")
+    for x, y in zip(st, di):
+        assert x.iteration_count == y.iteration_count
+        assert np.array_equal(x.primal_solution, y.primal_solution)
+        assert np.array_equal(x.dual_target_solution, y.dual_target_solution)
+
+
 def test_autotuner_times_every_candidate_and_picks_the_fastest(cuda):
     probs, pts = instances.batched_l1(count=12, lo=32, hi=400, seed=2)
     best, timings = pdot.tune_batched(pdot.default_parameters(1e-4), probs, cost="l1", points=pts, iterations=64)

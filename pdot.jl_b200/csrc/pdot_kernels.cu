@@ -295,7 +295,6 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
   long long issued = 0, consumed = 0;
   int cstage = 0;           // consumed % S, kept incrementally (no 64-bit division per unit)
   uint32_t cphase = 0;      // (consumed / S) & 1
-  int prev_stage = -1;      // the stage consumed last, refilled once its bulk store has read it
   for (int k = 0; k < S && prod.valid; ++k) {
     if (lane == 0) issue(prod.p, prod.j, k);
     prod.advance(warp);
@@ -334,12 +333,13 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
         failed = true;
         break;
       }
-      unsigned char* stg = ring + (size_t)stage * L::kStageBytes;
+      const unsigned char* stg = ring + (size_t)stage * L::kStageBytes;
       const TC* sC = reinterpret_cast<const TC*>(stg);
-      TX* sX = reinterpret_cast<TX*>(stg + L::kCBytes);
-      TX* sXa = reinterpret_cast<TX*>(stg + L::kCBytes + L::kXBytes);
+      const TX* sX = reinterpret_cast<const TX*>(stg + L::kCBytes);
+      const TX* sXa = reinterpret_cast<const TX*>(stg + L::kCBytes + L::kXBytes);
       const double vj = zero_g ? 0.0 : __ldg(v + j);
       cost.column(j);
+      const int64_t base = j * m + row0 + lane * R;
       double csk[RPL];
 #pragma unroll
       for (int k = 0; k < RPL; ++k) csk[k] = 0.0;
@@ -363,24 +363,9 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
             csk[k] += d;
             add_sq<TX>(sqk[k], d);
           }
-          // the new plan and average go back into the stage ...
-          vst<TX, R>(sX + r, xv);
-          vst<TX, R>(sXa + r, av);
+          vst<TX, R>(X + base + k * 32 * R, xv);
+          vst<TX, R>(Xa + base + k * 32 * R, av);
         }
-      }
-      // ... and one bulk store per array writes the unit out, so the stores
-      // move as two large transfers instead of per-lane 16-byte stores (with
-      // per-lane stores the pass ran its loads and its stores one after the
-      // other: 398 + 482 us against 879 us for both)
-      fence_proxy_async_smem();
-      __syncwarp();
-      if (lane == 0) {
-        const int64_t rows = (m - row0) < kPanelRows ? (m - row0) : kPanelRows;
-        const uint32_t xb = (uint32_t)(rows * sizeof(TX));
-        const int64_t off = j * m + row0;
-        bulk_s2g(X + off, smem_u32(sX), xb);
-        bulk_s2g(Xa + off, smem_u32(sXa), xb);
-        bulk_commit();
       }
       double cs = csk[0];
 #pragma unroll
@@ -394,17 +379,11 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
         cphase ^= 1u;
       }
       cons.advance(warp);
-      // refill the stage consumed one unit earlier: its bulk store has had a
-      // unit's time to read it (the wait lets only the newest store group pend)
-      if (prod.valid && prev_stage >= 0) {
-        if (lane == 0) {
-          bulk_wait_read<1>();
-          issue(prod.p, prod.j, prev_stage);
-        }
+      if (prod.valid) {
+        if (lane == 0) issue(prod.p, prod.j, stage);
         prod.advance(warp);
         ++issued;
       }
-      prev_stage = stage;
     }
 #pragma unroll
     for (int k = 0; k < RPL; ++k)
@@ -425,8 +404,6 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
     for (long long c = consumed; c < issued; ++c)
       mbar_wait_bounded(bar0 + 8 * (int)(c % S), (uint32_t)((c / S) & 1));
   }
-  // the warp's bulk stores complete before its shared memory goes away
-  if (lane == 0) bulk_wait_all();
   double sq = sqk[0];
 #pragma unroll
   for (int k = 1; k < RPL; ++k) sq += sqk[k];

@@ -186,6 +186,12 @@ typedef struct pdot_solver_options {
    * bit-identical. 0: automatic (the CUDA graph, which measured faster on
    * B200), 1: whenever the direct 16-byte pass runs, -1: never. */
   int32_t persistent_chunks;
+  /* Batched solver: the rows of one panel of its matrix passes' tiles (a unit
+   * is one column of one panel): 256 or 128, 0 = 256. A 128-row tile holds
+   * half the registers per thread, so three CTAs per SM are resident where a
+   * 256-row tile allows two, at twice the units of tall instances;
+   * pdot.tune_batched picks the tile. */
+  int32_t batch_panel_rows;
 } pdot_solver_options;
 
 /* ---- output -------------------------------------------------------------- */

@@ -8,10 +8,11 @@
 // duals and control FP64; the cost is stored FP32 or computed from FP32
 // coordinates (squared-Euclidean or L1).
 //
-// Work decomposition: the units (one column of one 256-row panel) of all active
-// instances are concatenated into one line and cut into contiguous CTA ranges
-// of equal cost, a unit costing its rows plus a fixed per-unit overhead (the
-// autotuner picks it). The units of uneven instances carry from 1 to 256 rows,
+// Work decomposition: the units (one column of one panel of 256 or 128 rows,
+// the batch's tile shape) of all active instances are concatenated into one
+// line and cut into contiguous CTA ranges of equal cost, a unit costing its
+// rows plus a fixed per-unit overhead (the autotuner picks the tile and the
+// overhead). The units of uneven instances carry from 1 to 256 rows,
 // so ranges of equal unit count would leave some CTAs with several times the
 // bytes of others. kb_compact recomputes the ranges (cta_begin) whenever the
 // active list changes. Row
@@ -41,9 +42,24 @@ namespace pdot {
 namespace {
 
 constexpr int kBR = 4;                       // FP32 rows per lane load
-constexpr int kBRPL = kPanelRows / (32 * kBR);  // loads per lane per unit
 constexpr int kMaxBatch = 1 << 16;
 constexpr int kJU = 2;  // columns per warp step of the batched primal pass
+
+// Tile shapes of the matrix passes: a unit is one column of one panel of PR
+// rows (256 or 128; the host picks one per batch, the autotuner between them).
+// A lane loads kBR rows PR / 128 times per unit, so a 128-row tile holds half
+// the per-row registers (row sums, row duals, source coordinates) and its
+// primal passes are compiled for three resident CTAs per SM instead of two,
+// with a ring of half the bytes in the staged form. The per-unit overhead of
+// the CTA split stays counted in 256-row units (kUnitCostRows).
+template <int PR>
+struct Tile {
+  static_assert(PR == 128 || PR == 256, "panels of 128 or 256 rows");
+  static constexpr int RPL = PR / (32 * kBR);                    // loads per lane per unit
+  static constexpr int kMinBlocks = PR == 256 ? 2 : 3;           // resident CTAs per SM of the primal passes
+  static constexpr int kRingBudget = PR == 256 ? 96 * 1024 : 48 * 1024;  // staged ring bytes per CTA
+};
+constexpr int kUnitCostRows = 256;
 
 struct BatchInstance {
   int64_t m, n, ld;  // rows, columns, padded leading dimension
@@ -52,7 +68,7 @@ struct BatchInstance {
   int64_t col_off;   // offset of the column vectors (n entries)
   int64_t pts_off;   // offset of the points (rows; times dim for elements)
   int64_t tpts_off;  // offset of the target points (rows)
-  int64_t panels;    // ceil(m / 256)
+  int64_t panels;    // ceil(m / panel rows)
   int64_t rblocks, cblocks;  // vector blocks over rows and columns
 };
 
@@ -78,7 +94,7 @@ struct BatchBuffers {
   double* v[2];
   double* r[2];
   double* c[2];
-  double* rowpart;         // (grid + total panels) * 256
+  double* rowpart;         // (grid + total panels) * panel rows
   double* colpart;         // total units
   double* sqpart;          // grid + num
   double* steppart;        // total vector blocks * kStepSums
@@ -128,10 +144,11 @@ __device__ __forceinline__ int find_segment(const long long* prefix, int count, 
 
 
 // A lane's per-load partial sums added in load order.
-__device__ __forceinline__ double lane_sum(const double (&x)[kBRPL]) {
+template <int N>
+__device__ __forceinline__ double lane_sum(const double (&x)[N]) {
   double t = x[0];
 #pragma unroll
-  for (int kq = 1; kq < kBRPL; ++kq) t += x[kq];
+  for (int kq = 1; kq < N; ++kq) t += x[kq];
   return t;
 }
 
@@ -169,9 +186,10 @@ __device__ __forceinline__ void sum_cta_slots(const double* part, const long lon
 
 // ---------------------------------------------------------------------------
 // Batched fused primal pass (FP32 plan): the per-entry step of pdot_kernels.cu.
-template <int CK>
-__global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
-  __shared__ double red[kWarps][kPanelRows];
+template <int CK, int PR>
+__global__ void __launch_bounds__(kThreads, Tile<PR>::kMinBlocks) kb_primal(BatchBuffers B) {
+  constexpr int kBRPL = Tile<PR>::RPL;
+  __shared__ double red[kWarps][PR];
   __shared__ double sqw[kWarps];
   const BatchActive act = *B.act;
   if (act.count == 0 || act.error) return;
@@ -213,7 +231,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
     for (long long p = ql0 / I.n; p * I.n < ql1; ++p) {
       const long long jb = (ql0 > p * I.n ? ql0 : p * I.n) - p * I.n;
       const long long je = (ql1 < (p + 1) * I.n ? ql1 : (p + 1) * I.n) - p * I.n;
-      const long long row0 = p * kPanelRows;
+      const long long row0 = p * PR;
       double acc[kBRPL][kBR];
       float ur[kBRPL][kBR];  // the FP32 plan's entry arithmetic takes the duals in FP32
       bool ok[kBRPL];
@@ -293,11 +311,11 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
         for (int e = 0; e < kBR; ++e) red[warp][kq * 32 * kBR + lane * kBR + e] = acc[kq][e];
       __syncthreads();
       const long long gp = B.panel_prefix[kk] + p;
-      for (int t = threadIdx.x; t < kPanelRows; t += kThreads) {
+      for (int t = threadIdx.x; t < PR; t += kThreads) {
         double s2 = red[0][t];
 #pragma unroll
         for (int w = 1; w < kWarps; ++w) s2 += red[w][t];
-        B.rowpart[(cta + gp) * kPanelRows + t] = s2;
+        B.rowpart[(cta + gp) * PR + t] = s2;
       }
       __syncthreads();
     }
@@ -327,13 +345,13 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal(BatchBuffers B) {
 // zero in the plan and in the stored cost. Every wait is bounded: on a timeout
 // the kernel sets kernel_error of the instance at hand, drains (bounded) the
 // copies in flight and leaves its remaining units alone.
-template <int CK>
+template <int CK, int PR>
 struct BatchStagedLayout {
   static constexpr bool kPts = is_point_cost(CK);
-  static constexpr int kCBytes = kPts ? 0 : kPanelRows * 4;
-  static constexpr int kXBytes = kPanelRows * 4;
+  static constexpr int kCBytes = kPts ? 0 : PR * 4;
+  static constexpr int kXBytes = PR * 4;
   static constexpr int kStageBytes = kCBytes + 2 * kXBytes;
-  static constexpr int S0 = (96 * 1024) / (kWarps * kStageBytes);
+  static constexpr int S0 = Tile<PR>::kRingBudget / (kWarps * kStageBytes);
   static constexpr int S = S0 > 6 ? 6 : (S0 < 2 ? 2 : S0);
   static constexpr int kRingBytes = kWarps * S * kStageBytes;
   static constexpr int kSmem = kRingBytes + kWarps * S * 8;
@@ -401,13 +419,16 @@ struct BatchCursor {
   }
 };
 
-template <int CK>
-__global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) {
-  using L = BatchStagedLayout<CK>;
-  static_assert(L::kSmem <= 100 * 1024, "two CTAs per SM hold their rings");
+template <int CK, int PR>
+__global__ void __launch_bounds__(kThreads, Tile<PR>::kMinBlocks) kb_primal_staged(BatchBuffers B) {
+  using L = BatchStagedLayout<CK, PR>;
+  constexpr int kBRPL = Tile<PR>::RPL;
+  // the rings, the row-sum tiles and the per-CTA reserve of the resident CTAs fit an SM's 228 KB
+  static_assert((L::kSmem + 8 * kWarps * (PR + 1) + 1024) * Tile<PR>::kMinBlocks <= 228 * 1024,
+                "the resident CTAs hold their rings");
   constexpr int S = L::S;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ double red[kWarps][kPanelRows];
+  __shared__ double red[kWarps][PR];
   __shared__ double sqw[kWarps];
   const BatchActive act = *B.act;
   if (act.count == 0 || act.error) return;
@@ -425,8 +446,8 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
 
   // lane 0 fills stage t with the producer cursor's unit
   auto issue = [&](const BatchCursor& c, int t) {
-    const long long row0 = (long long)c.p * kPanelRows;
-    const long long rows = ((long long)c.ld - row0) < kPanelRows ? ((long long)c.ld - row0) : kPanelRows;
+    const long long row0 = (long long)c.p * PR;
+    const long long rows = ((long long)c.ld - row0) < PR ? ((long long)c.ld - row0) : PR;
     const uint32_t xb = (uint32_t)(rows * 4);
     const uint32_t cb = L::kPts ? 0u : xb;
     const uint32_t bar = bar0 + 8 * t;
@@ -484,7 +505,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
     for (int kq = 0; kq < kBRPL; ++kq) sqk[kq] = 0.0;
     const long long ql0 = q - base_u, ql1 = seg_end - base_u;
     for (long long p = ql0 / I.n; p * I.n < ql1; ++p) {
-      const long long row0 = p * kPanelRows;
+      const long long row0 = p * PR;
       double acc[kBRPL][kBR];
       float ur[kBRPL][kBR];
       bool ok[kBRPL];
@@ -583,11 +604,11 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
         for (int e = 0; e < kBR; ++e) red[warp][kq * 32 * kBR + lane * kBR + e] = acc[kq][e];
       __syncthreads();
       const long long gp = B.panel_prefix[kk] + p;
-      for (int t = threadIdx.x; t < kPanelRows; t += kThreads) {
+      for (int t = threadIdx.x; t < PR; t += kThreads) {
         double s2 = red[0][t];
 #pragma unroll
         for (int w = 1; w < kWarps; ++w) s2 += red[w][t];
-        B.rowpart[(cta + gp) * kPanelRows + t] = s2;
+        B.rowpart[(cta + gp) * PR + t] = s2;
       }
       __syncthreads();
     }
@@ -617,6 +638,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_primal_staged(BatchBuffers B) 
 }
 
 // Batched dual step + per-instance step control (last CTA of each instance).
+template <int PR>
 __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConfig cfg, int grid) {
   const BatchActive act = *B.act;
   if (act.count == 0 || act.error) return;
@@ -639,19 +661,19 @@ __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConf
   if (lb < I.rblocks) {
     const long long i = lb * kVecThreads + threadIdx.x;
     if (i < I.m) {
-      const long long p = i / kPanelRows, t = i - p * kPanelRows;
+      const long long p = i / PR, t = i - p * PR;
       const long long gp = B.panel_prefix[kk] + p;
       const long long lo = bcta_of_unit(B.cta_begin, grid, ubase + p * I.n), hi = bcta_of_unit(B.cta_begin, grid, ubase + (p + 1) * I.n - 1);
       double sd = 0.0;
       if (!act.any_empty) {
         // every CTA owns a unit: the slots c + gp, c = lo..hi, all hold partials
-        sd = sum_strided(B.rowpart + (lo + gp) * kPanelRows + t, hi - lo + 1, kPanelRows);
+        sd = sum_strided(B.rowpart + (lo + gp) * PR + t, hi - lo + 1, PR);
       } else {
         // some CTA ranges are empty (the tail of a solve): skip them, their
         // slots hold nothing of this panel
         for (long long c = lo; c <= hi; ++c) {
           if (B.cta_begin[c] == B.cta_begin[c + 1]) continue;
-          sd += B.rowpart[(c + gp) * kPanelRows + t];
+          sd += B.rowpart[(c + gp) * PR + t];
         }
       }
       const long long o = I.row_off + i;
@@ -696,8 +718,9 @@ __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConf
 }
 
 // Batched evaluation, matrix part: per (CTA, instance) partials.
-template <int CK>
+template <int CK, int PR>
 __global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
+  constexpr int kBRPL = Tile<PR>::RPL;
   const BatchActive act = *B.act;
   if (act.count == 0 || act.error) return;
   const long long cta = blockIdx.x;
@@ -735,7 +758,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
     for (long long p = ql0 / I.n; p * I.n < ql1; ++p) {
       const long long jb = (ql0 > p * I.n ? ql0 : p * I.n) - p * I.n;
       const long long je = (ql1 < (p + 1) * I.n ? ql1 : (p + 1) * I.n) - p * I.n;
-      const long long row0 = p * kPanelRows;
+      const long long row0 = p * PR;
       double ur[kBRPL][kBR], uar[kBRPL][kBR];
       bool ok[kBRPL];
 #pragma unroll
@@ -886,6 +909,7 @@ __global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, Solve
 // units run panel-major, n units of 256 rows per full panel and n units of the
 // remaining rows in the last panel, so the start of a range follows in closed
 // form after a binary search over the instances' cost prefix.
+template <int PR>
 __global__ void kb_compact(BatchBuffers B, int grid) {
   __shared__ int flags[1024];
   __shared__ int base;
@@ -915,7 +939,7 @@ __global__ void kb_compact(BatchBuffers B, int grid) {
   }
   __syncthreads();
   long long units = 0, panels = 0, vblocks = 0, cost = 0;
-  const long long wu = (long long)B.unit_cost * kPanelRows;
+  const long long wu = (long long)B.unit_cost * kUnitCostRows;
   for (int off = 0; off < B.num; off += 1024) {
     const int k = off + threadIdx.x;
     flags[threadIdx.x] = (k < B.num && !B.st[k].done) ? 1 : 0;
@@ -972,8 +996,8 @@ __global__ void kb_compact(BatchBuffers B, int grid) {
       }
       const BatchInstance& I = B.inst[B.ids[lo]];
       const long long e = T - B.cost_prefix[lo];
-      const long long uf = 8 * kPanelRows + wu;                          // a unit of a full panel
-      const long long ul = 8 * (I.m - kPanelRows * (I.panels - 1)) + wu;  // a unit of the last panel
+      const long long uf = 8 * PR + wu;                          // a unit of a full panel
+      const long long ul = 8 * (I.m - PR * (I.panels - 1)) + wu;  // a unit of the last panel
       const long long F = I.n * uf;                                      // a full panel
       long long local;
       if (e < (I.panels - 1) * F) {
@@ -994,8 +1018,9 @@ __global__ void kb_compact(BatchBuffers B, int grid) {
 }
 
 // Per-instance cost norms (stage one, over the full unit line).
-template <int CK>
+template <int CK, int PR>
 __global__ void __launch_bounds__(kThreads, 2) kb_norms(BatchBuffers B) {
+  constexpr int kBRPL = Tile<PR>::RPL;
   const BatchActive act = *B.act;
   const long long cta = blockIdx.x;
   const long long q0 = B.cta_begin[cta], q1 = B.cta_begin[cta + 1];
@@ -1019,7 +1044,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_norms(BatchBuffers B) {
     for (long long p = ql0 / I.n; p * I.n < ql1; ++p) {
       const long long jb = (ql0 > p * I.n ? ql0 : p * I.n) - p * I.n;
       const long long je = (ql1 < (p + 1) * I.n ? ql1 : (p + 1) * I.n) - p * I.n;
-      const long long row0 = p * kPanelRows;
+      const long long row0 = p * PR;
       bool ok[kBRPL];
 #pragma unroll
       for (int kq = 0; kq < kBRPL; ++kq) ok[kq] = row0 + kq * 32 * kBR + lane * kBR < I.m;
@@ -1125,17 +1150,24 @@ __global__ void kb_convert_cost(const double* __restrict__ src, int64_t m, int64
   }
 }
 
-#define PDOT_BATCH_VARIANT(kind, KERNEL, LAUNCH)                                      \
-  do {                                                                                \
-    switch (kind) {                                                                   \
-      case PDOT_COST_F32: { auto kfn = KERNEL<PDOT_COST_F32>; LAUNCH; } break;        \
-      case pdot::kCostSqBase + 1: { auto kfn = KERNEL<pdot::kCostSqBase + 1>; LAUNCH; } break;    \
-      case pdot::kCostSqBase + 2: { auto kfn = KERNEL<pdot::kCostSqBase + 2>; LAUNCH; } break;    \
-      case pdot::kCostSqBase + 3: { auto kfn = KERNEL<pdot::kCostSqBase + 3>; LAUNCH; } break;    \
-      case pdot::kCostL1Base + 1: { auto kfn = KERNEL<pdot::kCostL1Base + 1>; LAUNCH; } break;    \
-      case pdot::kCostL1Base + 2: { auto kfn = KERNEL<pdot::kCostL1Base + 2>; LAUNCH; } break;    \
-      default: { auto kfn = KERNEL<pdot::kCostL1Base + 3>; LAUNCH; } break;                 \
-    }                                                                                 \
+#define PDOT_BATCH_KINDS(kind, KERNEL, PRV, LAUNCH)                                              \
+  switch (kind) {                                                                                 \
+    case PDOT_COST_F32: { auto kfn = KERNEL<PDOT_COST_F32, PRV>; LAUNCH; } break;                 \
+    case pdot::kCostSqBase + 1: { auto kfn = KERNEL<pdot::kCostSqBase + 1, PRV>; LAUNCH; } break; \
+    case pdot::kCostSqBase + 2: { auto kfn = KERNEL<pdot::kCostSqBase + 2, PRV>; LAUNCH; } break; \
+    case pdot::kCostSqBase + 3: { auto kfn = KERNEL<pdot::kCostSqBase + 3, PRV>; LAUNCH; } break; \
+    case pdot::kCostL1Base + 1: { auto kfn = KERNEL<pdot::kCostL1Base + 1, PRV>; LAUNCH; } break; \
+    case pdot::kCostL1Base + 2: { auto kfn = KERNEL<pdot::kCostL1Base + 2, PRV>; LAUNCH; } break; \
+    default: { auto kfn = KERNEL<pdot::kCostL1Base + 3, PRV>; LAUNCH; } break;                    \
+  }
+// a matrix-pass kernel for the cost kind and the tile's panel rows (128 or 256)
+#define PDOT_BATCH_VARIANT(kind, pr, KERNEL, LAUNCH)        \
+  do {                                                      \
+    if ((pr) == 128) {                                      \
+      PDOT_BATCH_KINDS(kind, KERNEL, 128, LAUNCH)           \
+    } else {                                                \
+      PDOT_BATCH_KINDS(kind, KERNEL, 256, LAUNCH)           \
+    }                                                       \
   } while (0)
 
 }  // namespace
@@ -1176,6 +1208,8 @@ class BatchSolver {
     dim_ = (pub_kind == PDOT_COST_SQEUCLID_POINTS || pub_kind == PDOT_COST_L1_POINTS) ? opt->point_dim : 0;
     kind_ = pdot::internal_cost_kind(pub_kind, dim_);
     use_graph_ = opt ? opt->use_cuda_graph != 0 : true;
+    pr_ = (opt && opt->batch_panel_rows) ? opt->batch_panel_rows : 256;
+    if (pr_ != 128 && pr_ != 256) bfail(PDOT_ERR_INVALID_ARGUMENT, "batch_panel_rows must be 0, 128 or 256");
     const int B = (int)P.num_instances;
     num_ = B;
     BCK(cudaSetDevice(device_));
@@ -1193,7 +1227,7 @@ class BatchSolver {
       I.col_off = co;
       I.pts_off = po;
       I.tpts_off = to;
-      I.panels = (I.m + pdot::kPanelRows - 1) / pdot::kPanelRows;
+      I.panels = (I.m + pr_ - 1) / pr_;
       I.rblocks = (I.m + pdot::kVecThreads - 1) / pdot::kVecThreads;
       I.cblocks = (I.n + pdot::kVecThreads - 1) / pdot::kVecThreads;
       xo += I.ld * I.n;
@@ -1218,14 +1252,14 @@ class BatchSolver {
     staged_ = pass == PDOT_PASS_STAGED || (pass == PDOT_PASS_AUTO && dim_ > 0);
     int occ = 1;
     if (staged_) {
-      PDOT_BATCH_VARIANT(kind_, pdot::kb_primal_staged, {
-        const int smem = staged_smem(kind_);
+      PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_primal_staged, {
+        const int smem = staged_smem(kind_, pr_);
         if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, pdot::kThreads, smem) != cudaSuccess || occ < 1)
           occ = 1;
       });
     } else {
-      PDOT_BATCH_VARIANT(kind_, pdot::kb_primal,
+      PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_primal,
                          if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, pdot::kThreads, 0) !=
                                  cudaSuccess ||
                              occ < 1) occ = 1);
@@ -1402,7 +1436,7 @@ class BatchSolver {
       wp_.eps = peps;
       recover_plans_ = true;
     }
-    D_.rowpart = alloc<double>(((size_t)grid_ + total_panels_) * pdot::kPanelRows);
+    D_.rowpart = alloc<double>(((size_t)grid_ + total_panels_) * pr_);
     D_.colpart = alloc<double>(total_units_);
     D_.sqpart = alloc<double>((size_t)grid_ + B);
     D_.steppart = alloc<double>((size_t)total_vblocks_ * pdot::kStepSums);
@@ -1536,9 +1570,9 @@ class BatchSolver {
     BCK(cudaMemsetAsync(D_.st, 0, num_ * sizeof(pdot::DevState), stream_));
     if (D_.winner) BCK(cudaMemsetAsync(D_.winner, 0x7F, num_ * sizeof(int), stream_));  // no winner yet
     BCK(cudaMemsetAsync(D_.rec, 0, num_ * sizeof(pdot_iteration_stats), stream_));
-    pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_, grid_);
+    launch_compact();
     BCK(cudaGetLastError());
-    PDOT_BATCH_VARIANT(kind_, pdot::kb_norms, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
+    PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_norms, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
     BCK(cudaGetLastError());
     pdot::kb_init_state<<<(num_ * 32 + 255) / 256, 256, 0, stream_>>>(D_, cfg_, grid_);
     BCK(cudaGetLastError());
@@ -1546,13 +1580,13 @@ class BatchSolver {
       wp_.st = D_.st;  // allocated after the recovery arguments were set up
       BCK(pdot::launch_warm_plan(wp_, plan_iters_, stream_));
     }
-    pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_, grid_);  // drops invalid problems
+    launch_compact();  // drops invalid problems
     BCK(cudaGetLastError());
     // warm instances start their restart information at the warm point, as
     // the reference starts it at its initial point (unless asked to start at
     // zero, kb_init_state's record)
     if (any_warm_ && !warm_zero_) {
-      PDOT_BATCH_VARIANT(kind_, pdot::kb_eval, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
+      PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_eval, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
       pdot::kb_eval_vec<<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_, 1);
       BCK(cudaGetLastError());
     }
@@ -1560,26 +1594,38 @@ class BatchSolver {
 
   bool is_eval(long long it) const { return (it - 1) % freq_ == 0 || it == limit_ + 1 || it <= 10; }
 
+  void launch_compact() {
+    if (pr_ == 128)
+      pdot::kb_compact<128><<<1, 1024, 0, stream_>>>(D_, grid_);
+    else
+      pdot::kb_compact<256><<<1, 1024, 0, stream_>>>(D_, grid_);
+  }
   void launch_eval() {
-    PDOT_BATCH_VARIANT(kind_, pdot::kb_eval, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
+    PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_eval, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
     pdot::kb_eval_vec<<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_, 0);
-    pdot::kb_compact<<<1, 1024, 0, stream_>>>(D_, grid_);
+    launch_compact();
     BCK(cudaGetLastError());
   }
-  static int staged_smem(int kind) {
+  static int staged_smem(int kind, int pr) {
     // the stored FP32 cost adds a plane to every stage; the coordinate costs do not
-    return kind == PDOT_COST_F32 ? pdot::BatchStagedLayout<PDOT_COST_F32>::kSmem
-                                 : pdot::BatchStagedLayout<pdot::kCostSqBase + 1>::kSmem;
+    if (pr == 128)
+      return kind == PDOT_COST_F32 ? pdot::BatchStagedLayout<PDOT_COST_F32, 128>::kSmem
+                                   : pdot::BatchStagedLayout<pdot::kCostSqBase + 1, 128>::kSmem;
+    return kind == PDOT_COST_F32 ? pdot::BatchStagedLayout<PDOT_COST_F32, 256>::kSmem
+                                 : pdot::BatchStagedLayout<pdot::kCostSqBase + 1, 256>::kSmem;
   }
 
   void launch_step() {
     if (staged_) {
-      const int smem = staged_smem(kind_);
-      PDOT_BATCH_VARIANT(kind_, pdot::kb_primal_staged, (kfn<<<grid_, pdot::kThreads, smem, stream_>>>(D_)));
+      const int smem = staged_smem(kind_, pr_);
+      PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_primal_staged, (kfn<<<grid_, pdot::kThreads, smem, stream_>>>(D_)));
     } else {
-      PDOT_BATCH_VARIANT(kind_, pdot::kb_primal, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
+      PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_primal, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
     }
-    pdot::kb_dual<<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_);
+    if (pr_ == 128)
+      pdot::kb_dual<128><<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_);
+    else
+      pdot::kb_dual<256><<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_);
     BCK(cudaGetLastError());
   }
 
@@ -1653,7 +1699,7 @@ class BatchSolver {
     if (tmp) BCK(cudaFree(tmp));
   }
 
-  int device_ = 0, num_ = 0, dim_ = 0, kind_ = 0, grid_ = 1;
+  int device_ = 0, num_ = 0, dim_ = 0, kind_ = 0, grid_ = 1, pr_ = 256;
   bool warm_zero_ = false;
   bool use_graph_ = true, any_warm_ = false, recover_plans_ = false, staged_ = false;
   int plan_iters_ = 0;
@@ -1697,6 +1743,9 @@ extern "C" int pdot_optimize_batched(const pdot_batch_problem* problem, const pd
     if (!points && !problem->cost_matrices) bfail(PDOT_ERR_INVALID_ARGUMENT, "null cost matrices");
     if (params->termination_evaluation_frequency < 1 || !(params->primal_importance > 0))
       bfail(PDOT_ERR_INVALID_ARGUMENT, "invalid parameters");
+    if (options && options->batch_panel_rows != 0 && options->batch_panel_rows != 128 &&
+        options->batch_panel_rows != 256)
+      bfail(PDOT_ERR_INVALID_ARGUMENT, "batch_panel_rows must be 0, 128 or 256");
     for (int64_t k = 0; k < problem->num_instances; ++k) {
       if (problem->num_rows[k] < 1 || problem->num_cols[k] < 1) bfail(PDOT_ERR_INVALID_ARGUMENT, "empty instance %lld", (long long)k);
       // the staged pass's producer cursor keeps positions inside an instance in 32 bits

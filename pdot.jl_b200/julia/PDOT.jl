@@ -265,6 +265,7 @@ struct CSolverOptions                           # pdot_solver_options
     warm_primal_weight::Float64
     batch_unit_cost::Float64
     persistent_chunks::Int32
+    batch_panel_rows::Int32
 end
 
 struct CBatchProblem                            # pdot_batch_problem
@@ -355,7 +356,7 @@ function solver_options(; device::Integer = 0, precision::Symbol = :f64, cost::U
     return CSolverOptions(Int32(device), Int32(1), Int32(0), PRECISIONS[precision], COSTS[c], Int32(point_dim),
                           source_points, target_points, 0.0, u0, v0, Int32(primal_pass), Int32(ctas_per_sm), X0,
                           eps, Int32(rounds), Int32(0), Int32(warm_restart_at_zero), Float64(warm_primal_weight), 0.0,
-                          Int32(0))
+                          Int32(0), Int32(0))
 end
 
 # points are given one per row (m x dim); the C ABI reads them row-major

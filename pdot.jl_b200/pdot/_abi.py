@@ -105,6 +105,7 @@ class SolverOptionsC(ct.Structure):
         ("warm_primal_weight", ct.c_double),
         ("batch_unit_cost", ct.c_double),
         ("persistent_chunks", ct.c_int32),
+        ("batch_panel_rows", ct.c_int32),
     ]
 
 

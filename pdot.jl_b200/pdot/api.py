@@ -557,7 +557,7 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
                      use_cuda_graph: bool = True, ctas_per_sm: int = 0, warm_starts=None,
                      return_primal: bool = True, recover_plan=None, race_groups=None,
                      primal_pass: str = "auto", warm_primal_weights=None, unit_cost: float = 0.25,
-                     warm_restart: str = "warm"):
+                     warm_restart: str = "warm", panel_rows: int = 256):
     """Solve many independent instances at once (pdot_optimize_batched).
 
     problems     a list of OptimalTransportProblem (cost_matrix may be None for
@@ -577,6 +577,10 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
     unit_cost    the matrix passes cut the active units into CTA ranges of
                  equal cost, a unit costing its rows + unit_cost * 256 (0..8,
                  in eighths); tune_batched picks it
+    panel_rows   the matrix passes' tile: a unit is one column of a panel of
+                 256 or 128 rows (128: fewer registers per thread, three
+                 resident CTAs per SM, twice the units of tall instances);
+                 tune_batched picks it
     return_primal  False leaves every primal_solution None (no m x n copies)
     Returns (outputs, seconds): a SaddlePointOutput per instance (its
     iteration_stats holds the final evaluation record) and the device time.
@@ -674,6 +678,7 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
         opts.point_dim = dim
     opts.ctas_per_sm = int(ctas_per_sm)
     opts.batch_unit_cost = float(unit_cost)
+    opts.batch_panel_rows = int(panel_rows)
     opts.primal_pass = {"auto": _abi.PASS_AUTO, "staged": _abi.PASS_STAGED, "direct": _abi.PASS_DIRECT}[primal_pass]
     cp = marshal_params(params)
     sec = ct.c_double(0.0)
@@ -688,19 +693,23 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
 
 
 BATCH_TUNING_CANDIDATES = [{"primal_pass": pp, "ctas_per_sm": c} for pp in ("staged", "direct") for c in (2, 1)]
+BATCH_TILE_SHAPES = ({"panel_rows": 128, "ctas_per_sm": 3}, {"panel_rows": 128, "ctas_per_sm": 2})
 BATCH_UNIT_COSTS = (0.0, 0.125, 0.25, 0.5, 8.0)
 
 
 def tune_batched(params: PdhgParameters, problems, *, cost: str = "f32", points=None, device: int = 0,
-                 iterations: int = 256, candidates=None, unit_costs=BATCH_UNIT_COSTS):
+                 iterations: int = 256, candidates=None, tile_shapes=BATCH_TILE_SHAPES,
+                 unit_costs=BATCH_UNIT_COSTS):
     """The batched solver's autotuner: times the first `iterations` iterations
     of the batch under candidate configurations and returns (best
     configuration, [(configuration, seconds)]); pass the configuration's keys
-    to optimize_batched. First the launch configuration (the primal pass,
-    staged by bulk copies or direct, times the resident CTAs per SM of the
-    matrix passes), then, for the best of those, the tile balance: the
-    per-unit overhead that the CTA split charges beside a unit's rows (0 cuts
-    ranges of equal rows, 8 nearly equal unit counts)."""
+    to optimize_batched. Three stages, each starting from the best so far:
+    the launch configuration (the primal pass, staged by bulk copies or
+    direct, times the resident CTAs per SM of the matrix passes) with
+    256-row tiles; the tile shape (128-row panels at three or two CTAs per
+    SM); the tile balance, the per-unit overhead that the CTA split charges
+    beside a unit's rows (0 cuts ranges of equal rows, 8 nearly equal unit
+    counts)."""
     import copy
 
     p = copy.deepcopy(params)
@@ -713,7 +722,10 @@ def tune_batched(params: PdhgParameters, problems, *, cost: str = "f32", points=
         timings.append((dict(cand), sec))
 
     for cand in candidates or BATCH_TUNING_CANDIDATES:
-        run({**cand, "unit_cost": 0.25})
+        run({"panel_rows": 256, **cand, "unit_cost": 0.25})
+    best = dict(min(timings, key=lambda t: t[1])[0])
+    for tile in tile_shapes:
+        run({**best, **tile})
     best = dict(min(timings, key=lambda t: t[1])[0])
     for uc in unit_costs:
         if uc != best["unit_cost"]:

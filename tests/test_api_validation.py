@@ -106,3 +106,12 @@ def test_persistent_chunks_flag_is_validated_before_device_work(built):
     assert api._options(0, True)[0].persistent_chunks == 0
     assert api._options(0, True, persistent=True)[0].persistent_chunks == 1
     assert api._options(0, True, persistent=False)[0].persistent_chunks == -1
+
+
+def test_batch_panel_rows_is_validated_before_device_work(built):
+    """The batched solver's tile takes panels of 128 or 256 rows (0: 256)."""
+    probs, pts = instances.batched_l1(count=2, lo=8, hi=16, seed=1)
+    with pytest.raises(_abi.PdotError) as ei:
+        pdot.optimize_batched(pdot.default_parameters(1e-4), probs, cost="l1", points=pts, panel_rows=192)
+    assert ei.value.code == _abi.PDOT_ERR_INVALID_ARGUMENT
+    assert "batch_panel_rows" in str(ei.value)

@@ -31,8 +31,9 @@ def fp64_kkt(C, a, b, X, u, v):
 SIZES = [(1, 1), (1, 17), (13, 1), (7, 5), (64, 64), (130, 77), (257, 300), (511, 129), (600, 601)]
 
 
-@pytest.mark.parametrize("cost", ["l1", "sqeuclid", "f32"])
-def test_batched_instances_solve_their_fp64_problems(cuda, cost):
+@pytest.mark.parametrize("cost, panel_rows", [("l1", 256), ("sqeuclid", 256), ("f32", 256), ("l1", 128),
+                                              ("f32", 128)])
+def test_batched_instances_solve_their_fp64_problems(cuda, cost, panel_rows):
     tol = 1e-4
     rng = np.random.default_rng(7)
     probs, pts, fp64 = [], [], []
@@ -45,7 +46,8 @@ def test_batched_instances_solve_their_fp64_problems(cuda, cost):
         probs.append(pdot.OptimalTransportProblem(C if cost == "f32" else None, a, b))
         pts.append((xs, ys))
     params = pdot.default_parameters(tol)
-    outs, seconds = pdot.optimize_batched(params, probs, cost=cost, points=None if cost == "f32" else pts)
+    outs, seconds = pdot.optimize_batched(params, probs, cost=cost, points=None if cost == "f32" else pts,
+                                          panel_rows=panel_rows)
     assert seconds > 0
     for (m, n), o, p64 in zip(SIZES, outs, fp64):
         assert o.termination_reason == OPTIMAL, (m, n, o.termination_string)
@@ -57,9 +59,11 @@ def test_batched_instances_solve_their_fp64_problems(cuda, cost):
         assert abs(pobj - ref_obj) <= 2 * tol * (1 + abs(ref_obj)), (m, n)
 
 
-def test_batched_matches_single_instance_mixed_precision_early(cuda):
+@pytest.mark.parametrize("panel_rows", [256, 128])
+def test_batched_matches_single_instance_mixed_precision_early(cuda, panel_rows):
     """Same arithmetic per entry as the single-instance FP32 solve of one
-    instance: the first evaluations agree to rounding of the sums."""
+    instance, with either tile: the first evaluations agree to rounding of the
+    sums."""
     rng = np.random.default_rng(3)
     m, n = 300, 200
     xs, ys = rng.uniform(0, 1, (m, 2)).astype(np.float32), rng.uniform(0, 1, (n, 2)).astype(np.float32)
@@ -67,7 +71,7 @@ def test_batched_matches_single_instance_mixed_precision_early(cuda):
     prob = pdot.OptimalTransportProblem(None, a, b)
     params = pdot.default_parameters(1e-4, iteration_limit=9)
     single = pdot.optimize(params, prob, precision="f32", cost="l1", points=(xs, ys))
-    outs, _ = pdot.optimize_batched(params, [prob], cost="l1", points=[(xs, ys)])
+    outs, _ = pdot.optimize_batched(params, [prob], cost="l1", points=[(xs, ys)], panel_rows=panel_rows)
     assert outs[0].iteration_count == single.iteration_count
     cs = single.iteration_stats[-1].convergence_information[0]
     cb = outs[0].iteration_stats[-1].convergence_information[0]
@@ -88,28 +92,30 @@ def test_batched_invalid_instance_does_not_stop_the_others(cuda):
     assert outs[0].termination_reason == OPTIMAL and outs[2].termination_reason == OPTIMAL
 
 
-def test_batched_is_deterministic(cuda):
+@pytest.mark.parametrize("panel_rows", [256, 128])
+def test_batched_is_deterministic(cuda, panel_rows):
     probs, pts = instances.batched_l1(count=24, lo=16, hi=300, seed=5)
     params = pdot.default_parameters(1e-4)
-    o1, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts)
-    o2, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts)
+    o1, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts, panel_rows=panel_rows)
+    o2, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts, panel_rows=panel_rows)
     for x, y in zip(o1, o2):
         assert x.iteration_count == y.iteration_count
         assert np.array_equal(x.primal_solution, y.primal_solution)
 
 
-@pytest.mark.parametrize("cost", ["l1", "f32"])
-def test_batched_staged_and_direct_passes_agree(cuda, cost):
+@pytest.mark.parametrize("cost, panel_rows", [("l1", 256), ("f32", 256), ("l1", 128), ("f32", 128)])
+def test_batched_staged_and_direct_passes_agree(cuda, cost, panel_rows):
     """The bulk-copy staged pass and the direct pass do the same arithmetic in
-    the same order over the same CTA partition (two CTAs per SM each), so the
-    solves agree bit for bit. Sizes include partial panels and rows that are
-    not a multiple of 4."""
+    the same order over the same CTA partition (the same tile, the same CTAs
+    per SM), so the solves agree bit for bit. Sizes include partial panels and
+    rows that are not a multiple of 4."""
     probs, pts = instances.batched_l1(count=20, lo=3, hi=700, seed=9)
     if cost == "f32":
         probs = [pdot.OptimalTransportProblem(instances.l1_cost(*pt), p.source_distribution, p.target_distribution)
                  for p, pt in zip(probs, pts)]
     params = pdot.default_parameters(1e-4)
     kw = {} if cost == "f32" else {"points": pts}
+    kw.update(panel_rows=panel_rows, ctas_per_sm=3 if panel_rows == 128 else 2)
     st, _ = pdot.optimize_batched(params, probs, cost=cost, primal_pass="staged", **kw)
     di, _ = pdot.optimize_batched(params, probs, cost=cost, primal_pass="direct", **kw)
     for x, y in zip(st, di):
@@ -119,9 +125,10 @@ def test_batched_staged_and_direct_passes_agree(cuda, cost):
         assert np.array_equal(x.dual_source_solution, y.dual_source_solution)
 
 
+@pytest.mark.parametrize("panel_rows", [256, 128])
 @pytest.mark.parametrize("sizes", [[(65, 40), (3, 5), (300, 200)], [(257, 70), (700, 650), (128, 3)],
-                                   [(3, 40), (300, 200)], [(65, 40), (300, 5)]])
-def test_batched_small_instances_both_pass_forms(cuda, sizes):
+                                   [(3, 40), (300, 200)], [(65, 40), (300, 5)], [(129, 7), (127, 300), (385, 2)]])
+def test_batched_small_instances_both_pass_forms(cuda, sizes, panel_rows):
     """Batches with a few rows or a few columns (fewer columns than warps, a
     single 8-row padded panel) beside larger instances, with point costs: the
     staged pass's copies and waits cover every unit (no bounded wait gives up)
@@ -133,8 +140,9 @@ def test_batched_small_instances_both_pass_forms(cuda, sizes):
         probs.append(pdot.OptimalTransportProblem(None, rng.dirichlet(np.ones(m)), rng.dirichlet(np.ones(n))))
         pts.append((xs, ys))
     params = pdot.default_parameters(1e-4, iteration_limit=3000)
-    st, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts, primal_pass="staged")
-    di, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts, primal_pass="direct")
+    kw = dict(panel_rows=panel_rows, ctas_per_sm=3 if panel_rows == 128 else 2)
+    st, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts, primal_pass="staged", **kw)
+    di, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts, primal_pass="direct", **kw)
     for x, y in zip(st, di):
         assert x.iteration_count == y.iteration_count
         assert np.array_equal(x.primal_solution, y.primal_solution)
@@ -144,9 +152,11 @@ def test_batched_small_instances_both_pass_forms(cuda, sizes):
 def test_autotuner_times_every_candidate_and_picks_the_fastest(cuda):
     probs, pts = instances.batched_l1(count=12, lo=32, hi=400, seed=2)
     best, timings = pdot.tune_batched(pdot.default_parameters(1e-4), probs, cost="l1", points=pts, iterations=64)
-    # the launch configurations at the default balance, then the other balances for the best of them
+    # the launch configurations with 256-row tiles at the default balance, the
+    # 128-row tiles for the best of them, then the other balances for the best
     others = [c for c in pdot.api.BATCH_UNIT_COSTS if c != 0.25]
-    assert len(timings) == len(pdot.api.BATCH_TUNING_CANDIDATES) + len(others)
+    assert len(timings) == len(pdot.api.BATCH_TUNING_CANDIDATES) + len(pdot.api.BATCH_TILE_SHAPES) + len(others)
+    assert {t[0]["panel_rows"] for t in timings} == {128, 256}
     assert best == min(timings, key=lambda t: t[1])[0]
     outs, _ = pdot.optimize_batched(pdot.default_parameters(1e-4), probs, cost="l1", points=pts, **best)
     assert all(o.termination_reason == OPTIMAL for o in outs)

@@ -191,6 +191,7 @@ __global__ void __launch_bounds__(kThreads, Tile<PR>::kMinBlocks) kb_primal(Batc
   constexpr int kBRPL = Tile<PR>::RPL;
   __shared__ double red[kWarps][PR];
   __shared__ double sqw[kWarps];
+  pdl_enter();
   const BatchActive act = *B.act;
   if (act.count == 0 || act.error) return;
   const long long cta = blockIdx.x;
@@ -430,6 +431,7 @@ __global__ void __launch_bounds__(kThreads, Tile<PR>::kMinBlocks) kb_primal_stag
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ double red[kWarps][PR];
   __shared__ double sqw[kWarps];
+  pdl_enter();
   const BatchActive act = *B.act;
   if (act.count == 0 || act.error) return;
   const long long cta = blockIdx.x;
@@ -640,6 +642,7 @@ __global__ void __launch_bounds__(kThreads, Tile<PR>::kMinBlocks) kb_primal_stag
 // Batched dual step + per-instance step control (last CTA of each instance).
 template <int PR>
 __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConfig cfg, int grid) {
+  pdl_enter();
   const BatchActive act = *B.act;
   if (act.count == 0 || act.error) return;
   const long long blk = blockIdx.x;
@@ -721,6 +724,7 @@ __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConf
 template <int CK, int PR>
 __global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
   constexpr int kBRPL = Tile<PR>::RPL;
+  pdl_enter();
   const BatchActive act = *B.act;
   if (act.count == 0 || act.error) return;
   const long long cta = blockIdx.x;
@@ -826,6 +830,7 @@ __global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
 // instance takes any other step of the evaluation block.
 __global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, SolveConfig cfg, int grid,
                                                             int start_only) {
+  pdl_enter();
   const BatchActive act = *B.act;
   if (act.count == 0 || act.error) return;
   const long long blk = blockIdx.x;
@@ -915,6 +920,7 @@ __global__ void kb_compact(BatchBuffers B, int grid) {
   __shared__ int base;
   __shared__ long long total_cost;
   __shared__ int empty_flag;
+  pdl_enter();
   if (threadIdx.x == 0) {
     base = 0;
     empty_flag = 0;
@@ -1594,17 +1600,17 @@ class BatchSolver {
 
   bool is_eval(long long it) const { return (it - 1) % freq_ == 0 || it == limit_ + 1 || it <= 10; }
 
+  // the loop's kernels are launched with programmatic dependent launch (pdot::pdl_launch)
   void launch_compact() {
-    if (pr_ == 128)
-      pdot::kb_compact<128><<<1, 1024, 0, stream_>>>(D_, grid_);
-    else
-      pdot::kb_compact<256><<<1, 1024, 0, stream_>>>(D_, grid_);
+    BCK(pdot::pdl_launch(pr_ == 128 ? pdot::kb_compact<128> : pdot::kb_compact<256>, dim3(1), dim3(1024), 0, stream_,
+                         D_, grid_));
   }
   void launch_eval() {
-    PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_eval, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
-    pdot::kb_eval_vec<<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_, 0);
+    PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_eval,
+                       BCK(pdot::pdl_launch(kfn, dim3(grid_), dim3(pdot::kThreads), 0, stream_, D_)));
+    BCK(pdot::pdl_launch(pdot::kb_eval_vec, dim3((unsigned)total_vblocks_), dim3(pdot::kVecThreads), 0, stream_, D_,
+                         cfg_, grid_, 0));
     launch_compact();
-    BCK(cudaGetLastError());
   }
   static int staged_smem(int kind, int pr) {
     // the stored FP32 cost adds a plane to every stage; the coordinate costs do not
@@ -1618,15 +1624,14 @@ class BatchSolver {
   void launch_step() {
     if (staged_) {
       const int smem = staged_smem(kind_, pr_);
-      PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_primal_staged, (kfn<<<grid_, pdot::kThreads, smem, stream_>>>(D_)));
+      PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_primal_staged,
+                         BCK(pdot::pdl_launch(kfn, dim3(grid_), dim3(pdot::kThreads), smem, stream_, D_)));
     } else {
-      PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_primal, (kfn<<<grid_, pdot::kThreads, 0, stream_>>>(D_)));
+      PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_primal,
+                         BCK(pdot::pdl_launch(kfn, dim3(grid_), dim3(pdot::kThreads), 0, stream_, D_)));
     }
-    if (pr_ == 128)
-      pdot::kb_dual<128><<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_);
-    else
-      pdot::kb_dual<256><<<(unsigned)total_vblocks_, pdot::kVecThreads, 0, stream_>>>(D_, cfg_, grid_);
-    BCK(cudaGetLastError());
+    BCK(pdot::pdl_launch(pr_ == 128 ? pdot::kb_dual<128> : pdot::kb_dual<256>, dim3((unsigned)total_vblocks_),
+                         dim3(pdot::kVecThreads), 0, stream_, D_, cfg_, grid_));
   }
 
   bool regular_start(long long it) const {

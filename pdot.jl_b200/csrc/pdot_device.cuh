@@ -9,6 +9,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cuda_bf16.h>
+#include <utility>
 
 #include "pdot_common.cuh"
 
@@ -453,6 +454,43 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity,
     }
   }
   return false;
+}
+
+// Programmatic dependent launch. The kernels of the iteration loop are
+// launched with programmatic stream serialization (pdl_launch): the next
+// kernel in the stream may be scheduled before this one ends, and its CTAs
+// then block in griddepcontrol.wait until this grid has completed and its
+// writes are visible. Every such kernel calls pdl_wait() before it touches
+// global memory (reads of the previous kernel's results and writes of the
+// buffers it reads alike), then pdl_trigger() so that the kernel after it may
+// be scheduled while it runs. Both are no-ops in a kernel launched without
+// the attribute. The time saved is the launch and ramp of each kernel, which
+// is most of an iteration's time on small problems.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_enter() {
+  pdl_wait();
+  pdl_trigger();
+}
+
+// Build knob: PDOT_PDL 0 launches the loop's kernels without the attribute.
+#ifndef PDOT_PDL
+#define PDOT_PDL 1
+#endif
+template <typename... P, typename... A>
+inline cudaError_t pdl_launch(void (*kfn)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              A&&... args) {
+  cudaLaunchConfig_t c = {};
+  c.gridDim = grid;
+  c.blockDim = block;
+  c.dynamicSmemBytes = smem;
+  c.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  c.attrs = at;
+  c.numAttrs = PDOT_PDL ? 1 : 0;
+  return cudaLaunchKernelEx(&c, kfn, std::forward<A>(args)...);
 }
 
 // Grid-wide barrier of a persistent launch whose CTAs are all co-resident (a

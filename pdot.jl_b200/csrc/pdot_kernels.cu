@@ -191,11 +191,13 @@ __device__ __forceinline__ void k1_primal_impl(const Buffers& B, const Geometry&
 
 template <typename TX, int CK, int R>
 __global__ void __launch_bounds__(kThreads, 2) k1_primal(Buffers B, Geometry g) {
+  pdl_enter();
   k1_primal_impl<TX, CK, R, false>(B, g, blockIdx.x);
 }
 // the same pass before an evaluation: it also leaves the evaluation's plan sums
 template <typename TX, int CK, int R>
 __global__ void __launch_bounds__(kThreads, 2) k1_primal_xs(Buffers B, Geometry g) {
+  pdl_enter();
   k1_primal_impl<TX, CK, R, true>(B, g, blockIdx.x);
 }
 
@@ -424,6 +426,7 @@ __device__ __forceinline__ void k1_primal_staged_impl(const Buffers& B, const Ge
 // reads it would save the evaluation (8 B per entry with an FP32 plan).
 template <typename TX, int CK>
 __global__ void __launch_bounds__(kThreads, 2) k1_primal_staged(Buffers B, Geometry g) {
+  pdl_enter();
   k1_primal_staged_impl<TX, CK>(B, g);
 }
 
@@ -531,6 +534,7 @@ __device__ __forceinline__ void k2_dual_body(const Buffers& B, const Geometry& g
 }
 
 __global__ void __launch_bounds__(kVecThreads) k2_dual(Buffers B, Geometry g, SolveConfig cfg) {
+  pdl_enter();
   k2_dual_body(B, g, cfg, blockIdx.x, gridDim.x);
 }
 
@@ -658,6 +662,7 @@ __device__ __forceinline__ void k3_eval_body(const Buffers& B, const Geometry& g
 
 template <typename TX, int CK, int R>
 __global__ void __launch_bounds__(kThreads, 2) k3_eval(Buffers B, Geometry g) {
+  pdl_enter();
   k3_eval_body<TX, CK, R>(B, g, blockIdx.x);
 }
 
@@ -735,6 +740,7 @@ __device__ __forceinline__ void k4_eval_body(const Buffers& B, const Geometry& g
 }
 
 __global__ void __launch_bounds__(kVecThreads) k4_eval(Buffers B, Geometry g, SolveConfig cfg, int start_only) {
+  pdl_enter();
   k4_eval_body(B, g, cfg, start_only, blockIdx.x, gridDim.x);
 }
 
@@ -1122,19 +1128,22 @@ cudaError_t launch_init(const Buffers& B, const Geometry& g, const SolveConfig& 
   return cudaGetLastError();
 }
 
+// The loop's kernels are launched with programmatic dependent launch (pdl_launch).
 cudaError_t launch_primal(const Buffers& B, const Geometry& g, cudaStream_t s, int xsums) {
+  cudaError_t e = cudaSuccess;
   if (g.tma)
-    PDOT_STAGED_VARIANT(g, k1_primal_staged, (kfn<<<g.grid, kThreads, smem, s>>>(B, g)));
+    PDOT_STAGED_VARIANT(g, k1_primal_staged, (e = pdl_launch(kfn, dim3((unsigned)g.grid), dim3(kThreads), smem, s, B, g)));
   else if (xsums)
-    PDOT_VARIANT(g, k1_primal_xs, (kfn<<<g.grid, kThreads, 0, s>>>(B, g)));
+    PDOT_VARIANT(g, k1_primal_xs, (e = pdl_launch(kfn, dim3((unsigned)g.grid), dim3(kThreads), 0, s, B, g)));
   else
-    PDOT_VARIANT(g, k1_primal, (kfn<<<g.grid, kThreads, 0, s>>>(B, g)));
-  return cudaGetLastError();
+    PDOT_VARIANT(g, k1_primal, (e = pdl_launch(kfn, dim3((unsigned)g.grid), dim3(kThreads), 0, s, B, g)));
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t launch_dual(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s) {
-  k2_dual<<<g.dual_row_blocks + g.col_blocks, kVecThreads, 0, s>>>(B, g, cfg);
-  return cudaGetLastError();
+  const cudaError_t e =
+      pdl_launch(k2_dual, dim3((unsigned)(g.dual_row_blocks + g.col_blocks)), dim3(kVecThreads), 0, s, B, g, cfg);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t launch_step(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s, int xsums) {
@@ -1158,9 +1167,12 @@ cudaError_t launch_chunk(const Buffers& B, const Geometry& g, const SolveConfig&
 
 cudaError_t launch_eval(const Buffers& B, const Geometry& g, const SolveConfig& cfg, cudaStream_t s,
                         int start_only) {
-  PDOT_VARIANT(g, k3_eval, (kfn<<<g.grid, kThreads, 0, s>>>(B, g)));
-  k4_eval<<<g.row_blocks + g.col_blocks, kVecThreads, 0, s>>>(B, g, cfg, start_only);
-  return cudaGetLastError();
+  cudaError_t e = cudaSuccess;
+  PDOT_VARIANT(g, k3_eval, (e = pdl_launch(kfn, dim3((unsigned)g.grid), dim3(kThreads), 0, s, B, g)));
+  if (e != cudaSuccess) return e;
+  e = pdl_launch(k4_eval, dim3((unsigned)(g.row_blocks + g.col_blocks)), dim3(kVecThreads), 0, s, B, g, cfg,
+                 start_only);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t launch_primal_pass(const Geometry& g, const double* C, double* X, double* Xa, const double* u,

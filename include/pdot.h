@@ -184,7 +184,10 @@ typedef struct pdot_solver_options {
    * one) as one persistent cooperative launch with grid barriers between the
    * phases, instead of a CUDA graph of separate launches; the results are
    * bit-identical. 0: automatic (the CUDA graph, which measured faster on
-   * B200), 1: whenever the direct 16-byte pass runs, -1: never. */
+   * B200), 1: whenever the direct 16-byte pass runs, -1: never. The batched
+   * solver takes it too: 1 runs its regular chunks (evaluation, compaction,
+   * steps) as one persistent launch with the direct pass throughout (the
+   * staged pass is then refused). */
   int32_t persistent_chunks;
   /* Batched solver: the rows of one panel of its matrix passes' tiles (a unit
    * is one column of one panel): 256 or 128, 0 = 256. A 128-row tile holds

@@ -77,6 +77,8 @@ struct BatchActive {
   int any_empty;          // some CTA range holds no unit (only in the tail of a solve)
   long long total_units;
   int error;              // a bounded wait gave up: every later launch returns at once
+  unsigned int bar_count; // grid barrier of the persistent chunk: arrivals
+  unsigned int bar_gen;   // and generation
   int pad_;
 };
 
@@ -129,12 +131,40 @@ __device__ __forceinline__ long long bcta_of_unit(const long long* cta_begin, in
   }
   return lo;
 }
+// Loads of data that another CTA may have written earlier in the same launch
+// (CO: the persistent chunk, where the dual step, the compaction and the
+// primal pass are phases of one launch) go through L2 (ld.global.cg); the
+// per-launch kernels read them through the read-only path.
+template <bool CO, typename T>
+__device__ __forceinline__ T ldro(const T* p) {
+  if constexpr (CO)
+    return __ldcg(p);
+  else
+    return __ldg(p);
+}
+template <bool CO, typename T, int R>
+__device__ __forceinline__ void vldro(const T* p, T (&v)[R]) {
+  if constexpr (CO)
+    vldcg<T, R>(p, v);
+  else
+    vldg<T, R>(p, v);
+}
+// the plan, which the pass also writes: a plain load, or through L2
+template <bool CO, typename T, int R>
+__device__ __forceinline__ void vldx(const T* p, T (&v)[R]) {
+  if constexpr (CO)
+    vldcg<T, R>(p, v);
+  else
+    vld<T, R>(p, v);
+}
+
 // largest k in [0, count) with prefix[k] <= q
+template <bool CO = false>
 __device__ __forceinline__ int find_segment(const long long* prefix, int count, long long q) {
   int lo = 0, hi = count - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(prefix + mid) <= q)
+    if (ldro<CO>(prefix + mid) <= q)
       lo = mid;
     else
       hi = mid - 1;
@@ -186,19 +216,19 @@ __device__ __forceinline__ void sum_cta_slots(const double* part, const long lon
 
 // ---------------------------------------------------------------------------
 // Batched fused primal pass (FP32 plan): the per-entry step of pdot_kernels.cu.
-template <int CK, int PR>
-__global__ void __launch_bounds__(kThreads, Tile<PR>::kMinBlocks) kb_primal(BatchBuffers B) {
+// The body of CTA range `cta` (a kernel's CTA, or a virtual CTA of the
+// persistent chunk).
+template <int CK, int PR, bool CO>
+__device__ __forceinline__ void kb_primal_body(const BatchBuffers& B, const long long cta) {
   constexpr int kBRPL = Tile<PR>::RPL;
   __shared__ double red[kWarps][PR];
   __shared__ double sqw[kWarps];
-  pdl_enter();
   const BatchActive act = *B.act;
   if (act.count == 0 || act.error) return;
-  const long long cta = blockIdx.x;
   const long long q0 = B.cta_begin[cta], q1 = B.cta_begin[cta + 1];
   if (q0 >= q1) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int kk = find_segment(B.unit_prefix, act.count, q0);
+  int kk = find_segment<CO>(B.unit_prefix, act.count, q0);
   long long q = q0;
   while (q < q1) {
     const int k = B.ids[kk];
@@ -243,7 +273,7 @@ __global__ void __launch_bounds__(kThreads, Tile<PR>::kMinBlocks) kb_primal(Batc
 #pragma unroll
         for (int e = 0; e < kBR; ++e) {
           acc[kq][e] = 0.0;
-          ur[kq][e] = (ok[kq] && i + e < I.m && !zero_g) ? (float)__ldg(u + i + e) : 0.0f;
+          ur[kq][e] = (ok[kq] && i + e < I.m && !zero_g) ? (float)ldro<CO>(u + i + e) : 0.0f;
         }
       }
       cost.panel(row0, lane, I.m, ok);
@@ -258,7 +288,7 @@ __global__ void __launch_bounds__(kThreads, Tile<PR>::kMinBlocks) kb_primal(Batc
         for (int ju = 0; ju < kJU; ++ju) {
           const long long jj = j + ju * kWarps;
           if (jj >= je) continue;
-          vj[ju] = zero_g ? 0.0f : (float)__ldg(v + jj);
+          vj[ju] = zero_g ? 0.0f : (float)ldro<CO>(v + jj);
           cost.column(jj);
           const long long col = jj * I.ld + row0 + lane * kBR;
 #pragma unroll
@@ -266,8 +296,8 @@ __global__ void __launch_bounds__(kThreads, Tile<PR>::kMinBlocks) kb_primal(Batc
             if (ok[kq]) {
               const long long idx = col + kq * 32 * kBR;
               cost.get(idx, kq, cv[ju][kq]);
-              vld<float, kBR>(X + idx, xv[ju][kq]);
-              if (!first) vld<float, kBR>(Xa + idx, av[ju][kq]);
+              vldx<CO>(X + idx, xv[ju][kq]);
+              if (!first) vldx<CO>(Xa + idx, av[ju][kq]);
             }
           }
         }
@@ -333,6 +363,12 @@ __global__ void __launch_bounds__(kThreads, Tile<PR>::kMinBlocks) kb_primal(Batc
     q = seg_end;
     ++kk;
   }
+}
+
+template <int CK, int PR>
+__global__ void __launch_bounds__(kThreads, Tile<PR>::kMinBlocks) kb_primal(BatchBuffers B) {
+  pdl_enter();
+  kb_primal_body<CK, PR, false>(B, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -640,14 +676,13 @@ __global__ void __launch_bounds__(kThreads, Tile<PR>::kMinBlocks) kb_primal_stag
 }
 
 // Batched dual step + per-instance step control (last CTA of each instance).
-template <int PR>
-__global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConfig cfg, int grid) {
-  pdl_enter();
+template <int PR, bool CO>
+__device__ __forceinline__ void kb_dual_body(const BatchBuffers& B, const SolveConfig& cfg, const int grid,
+                                             const long long blk) {
   const BatchActive act = *B.act;
   if (act.count == 0 || act.error) return;
-  const long long blk = blockIdx.x;
   if (blk >= B.vblock_prefix[act.count]) return;
-  const int kk = find_segment(B.vblock_prefix, act.count, blk);
+  const int kk = find_segment<CO>(B.vblock_prefix, act.count, blk);
   const int k = B.ids[kk];
   const BatchInstance I = B.inst[k];
   DevState* st = B.st + k;
@@ -719,25 +754,28 @@ __global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConf
     st->ticket_step = 0;
   }
 }
+template <int PR>
+__global__ void __launch_bounds__(kVecThreads) kb_dual(BatchBuffers B, SolveConfig cfg, int grid) {
+  pdl_enter();
+  kb_dual_body<PR, false>(B, cfg, grid, blockIdx.x);
+}
 
 // Batched evaluation, matrix part: per (CTA, instance) partials.
-template <int CK, int PR>
-__global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
+template <int CK, int PR, bool CO>
+__device__ __forceinline__ void kb_eval_body(const BatchBuffers& B, const long long cta, const int grid) {
   constexpr int kBRPL = Tile<PR>::RPL;
-  pdl_enter();
   const BatchActive act = *B.act;
   if (act.count == 0 || act.error) return;
-  const long long cta = blockIdx.x;
   const long long q0 = B.cta_begin[cta], q1 = B.cta_begin[cta + 1];
   if (q0 >= q1) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int kk = find_segment(B.unit_prefix, act.count, q0);
+  int kk = find_segment<CO>(B.unit_prefix, act.count, q0);
   long long q = q0;
   while (q < q1) {
     const int k = B.ids[kk];
     const BatchInstance I = B.inst[k];
     DevState* st = B.st + k;
-    if (cta == bcta_of_unit(B.cta_begin, (int)gridDim.x, B.unit_prefix[kk]) && threadIdx.x == 0) st->eval_t0_ns = globaltimer_ns();
+    if (cta == bcta_of_unit(B.cta_begin, grid, B.unit_prefix[kk]) && threadIdx.x == 0) st->eval_t0_ns = globaltimer_ns();
     const long long base_u = B.unit_prefix[kk];
     const long long seg_end = min(q1, (long long)B.unit_prefix[kk + 1]);
     const int buf = st->buf;
@@ -772,14 +810,14 @@ __global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
 #pragma unroll
         for (int e = 0; e < kBR; ++e) {
           const bool in = ok[kq] && i + e < I.m;
-          ur[kq][e] = in ? __ldg(u + i + e) : 0.0;
-          uar[kq][e] = (in && have_avg) ? __ldg(ua + i + e) : 0.0;
+          ur[kq][e] = in ? ldro<CO>(u + i + e) : 0.0;
+          uar[kq][e] = (in && have_avg) ? ldro<CO>(ua + i + e) : 0.0;
         }
       }
       cost.panel(row0, lane, I.m, ok);
       for (long long j = jb + warp; j < je; j += kWarps) {
-        const double vj = __ldg(v + j);
-        const double vaj = have_avg ? __ldg(va + j) : 0.0;
+        const double vj = ldro<CO>(v + j);
+        const double vaj = have_avg ? ldro<CO>(va + j) : 0.0;
         cost.column(j);
         const long long col = j * I.ld + row0 + lane * kBR;
 #pragma unroll
@@ -790,8 +828,8 @@ __global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
           typename CostReader<CK, kBR, kBRPL>::value_t cv[kBR];
           float xv[kBR], av[kBR];
           cost.get(idx, kq, cv);
-          vldg<float, kBR>(X + idx, xv);
-          if (have_avg) vldg<float, kBR>(Xa + idx, av);
+          vldro<CO>(X + idx, xv);
+          if (have_avg) vldro<CO>(Xa + idx, av);
 #pragma unroll
           for (int e = 0; e < kBR; ++e) {
             if (i + e >= I.m) continue;
@@ -822,20 +860,24 @@ __global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
     ++kk;
   }
 }
+template <int CK, int PR>
+__global__ void __launch_bounds__(kThreads, 2) kb_eval(BatchBuffers B) {
+  pdl_enter();
+  kb_eval_body<CK, PR, false>(B, blockIdx.x, (int)gridDim.x);
+}
 
 // Batched evaluation, vector part + per-instance evaluation control.
 // start_only: the evaluation of the initial points, run once after
 // kb_init_state when some instance starts warm; the warm instances record
 // their start point as the last restart point (record_start_point) and no
 // instance takes any other step of the evaluation block.
-__global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, SolveConfig cfg, int grid,
-                                                            int start_only) {
-  pdl_enter();
+template <bool CO>
+__device__ __forceinline__ void kb_eval_vec_body(const BatchBuffers& B, const SolveConfig& cfg, const int grid,
+                                                 const int start_only, const long long blk) {
   const BatchActive act = *B.act;
   if (act.count == 0 || act.error) return;
-  const long long blk = blockIdx.x;
   if (blk >= B.vblock_prefix[act.count]) return;
-  const int kk = find_segment(B.vblock_prefix, act.count, blk);
+  const int kk = find_segment<CO>(B.vblock_prefix, act.count, blk);
   const int k = B.ids[kk];
   const BatchInstance I = B.inst[k];
   DevState* st = B.st + k;
@@ -906,6 +948,11 @@ __global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, Solve
     st->ticket_eval = 0;
   }
 }
+__global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, SolveConfig cfg, int grid,
+                                                            int start_only) {
+  pdl_enter();
+  kb_eval_vec_body<false>(B, cfg, grid, start_only, blockIdx.x);
+}
 
 // Rebuild the active list and its prefix sums (one CTA, instances in order),
 // then the CTA ranges: CTA c starts at the first active unit whose cumulative
@@ -914,13 +961,15 @@ __global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, Solve
 // units run panel-major, n units of 256 rows per full panel and n units of the
 // remaining rows in the last panel, so the start of a range follows in closed
 // form after a binary search over the instances' cost prefix.
+// One CTA of blockDim.x <= 1024 threads runs it (the kernel: 1024; the
+// persistent chunk: CTA 0 with its 256).
 template <int PR>
-__global__ void kb_compact(BatchBuffers B, int grid) {
+__device__ __forceinline__ void kb_compact_body(const BatchBuffers& B, const int grid) {
   __shared__ int flags[1024];
   __shared__ int base;
   __shared__ long long total_cost;
   __shared__ int empty_flag;
-  pdl_enter();
+  const int T = (int)blockDim.x;
   if (threadIdx.x == 0) {
     base = 0;
     empty_flag = 0;
@@ -946,13 +995,13 @@ __global__ void kb_compact(BatchBuffers B, int grid) {
   __syncthreads();
   long long units = 0, panels = 0, vblocks = 0, cost = 0;
   const long long wu = (long long)B.unit_cost * kUnitCostRows;
-  for (int off = 0; off < B.num; off += 1024) {
+  for (int off = 0; off < B.num; off += T) {
     const int k = off + threadIdx.x;
     flags[threadIdx.x] = (k < B.num && !B.st[k].done) ? 1 : 0;
     __syncthreads();
     if (threadIdx.x == 0) {
       int c = base;
-      for (int t = 0; t < 1024 && off + t < B.num; ++t) {
+      for (int t = 0; t < T && off + t < B.num; ++t) {
         if (!flags[t]) continue;
         const int kk = off + t;
         const BatchInstance& I = B.inst[kk];
@@ -1021,6 +1070,63 @@ __global__ void kb_compact(BatchBuffers B, int grid) {
     if (B.cta_begin[c] == B.cta_begin[c + 1]) empty_flag = 1;
   __syncthreads();
   if (threadIdx.x == 0) B.act->any_empty = empty_flag;
+}
+template <int PR>
+__global__ void kb_compact(BatchBuffers B, int grid) {
+  pdl_enter();
+  kb_compact_body<PR>(B, grid);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent chunk: one cooperative launch runs a regular chunk of loop bodies
+// of the whole batch (the evaluation, the compaction, then `steps` iterations
+// of primal pass and dual step) with grid barriers between the phases instead
+// of kernel boundaries. Every phase runs the body of its kernel over the same
+// virtual CTAs (physical CTA b takes the CTA ranges b, b + gridDim.x, ... of
+// the `grid` ranges the kernels use) and the same vector blocks, with the same
+// last-block elections, so the results are bit-identical to the CUDA graph's
+// launches. It runs the direct primal pass: the staged pass's ring does not
+// fit beside the other phases' shared memory. Data written earlier in the
+// launch is loaded through L2 (CO = true), never through the read-only path.
+// A barrier whose poll runs out sets the batch's error word and the CTA
+// leaves; the other CTAs' polls see the word and leave too.
+template <int CK, int PR>
+__global__ void __launch_bounds__(kThreads, 1)
+    kb_chunk(BatchBuffers B, SolveConfig cfg, int grid, int vblocks, int steps) {
+  static_assert(kThreads == kVecThreads, "the chunk runs the vector passes' blocks on its CTAs");
+  BatchActive* A = B.act;
+  const unsigned P = gridDim.x;
+  auto sync = [&]() -> bool {
+    if (grid_barrier(&A->bar_count, &A->bar_gen, P, &A->error)) return true;
+    if (threadIdx.x == 0) atomicExch(&A->error, 1);
+    return false;
+  };
+  for (long long c = blockIdx.x; c < grid; c += P) {
+    kb_eval_body<CK, PR, true>(B, c, grid);
+    __syncthreads();
+  }
+  if (!sync()) return;
+  for (long long b = blockIdx.x; b < vblocks; b += P) {
+    kb_eval_vec_body<true>(B, cfg, grid, 0, b);
+    __syncthreads();
+  }
+  if (!sync()) return;
+  if (blockIdx.x == 0) kb_compact_body<PR>(B, grid);
+  if (!sync()) return;
+  for (int k = 0; k < steps; ++k) {
+    // the same value in every CTA: read after the same barrier
+    if (__ldcg(&A->count) == 0 || __ldcg(&A->error) != 0) return;
+    for (long long c = blockIdx.x; c < grid; c += P) {
+      kb_primal_body<CK, PR, true>(B, c);
+      __syncthreads();
+    }
+    if (!sync()) return;
+    for (long long b = blockIdx.x; b < vblocks; b += P) {
+      kb_dual_body<PR, true>(B, cfg, grid, b);
+      __syncthreads();
+    }
+    if (!sync()) return;
+  }
 }
 
 // Per-instance cost norms (stage one, over the full unit line).
@@ -1255,7 +1361,12 @@ class BatchSolver {
     // plan and average are all there is to load), direct 16-byte loads for the
     // stored FP32 cost; primal_pass overrides
     const int pass = opt ? opt->primal_pass : PDOT_PASS_AUTO;
-    staged_ = pass == PDOT_PASS_STAGED || (pass == PDOT_PASS_AUTO && dim_ > 0);
+    // persistent chunks (1) run the direct pass throughout; 0 (automatic) and
+    // -1 keep the CUDA graph, which measured faster on B200
+    persistent_ = opt && opt->persistent_chunks == 1 && use_graph_;
+    if (persistent_ && pass == PDOT_PASS_STAGED)
+      bfail(PDOT_ERR_INVALID_ARGUMENT, "persistent chunks run the direct primal pass (primal_pass AUTO or DIRECT)");
+    staged_ = !persistent_ && (pass == PDOT_PASS_STAGED || (pass == PDOT_PASS_AUTO && dim_ > 0));
     int occ = 1;
     if (staged_) {
       PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_primal_staged, {
@@ -1274,6 +1385,17 @@ class BatchSolver {
     grid_ = (int)std::min<int64_t>((int64_t)sms * occ, std::max<int64_t>(units, 1));
     if (opt && opt->ctas_per_sm > 0)
       grid_ = (int)std::min<int64_t>((int64_t)std::min(opt->ctas_per_sm, occ) * sms, std::max<int64_t>(units, 1));
+    if (persistent_) {
+      // as many co-resident CTAs as the chunk kernel allows, at most one per CTA range
+      int coop = 0, cocc = 0;
+      BCK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device_));
+      PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_chunk, {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cocc, kfn, pdot::kThreads, 0) != cudaSuccess) cocc = 0;
+      });
+      cudaGetLastError();
+      if (!coop || cocc < 1) bfail(PDOT_ERR_CUDA, "this device cannot run the persistent chunk kernel");
+      chunk_ctas_ = std::min(sms * cocc, grid_);
+    }
     // per-unit overhead of the CTA split, in eighths of a full unit (0..64)
     if (opt && opt->warm_restart_at_zero != 0 && opt->warm_restart_at_zero != 1)
       bfail(PDOT_ERR_INVALID_ARGUMENT, "warm_restart_at_zero must be 0 or 1");
@@ -1466,7 +1588,7 @@ class BatchSolver {
     BCK(cudaMallocHost(&hp, sizeof(pdot::BatchActive) * 2));
     host_act_ = static_cast<pdot::BatchActive*>(hp);
     for (int k = 0; k < 2; ++k) BCK(cudaEventCreateWithFlags(&ev_[k], cudaEventDisableTiming));
-    if (use_graph_) capture();
+    if (use_graph_ && !persistent_) capture();
   }
 
   ~BatchSolver() {
@@ -1499,7 +1621,7 @@ class BatchSolver {
       ++completed;
       if (a.error) {
         BCK(cudaStreamSynchronize(stream_));
-        bfail(PDOT_ERR_CUDA, "the staged primal pass gave up waiting for its copies");
+        bfail(PDOT_ERR_CUDA, "a bounded wait timed out (the staged primal pass's copies or a persistent chunk barrier)");
       }
       if (a.count == 0) break;
       if (it > (long long)limit_ + 2 * freq_ + 16)
@@ -1635,7 +1757,7 @@ class BatchSolver {
   }
 
   bool regular_start(long long it) const {
-    if (!graph_ || it <= 10 || (it - 1) % freq_ != 0) return false;
+    if (!(graph_ || persistent_) || it <= 10 || (it - 1) % freq_ != 0) return false;
     for (long long k = it + 1; k < it + freq_; ++k)
       if (is_eval(k)) return false;
     return true;
@@ -1643,7 +1765,10 @@ class BatchSolver {
 
   void enqueue_chunk(long long& it) {
     if (regular_start(it)) {
-      BCK(cudaGraphLaunch(graph_, stream_));
+      if (persistent_)
+        launch_persistent_chunk();
+      else
+        BCK(cudaGraphLaunch(graph_, stream_));
       it += freq_;
       return;
     }
@@ -1654,6 +1779,15 @@ class BatchSolver {
       ++it;
       ++k;
     } while (k < freq_ && !regular_start(it));
+  }
+
+  // the regular chunk as one cooperative launch of kb_chunk (bit-identical to the graph)
+  void launch_persistent_chunk() {
+    int grid = grid_, vblocks = (int)total_vblocks_, steps = (int)freq_;
+    void* args[] = {&D_, &cfg_, &grid, &vblocks, &steps};
+    PDOT_BATCH_VARIANT(kind_, pr_, pdot::kb_chunk,
+                       BCK(cudaLaunchCooperativeKernel((const void*)kfn, dim3(chunk_ctas_), dim3(pdot::kThreads),
+                                                       args, 0, stream_)));
   }
 
   void capture() {
@@ -1704,7 +1838,8 @@ class BatchSolver {
     if (tmp) BCK(cudaFree(tmp));
   }
 
-  int device_ = 0, num_ = 0, dim_ = 0, kind_ = 0, grid_ = 1, pr_ = 256;
+  int device_ = 0, num_ = 0, dim_ = 0, kind_ = 0, grid_ = 1, pr_ = 256, chunk_ctas_ = 0;
+  bool persistent_ = false;  // regular chunks run as one persistent cooperative launch
   bool warm_zero_ = false;
   bool use_graph_ = true, any_warm_ = false, recover_plans_ = false, staged_ = false;
   int plan_iters_ = 0;
@@ -1751,6 +1886,8 @@ extern "C" int pdot_optimize_batched(const pdot_batch_problem* problem, const pd
     if (options && options->batch_panel_rows != 0 && options->batch_panel_rows != 128 &&
         options->batch_panel_rows != 256)
       bfail(PDOT_ERR_INVALID_ARGUMENT, "batch_panel_rows must be 0, 128 or 256");
+    if (options && (options->persistent_chunks < -1 || options->persistent_chunks > 1))
+      bfail(PDOT_ERR_INVALID_ARGUMENT, "persistent_chunks must be -1, 0 or 1");
     for (int64_t k = 0; k < problem->num_instances; ++k) {
       if (problem->num_rows[k] < 1 || problem->num_cols[k] < 1) bfail(PDOT_ERR_INVALID_ARGUMENT, "empty instance %lld", (long long)k);
       // the staged pass's producer cursor keeps positions inside an instance in 32 bits

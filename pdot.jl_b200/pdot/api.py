@@ -557,7 +557,7 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
                      use_cuda_graph: bool = True, ctas_per_sm: int = 0, warm_starts=None,
                      return_primal: bool = True, recover_plan=None, race_groups=None,
                      primal_pass: str = "auto", warm_primal_weights=None, unit_cost: float = 0.25,
-                     warm_restart: str = "warm", panel_rows: int = 256):
+                     warm_restart: str = "warm", panel_rows: int = 256, persistent: bool = False):
     """Solve many independent instances at once (pdot_optimize_batched).
 
     problems     a list of OptimalTransportProblem (cost_matrix may be None for
@@ -581,6 +581,11 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
                  256 or 128 rows (128: fewer registers per thread, three
                  resident CTAs per SM, twice the units of tall instances);
                  tune_batched picks it
+    persistent   True: every regular chunk of loop bodies (the evaluation,
+                 the compaction and the steps up to the next evaluation) runs
+                 as one persistent cooperative launch with grid barriers
+                 between the phases, with the direct primal pass; the results
+                 are bit-identical to the CUDA graph of launches (False)
     return_primal  False leaves every primal_solution None (no m x n copies)
     Returns (outputs, seconds): a SaddlePointOutput per instance (its
     iteration_stats holds the final evaluation record) and the device time.
@@ -679,6 +684,7 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
     opts.ctas_per_sm = int(ctas_per_sm)
     opts.batch_unit_cost = float(unit_cost)
     opts.batch_panel_rows = int(panel_rows)
+    opts.persistent_chunks = 1 if persistent else 0
     opts.primal_pass = {"auto": _abi.PASS_AUTO, "staged": _abi.PASS_STAGED, "direct": _abi.PASS_DIRECT}[primal_pass]
     cp = marshal_params(params)
     sec = ct.c_double(0.0)
@@ -692,7 +698,8 @@ def optimize_batched(params: PdhgParameters, problems, *, cost: str = "f32", poi
     return out, sec.value
 
 
-BATCH_TUNING_CANDIDATES = [{"primal_pass": pp, "ctas_per_sm": c} for pp in ("staged", "direct") for c in (2, 1)]
+BATCH_TUNING_CANDIDATES = ([{"primal_pass": pp, "ctas_per_sm": c} for pp in ("staged", "direct") for c in (2, 1)]
+                           + [{"primal_pass": "direct", "ctas_per_sm": 2, "persistent": True}])
 BATCH_TILE_SHAPES = ({"panel_rows": 128, "ctas_per_sm": 3}, {"panel_rows": 128, "ctas_per_sm": 2})
 BATCH_UNIT_COSTS = (0.0, 0.125, 0.25, 0.5, 8.0)
 
@@ -705,8 +712,8 @@ def tune_batched(params: PdhgParameters, problems, *, cost: str = "f32", points=
     configuration, [(configuration, seconds)]); pass the configuration's keys
     to optimize_batched. Three stages, each starting from the best so far:
     the launch configuration (the primal pass, staged by bulk copies or
-    direct, times the resident CTAs per SM of the matrix passes) with
-    256-row tiles; the tile shape (128-row panels at three or two CTAs per
+    direct, times the resident CTAs per SM of the matrix passes, and the
+    persistent chunk launch with the direct pass) with 256-row tiles; the tile shape (128-row panels at three or two CTAs per
     SM); the tile balance, the per-unit overhead that the CTA split charges
     beside a unit's rows (0 cuts ranges of equal rows, 8 nearly equal unit
     counts)."""

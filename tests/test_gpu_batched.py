@@ -189,3 +189,60 @@ def test_batch_unit_cost_is_validated(cuda):
     with pytest.raises(pdot.api._abi.PdotError) as ei:
         pdot.optimize_batched(pdot.default_parameters(1e-4), probs, cost="l1", points=pts, unit_cost=9.0)
     assert ei.value.code == pdot.api._abi.PDOT_ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("cost, panel_rows", [("l1", 256), ("f32", 256), ("l1", 128)])
+def test_batched_persistent_chunks_match_the_graph(cuda, cost, panel_rows):
+    """A regular chunk as one persistent cooperative launch runs every phase's
+    body over the same virtual CTA ranges and vector blocks as the graph's
+    launches (the direct pass, the same CTAs per SM), so the solves agree bit
+    for bit, through compactions that drop finished instances."""
+    probs, pts = instances.batched_l1(count=20, lo=3, hi=700, seed=9)
+    if cost == "f32":
+        probs = [pdot.OptimalTransportProblem(instances.l1_cost(*pt), p.source_distribution, p.target_distribution)
+                 for p, pt in zip(probs, pts)]
+    params = pdot.default_parameters(1e-4)
+    kw = {} if cost == "f32" else {"points": pts}
+    kw.update(panel_rows=panel_rows, ctas_per_sm=2, primal_pass="direct")
+    gr, _ = pdot.optimize_batched(params, probs, cost=cost, **kw)
+    pe, _ = pdot.optimize_batched(params, probs, cost=cost, persistent=True, **kw)
+    iters = set()
+    for x, y in zip(gr, pe):
+        assert x.termination_reason == OPTIMAL
+        assert x.termination_reason == y.termination_reason
+        assert x.iteration_count == y.iteration_count
+        assert np.array_equal(x.primal_solution, y.primal_solution)
+        assert np.array_equal(x.dual_source_solution, y.dual_source_solution)
+        assert np.array_equal(x.dual_target_solution, y.dual_target_solution)
+        iters.add(x.iteration_count)
+    assert max(iters) > 256 and len(iters) > 1  # a whole regular chunk, instances ending at different ones
+
+
+def test_batched_persistent_chunks_with_warm_starts_and_races(cuda):
+    """Warm starts with recovered plans and race groups through the persistent
+    chunk: the same outputs as the graph, bit for bit."""
+    probs, pts = instances.batched_l1(count=6, lo=40, hi=300, seed=4)
+    params = pdot.default_parameters(1e-4)
+    cold, _ = pdot.optimize_batched(params, probs, cost="l1", points=pts)
+    rng = np.random.default_rng(0)
+    warm = [(o.dual_source_solution * (1 + 0.05 * rng.standard_normal(o.dual_source_solution.size)),
+             o.dual_target_solution) for o in cold]
+    probs2, pts2 = probs + probs, pts + pts
+    ws = [None] * len(probs) + warm
+    groups = list(range(len(probs))) * 2
+    kw = dict(cost="l1", points=pts2, warm_starts=ws, race_groups=groups, recover_plan=(3e-4, 20),
+              primal_pass="direct", ctas_per_sm=2)
+    gr, _ = pdot.optimize_batched(params, probs2, **kw)
+    pe, _ = pdot.optimize_batched(params, probs2, persistent=True, **kw)
+    for x, y in zip(gr, pe):
+        assert x.termination_reason == y.termination_reason
+        assert x.iteration_count == y.iteration_count
+        assert np.array_equal(x.primal_solution, y.primal_solution)
+
+
+def test_batched_persistent_chunks_need_the_direct_pass(cuda):
+    probs, pts = instances.batched_l1(count=2, lo=8, hi=16, seed=1)
+    with pytest.raises(pdot.api._abi.PdotError) as ei:
+        pdot.optimize_batched(pdot.default_parameters(1e-4), probs, cost="l1", points=pts, persistent=True,
+                              primal_pass="staged")
+    assert ei.value.code == pdot.api._abi.PDOT_ERR_INVALID_ARGUMENT

@@ -663,19 +663,34 @@ def run_ours(args, world, rank, local):
         else:
             prob = pdot.OptimalTransportProblem(C_host.numpy().T, a_h, b_h)
         eparams = pdot.default_parameters(TOL, iteration_limit=args.steps)
+        # the caller's output arrays, page-locked like the input and reused by every call
+        X_pin = torch.empty((n, m), dtype=torch.float64, pin_memory=True)
+        u_pin = torch.empty(m, dtype=torch.float64, pin_memory=True)
+        v_pin = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        out_arrays = (X_pin.numpy().T, u_pin.numpy(), v_pin.numpy())
         # one untimed call first, as the warm-up steps of the primary region
-        pdot.optimize(pdot.default_parameters(TOL, iteration_limit=max(args.warmup, 1)), prob, device=local, **ekw)
-        # three timed calls, the median reported (each allocates, copies in, solves, copies out, frees)
-        calls = []
-        for _ in range(3):
-            torch.cuda.synchronize()
-            barrier(world)
-            w0 = time.perf_counter()
-            out = pdot.optimize(eparams, prob, device=local, **ekw)
-            torch.cuda.synchronize()
-            w1 = time.perf_counter()
-            calls.append(max_over_ranks(w1 - w0, world, device))
+        pdot.optimize(pdot.default_parameters(TOL, iteration_limit=max(args.warmup, 1)), prob, device=local,
+                      out=out_arrays, **ekw)
+
+        def timed_calls(**kw):
+            # three timed calls, the median reported (each allocates on the device, copies in, solves,
+            # copies out, frees)
+            calls = []
+            res = None
+            for _ in range(3):
+                torch.cuda.synchronize()
+                barrier(world)
+                w0 = time.perf_counter()
+                res = pdot.optimize(eparams, prob, device=local, **ekw, **kw)
+                torch.cuda.synchronize()
+                w1 = time.perf_counter()
+                calls.append(max_over_ranks(w1 - w0, world, device))
+            return res, calls
+
+        out, calls = timed_calls(out=out_arrays)
         e_sec = statistics.median(calls)
+        fresh, fresh_calls = timed_calls()
+        assert np.array_equal(fresh.primal_solution, out.primal_solution)
         vec_bytes = 8 * (m + n)
         h2d = (8 * (m + n) * xs.shape[1] // 2 if cost == "sqeuclid" else 8 * N) + vec_bytes
         e2e = {"value": world * out.iteration_count / e_sec, "unit": UNIT,
@@ -684,9 +699,13 @@ def run_ours(args, world, rank, local):
                "iterations_per_call": out.iteration_count, "seconds_per_call": e_sec,
                "seconds_of_the_three_calls": calls,
                "note": "the median of three pdot.optimize calls after one untimed call: H2D of C, a, b "
-                       "from pinned memory, the solve, D2H of the returned plan and duals into fresh host "
-                       "arrays; bytes amortised per iteration"}
-        del C_host
+                       "from pinned memory, the solve, D2H of the plan and duals into the caller's pinned "
+                       "output arrays (out=); bytes amortised per iteration",
+               "fresh_host_arrays": {
+                   "value": world * fresh.iteration_count / statistics.median(fresh_calls),
+                   "seconds_of_the_three_calls": fresh_calls,
+                   "note": "the same calls returning fresh numpy arrays (allocated and first touched per call)"}}
+        del C_host, X_pin, u_pin, v_pin, out_arrays
 
     mixed = None
     if not args.no_mp and precision == "f64":

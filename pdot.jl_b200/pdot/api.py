@@ -324,11 +324,28 @@ def stats_from_c(s: _abi.IterationStatsC) -> IterationStats:
     )
 
 
+def _check_out(out, m: int, n: int):
+    """The caller's (X, u, v) output arrays: FP64, X m x n column-major, u of
+    m and v of n entries, contiguous and writeable."""
+    if len(out) != 3:
+        raise ValueError("out must be (X, u, v)")
+    X, u, v = out
+    for name, arr, shape in (("X", X, (m, n)), ("u", u, (m,)), ("v", v, (n,))):
+        if not isinstance(arr, np.ndarray) or arr.dtype != np.float64 or arr.shape != shape:
+            raise ValueError(f"out {name} must be a float64 array of shape {shape}")
+        if not arr.flags.writeable or not (arr.flags.f_contiguous if name == "X" else arr.flags.c_contiguous):
+            raise ValueError(f"out {name} must be writeable and {'column-major' if name == 'X' else 'contiguous'}")
+    return X, u, v
+
+
 class OutputBuffers:
-    def __init__(self, m: int, n: int, stats_capacity: int):
-        self.X = np.zeros((m, n), dtype=np.float64, order="F")
-        self.u = np.zeros(m, dtype=np.float64)
-        self.v = np.zeros(n, dtype=np.float64)
+    def __init__(self, m: int, n: int, stats_capacity: int, out=None):
+        if out is not None:
+            self.X, self.u, self.v = _check_out(out, m, n)
+        else:
+            self.X = np.zeros((m, n), dtype=np.float64, order="F")
+            self.u = np.zeros(m, dtype=np.float64)
+            self.v = np.zeros(n, dtype=np.float64)
         self.stats = (_abi.IterationStatsC * max(stats_capacity, 1))()
         self.c = _abi.SaddlePointOutputC()
         self.c.primal_solution = _dptr(self.X)
@@ -457,13 +474,17 @@ def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device
              cost_scale: Optional[float] = None, warm_start=None, primal_pass: str = "auto",
              recover_plan=None, fail_bounded_waits: bool = False,
              warm_primal_weight: Optional[float] = None, warm_restart: str = "warm",
-             persistent: Optional[bool] = None) -> SaddlePointOutput:
+             persistent: Optional[bool] = None, out=None) -> SaddlePointOutput:
     """PDOT.optimize, src/solver_gpu.jl:413-720, run by libpdot.so on the GPU.
 
     The keyword options beyond `device` select this implementation's mixed
     precision (FP32 plan; FP32/BF16/coordinate cost), a warm start from
     given duals (and plan) and how regular chunks launch (`persistent`, see
-    _options); the defaults are the FP64 drop-in."""
+    _options); the defaults are the FP64 drop-in. `out` = (X, u, v) are the
+    caller's arrays for the solution (float64; X m x n column-major), as the
+    C ABI's output pointers are: reused across calls they save the allocation
+    and first touch of fresh arrays, and page-locked ones (a pinned torch
+    tensor's numpy view) receive the plan by one DMA."""
     validate(params)
     lib = _abi.load()
     mp = MarshalledProblem(problem)
@@ -473,7 +494,7 @@ def optimize(params: PdhgParameters, problem: OptimalTransportProblem, *, device
                            recover_plan=recover_plan, fail_bounded_waits=fail_bounded_waits,
                            warm_primal_weight=warm_primal_weight, warm_restart=warm_restart,
                            persistent=persistent)
-    ob = OutputBuffers(mp.m, mp.n, stats_capacity_for(params))
+    ob = OutputBuffers(mp.m, mp.n, stats_capacity_for(params), out=out)
     rc = lib.pdot_optimize(ct.byref(mp.c), ct.byref(cp), ct.byref(opts), ct.byref(ob.c))
     _abi.check(lib, rc, "pdot_optimize")
     return ob.to_output()

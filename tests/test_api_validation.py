@@ -115,3 +115,24 @@ def test_batch_panel_rows_is_validated_before_device_work(built):
         pdot.optimize_batched(pdot.default_parameters(1e-4), probs, cost="l1", points=pts, panel_rows=192)
     assert ei.value.code == _abi.PDOT_ERR_INVALID_ARGUMENT
     assert "batch_panel_rows" in str(ei.value)
+
+
+def test_caller_output_arrays_are_checked_before_device_work(built):
+    prob = instances.uniform_sqeuclid(4, 3, seed=0)
+    params = pdot.default_parameters(1e-4)
+    good = (np.zeros((4, 3), order="F"), np.zeros(4), np.zeros(3))
+    bad = [
+        (np.zeros((4, 3), order="C"), good[1], good[2]),          # X row-major
+        (np.zeros((3, 4), order="F"), good[1], good[2]),          # X shape
+        (np.zeros((4, 3), order="F", dtype=np.float32), good[1], good[2]),
+        (good[0], np.zeros(3), good[2]),                          # u size
+        (good[0], good[1], np.zeros(4)),                          # v size
+        good[:2],
+    ]
+    for out in bad:
+        with pytest.raises(ValueError):
+            pdot.optimize(params, prob, out=out)
+    ro = np.zeros(4)
+    ro.flags.writeable = False
+    with pytest.raises(ValueError):
+        pdot.optimize(params, prob, out=(good[0], ro, good[2]))

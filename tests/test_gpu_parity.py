@@ -356,3 +356,26 @@ def test_device_cost_builder_matches_host_generator(cuda):
     _abi.check(lib, rc, "pdot_sqeuclid_cost_f64")
     torch.cuda.synchronize()
     assert np.array_equal(C.cpu().numpy().T, instances.sqeuclid_cost(xs, ys))
+
+
+def test_caller_output_arrays_receive_the_same_solution(cuda):
+    """optimize(out=(X, u, v)) writes the solution into the caller's arrays,
+    page-locked (one DMA) or pageable (staged copy), bit for bit what the
+    default fresh arrays receive; the arrays are reused across calls."""
+    import torch
+
+    prob = instances.uniform_sqeuclid(3000, 2000, seed=4)
+    params = pdot.default_parameters(1e-4, iteration_limit=40)
+    ref = pdot.optimize(params, prob)
+    m, n = 3000, 2000
+    pinned = (torch.empty((n, m), dtype=torch.float64, pin_memory=True).numpy().T,
+              torch.empty(m, dtype=torch.float64, pin_memory=True).numpy(),
+              torch.empty(n, dtype=torch.float64, pin_memory=True).numpy())
+    pageable = (np.full((m, n), np.nan, order="F"), np.full(m, np.nan), np.full(n, np.nan))
+    for out in (pinned, pageable, pinned):
+        res = pdot.optimize(params, prob, out=out)
+        assert res.primal_solution is out[0]
+        assert res.iteration_count == ref.iteration_count
+        assert np.array_equal(out[0], ref.primal_solution)
+        assert np.array_equal(out[1], ref.dual_source_solution)
+        assert np.array_equal(out[2], ref.dual_target_solution)

@@ -452,22 +452,33 @@ def run_c2(args, device, local):
 WARM_GRID, WARM_EPS, WARM_ROUNDS = 128, 3e-4, 100  # coarse-to-fine warm start of the 20000 x 15000 solve
 
 
-def run_warm_mixed(args, params, m, n, xs, ys, a_h, b_h, Ct, a, b, xs_d, ys_d, device, local, fp64_ttk):
+def run_warm_mixed(args, params, m, n, xs, ys, a_h, b_h, Ct, a, b, xs_d, ys_d, device, local, fp64_ttk,
+                   learned=False):
     """The mixed-precision solve (FP32 plan, cost from FP32 coordinates) from
     the coarse-to-fine warm start: points binned on a 128 x 128 grid, the binned
     problem solved, its duals extended to every point by the c-transform, a
     plan recovered from them by 100 balancing rounds (eps 3e-4), then PDHG to
-    relative KKT 1e-4. One wall-clock region covers all of it, from the host
-    points to the plan back on the host; the answer is judged on the FP64
-    problem."""
+    relative KKT 1e-4. With `learned`, the coarse solve itself starts from the
+    packaged network's 32 x 32 prediction (multiscale.learned_coarse_to_fine_duals;
+    loading the network is outside the region). One wall-clock region covers
+    all of it, from the host points to the plan back on the host; the answer is
+    judged on the FP64 problem."""
     import torch
 
     import pdot
     from pdot import multiscale
 
+    starter = None
+    if learned:
+        from pdot import learned as learned_mod
+
+        starter = learned_mod.WarmStarter(device=local)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    u, v, info = multiscale.coarse_to_fine_duals(xs, ys, a_h, b_h, G=WARM_GRID, device=local)
+    if learned:
+        u, v, info = multiscale.learned_coarse_to_fine_duals(xs, ys, a_h, b_h, starter, G=WARM_GRID)
+    else:
+        u, v, info = multiscale.coarse_to_fine_duals(xs, ys, a_h, b_h, G=WARM_GRID, device=local)
     t1 = time.perf_counter()
     ud = torch.from_numpy(u).to(device)
     vd = torch.from_numpy(v).to(device)
@@ -483,7 +494,9 @@ def run_warm_mixed(args, params, m, n, xs, ys, a_h, b_h, Ct, a, b, xs_d, ys_d, d
                           torch.from_numpy(res.dual_target_solution).to(device))
     del X_t
     total = t2 - t0
-    return {"workload": f"FP32 plan, cost from FP32 coordinates, coarse-to-fine warm start (grid {WARM_GRID}, "
+    kind = "learned coarse-to-fine warm start (the network's 32 x 32 duals start the " if learned else \
+        "coarse-to-fine warm start ("
+    return {"workload": f"FP32 plan, cost from FP32 coordinates, {kind}grid {WARM_GRID} coarse solve, "
                         f"plan recovered with eps {WARM_EPS}, {WARM_ROUNDS} rounds), tol {TOL}",
             "seconds": total, "prep_seconds": t1 - t0, "coarse": info, "iterations": res.iteration_count,
             "termination": res.termination_string, "fp64_evaluation": k64,
@@ -714,6 +727,9 @@ def run_ours(args, world, rank, local):
         if not args.no_ttk:
             mixed["sqeuclid"]["warm_start"] = run_warm_mixed(args, params, m, n, xs, ys, a_h, b_h, Ct, a, b, xs_d,
                                                              ys_d, device, local, ttk["seconds"] if ttk else None)
+            mixed["sqeuclid"]["learned_warm_start"] = run_warm_mixed(
+                args, params, m, n, xs, ys, a_h, b_h, Ct, a, b, xs_d, ys_d, device, local,
+                ttk["seconds"] if ttk else None, learned=True)
 
     batched = run_batched(args, device) if not args.no_batched else None
     learned_ws = run_learned(args, device) if not args.no_learned else None

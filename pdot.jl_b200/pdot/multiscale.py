@@ -94,33 +94,68 @@ def c_transform(points, centres: np.ndarray, dual: np.ndarray, scale: float, *, 
     return out.cpu().numpy()
 
 
-def learned_to_fine_duals(xs, ys, a, b, starter, *, scale: float | None = None, floor: float = 1e-6):
-    """Warm-start duals (u, v) for the fine problem from the learned network
-    instead of a coarse solve: both point sets are binned on the network's
-    32 x 32 grid over their common bounding square, the network predicts the
-    grid problem's duals (its cost is the squared grid distance divided by its
-    maximum, 2 * 31^2), they are rescaled to the fine cost between cell centres,
-    scale * (side / 32)^2 * |g_I - g_J|^2, and extended to every point by the
-    c-transform over the non-empty cells. `starter` is a learned.WarmStarter;
-    empty cells get `floor` mass before the histograms are renormalised, as the
-    training histograms carry a small floor."""
+def _grid_prediction(xs, ys, a, b, starter, scale: float, floor: float):
+    """The network's duals of the binned problem on its 32 x 32 grid over the
+    common bounding square of the two point sets (empty cells get `floor` mass
+    before the histograms are renormalised, as the training histograms carry a
+    small floor), rescaled to the cost scale * ||c_I - c_J||^2 between cell
+    centres: (centres, non-empty source cells, non-empty target cells, source
+    duals, target duals)."""
     from .learned import SIDE
 
     G = SIDE
-    xs, ys = np.asarray(xs, dtype=np.float64), np.asarray(ys, dtype=np.float64)
-    s = scale if scale is not None else 1.0 / max_sq_distance(xs, ys, device=starter.device)
     lo, side = bounding_square(xs, ys)
     A, _ = bin_masses(xs, a, lo, side, G)
     B, _ = bin_masses(ys, b, lo, side, G)
     ha = (A + floor) / (A + floor).sum()
     hb = (B + floor) / (B + floor).sum()
     U, V = starter.predict(ha[None, :], hb[None, :])
-    kappa = s * (side / G) ** 2 * 2.0 * (G - 1) ** 2
-    cent = cell_centres(lo, side, G)
-    ia, ib = np.nonzero(A > 0)[0], np.nonzero(B > 0)[0]
-    u = c_transform(xs, cent[ib], kappa * V[0][ib], s, device=starter.device)
-    v = c_transform(ys, cent[ia], kappa * U[0][ia], s, device=starter.device)
+    # the network's cost is the squared grid distance divided by its maximum, 2 * 31^2
+    kappa = scale * (side / G) ** 2 * 2.0 * (G - 1) ** 2
+    return cell_centres(lo, side, G), np.nonzero(A > 0)[0], np.nonzero(B > 0)[0], kappa * U[0], kappa * V[0]
+
+
+def learned_to_fine_duals(xs, ys, a, b, starter, *, scale: float | None = None, floor: float = 1e-6):
+    """Warm-start duals (u, v) for the fine problem from the learned network
+    instead of a coarse solve: the network predicts the duals of the problem
+    binned on its 32 x 32 grid (_grid_prediction), and they are extended to
+    every point by the c-transform over the non-empty cells. `starter` is a
+    learned.WarmStarter."""
+    xs, ys = np.asarray(xs, dtype=np.float64), np.asarray(ys, dtype=np.float64)
+    s = scale if scale is not None else 1.0 / max_sq_distance(xs, ys, device=starter.device)
+    cent, ia, ib, U, V = _grid_prediction(xs, ys, a, b, starter, s, floor)
+    u = c_transform(xs, cent[ib], V[ib], s, device=starter.device)
+    v = c_transform(ys, cent[ia], U[ia], s, device=starter.device)
     return u, v, {"cells": [int(ia.size), int(ib.size)]}
+
+
+def learned_coarse_to_fine_duals(xs, ys, a, b, starter, *, G: int = 128, tol: float = 1e-4,
+                                 iteration_limit: int = 200_000, floor: float = 1e-6,
+                                 recover_plan=(3e-4, 100), warm_restart: str = "zero"):
+    """Warm-start duals (u, v) for the fine problem through a learned coarse
+    solve: the network's 32 x 32 duals (_grid_prediction), extended by the
+    c-transform to the non-empty cells of a G x G binning, warm-start the G x G
+    coarse solve (a plan recovered from them, the zero point's restart record
+    as the network's grid warm starts use); its duals are then extended to
+    every point, as coarse_to_fine_duals does. Returns (u, v, facts)."""
+    from .solve import default_parameters
+
+    xs, ys = np.asarray(xs, dtype=np.float64), np.asarray(ys, dtype=np.float64)
+    dev = starter.device
+    s = 1.0 / max_sq_distance(xs, ys, device=dev)
+    Cc, A, B, ca, cb = coarse_problem(xs, ys, a, b, G, s)
+    cent, ia, ib, U, V = _grid_prediction(xs, ys, a, b, starter, s, floor)
+    u0 = c_transform(ca, cent[ib], V[ib], s, device=dev)
+    v0 = c_transform(cb, cent[ia], U[ia], s, device=dev)
+    params = default_parameters(tol, iteration_limit=iteration_limit)
+    out = api.optimize(params, api.OptimalTransportProblem(Cc, A, B), device=dev, warm_start=(u0, v0),
+                       recover_plan=recover_plan, warm_restart=warm_restart)
+    u = c_transform(xs, cb, out.dual_target_solution, s, device=dev)
+    v = c_transform(ys, ca, out.dual_source_solution, s, device=dev)
+    info = {"cells": [int(A.size), int(B.size)], "coarse_iterations": out.iteration_count,
+            "coarse_termination": out.termination_string,
+            "coarse_seconds": out.iteration_stats[-1].cumulative_time_sec}
+    return u, v, info
 
 
 def coarse_to_fine_duals(xs, ys, a, b, *, G: int = 128, tol: float = 1e-4, iteration_limit: int = 200_000,

@@ -47,3 +47,28 @@ def test_coarse_to_fine_warm_start_solves_the_fine_problem(cuda):
     out = pdot.optimize(pdot.default_parameters(1e-4), prob, precision="f32", cost="sqeuclid", points=pts,
                         warm_start=(u, v), recover_plan=(3e-4, 100))
     assert out.termination_reason == pdot.TerminationReason.TERMINATION_REASON_OPTIMAL
+
+
+@pytest.mark.parametrize("coarse", [False, True])
+def test_learned_point_cloud_warm_starts_solve_the_fine_problem(cuda, coarse):
+    """The packaged network's warm starts for a point cloud: its 32 x 32 grid
+    duals extended to every point, or first to the cells of a 16 x 16 coarse
+    solve that they warm-start. The duals are finite and the fine solve from
+    them ends optimal."""
+    import pdot
+    from pdot import learned
+
+    xs, ys, a, b = instances.gauss_mixture_instance(400, 300, seed=3)
+    st = learned.WarmStarter(device=0)
+    if coarse:
+        u, v, info = multiscale.learned_coarse_to_fine_duals(xs, ys, a, b, st, G=16)
+        assert info["coarse_termination"] == "OPTIMAL"
+    else:
+        u, v, info = multiscale.learned_to_fine_duals(xs, ys, a, b, st)
+    assert u.shape == (400,) and v.shape == (300,)
+    assert np.all(np.isfinite(u)) and np.all(np.isfinite(v))
+    prob = pdot.OptimalTransportProblem(None, a, b)
+    pts = (xs.astype(np.float32), ys.astype(np.float32))
+    out = pdot.optimize(pdot.default_parameters(1e-4), prob, precision="f32", cost="sqeuclid", points=pts,
+                        warm_start=(u, v), recover_plan=(3e-4, 100))
+    assert out.termination_reason == pdot.TerminationReason.TERMINATION_REASON_OPTIMAL

@@ -12,7 +12,7 @@
 // the batch's tile shape) of all active instances are concatenated into one
 // line and cut into contiguous CTA ranges of equal cost, a unit costing its
 // rows plus a fixed per-unit overhead (the autotuner picks the tile and the
-// overhead). The units of uneven instances carry from 1 to 256 rows,
+// overhead). The units of uneven instances carry from 1 to the panel's rows,
 // so ranges of equal unit count would leave some CTAs with several times the
 // bytes of others. kb_compact recomputes the ranges (cta_begin) whenever the
 // active list changes. Row
@@ -958,7 +958,7 @@ __global__ void __launch_bounds__(kVecThreads) kb_eval_vec(BatchBuffers B, Solve
 // then the CTA ranges: CTA c starts at the first active unit whose cumulative
 // cost reaches c / grid of the total, a unit costing 8 * rows + unit_cost * 256
 // (integers, so the split is exact and repeatable). Within an instance the
-// units run panel-major, n units of 256 rows per full panel and n units of the
+// units run panel-major, n units of PR rows per full panel and n units of the
 // remaining rows in the last panel, so the start of a range follows in closed
 // form after a binary search over the instances' cost prefix.
 // One CTA of blockDim.x <= 1024 threads runs it (the kernel: 1024; the

@@ -1363,7 +1363,7 @@ class BatchSolver {
     const int pass = opt ? opt->primal_pass : PDOT_PASS_AUTO;
     // persistent chunks (1) run the direct pass throughout; 0 (automatic) and
     // -1 keep the CUDA graph, which measured faster on B200
-    persistent_ = opt && opt->persistent_chunks == 1 && use_graph_;
+    persistent_ = opt && opt->persistent_chunks == 1;
     if (persistent_ && pass == PDOT_PASS_STAGED)
       bfail(PDOT_ERR_INVALID_ARGUMENT, "persistent chunks run the direct primal pass (primal_pass AUTO or DIRECT)");
     staged_ = !persistent_ && (pass == PDOT_PASS_STAGED || (pass == PDOT_PASS_AUTO && dim_ > 0));
